@@ -1,0 +1,155 @@
+/*
+ * parlayann_b200.h -- C ABI of the B200 (sm_100a) implementation of
+ * ParlayANN's beam search and Vamana build.
+ *
+ * Every entry point returns an int status (PANN_OK = 0) and records a message
+ * for pann_last_error() on failure; none aborts the process. Plain pointers
+ * and sizes only. Host-buffer entry points copy inputs in and results out and
+ * return when results are in the caller's buffers; *_device entry points take
+ * device pointers and a cudaStream_t (passed as void*) and return without
+ * synchronising.
+ *
+ * Each declaration names the reference interface it replaces
+ * (paths relative to the ParlayANN checkout).
+ */
+#ifndef PARLAYANN_B200_H_
+#define PARLAYANN_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; the reference abort()s in these cases
+ * (beamSearch.h:51-57,507-511,557-562; graph.h:79-83; index.h:193-199) */
+#define PANN_OK 0
+#define PANN_EINVAL 1    /* bad argument (k > L, no start point, bad id, ...) */
+#define PANN_ENOMEM 2    /* device or host allocation failed */
+#define PANN_ETIMEOUT 3  /* a bounded device wait gave up */
+#define PANN_EDEVICE 4   /* CUDA error, or no usable sm_100 device */
+#define PANN_EOVERFLOW 5 /* a query's seen-set or visited list outgrew every tier */
+#define PANN_ESHORT 6    /* a query returned fewer than k results (beamSearch.h:557-562) */
+
+/* element types: uint8_t, int8_t, float (Euclidian_Point<T> / Mips_Point<T>) */
+#define PANN_U8 0
+#define PANN_I8 1
+#define PANN_F32 2
+/* distances: Euclidian (euclidian_point.h:45-90) and mips (mips_point.h:44-66) */
+#define PANN_L2 0
+#define PANN_MIPS 1
+
+typedef struct pann_index pann_index;
+
+/* QueryParams (algorithms/utils/types.h:233-252): k, beamSize, limit,
+ * degree_limit, batch_factor. */
+typedef struct {
+  uint32_t k;
+  uint32_t beam;          /* beamSize (L) */
+  uint64_t limit;         /* maximum number of visited nodes */
+  uint32_t degree_limit;  /* neighbours read per visited node */
+  double batch_factor;    /* deferral threshold, fraction of beam */
+} pann_query_params;
+
+/* BuildParams fields used by the Vamana build (types.h:155-230). */
+typedef struct {
+  uint32_t R;             /* max degree */
+  uint32_t L;             /* build beam */
+  double alpha;
+  int32_t num_passes;     /* alpha = 1.0 on all but the last pass (index.h:173-178) */
+  double batch_factor;    /* QueryParams.batch_factor of the build searches */
+  uint64_t perm_seed;     /* insertion order when perm == NULL */
+  int32_t sort_neighbors; /* final per-vertex sort by distance (index.h:180-185) */
+} pann_build_params;
+
+/* Per-query counters of stats<T> (stats.h:120-155) plus seen-set diagnostics. */
+typedef struct {
+  double seconds;          /* whole build, device time */
+  double search_seconds;   /* beam search phase (t_beam, index.h:245,275) */
+  double prune_seconds;    /* robustPrune of inserted points (inside t_beam) */
+  double reverse_seconds;  /* reverse edges: group + append/prune (t_bidirect + t_prune) */
+  uint64_t dist_cmps;      /* distance comparisons of searches + prunes */
+  uint64_t visited_total;  /* sum of visited-list sizes */
+  uint32_t batches;        /* batch_insert rounds over all passes */
+  uint32_t flagged;        /* searches where the reference hashset would have grown */
+} pann_build_stats;
+
+/* ---------------------------------------------------------------- index */
+
+/* Create an empty index on the current CUDA device: n points of dimension d,
+ * element type dtype (PANN_U8/I8/F32), distance metric (PANN_L2/MIPS), graph
+ * max degree R. Replaces PointRange<P>(...) + Graph<uint>(maxDeg, n)
+ * (point_range.h:54-117, graph.h:147-149). */
+int pann_index_create(pann_index** out, int dtype, int metric, uint64_t n, uint32_t d, uint32_t R);
+int pann_index_destroy(pann_index* idx);
+
+/* Load the n x d vectors (dense, row-major) into HBM. on_device != 0 means
+ * `vectors` is a device pointer. Replaces PointRange(char* file)
+ * (point_range.h:74-117). */
+int pann_index_set_points(pann_index* idx, const void* vectors, int on_device);
+
+/* Upload / download the graph in the reference layout: n rows of R+1 uint32,
+ * slot 0 = degree (graph.h:138-145,239-247). */
+int pann_graph_upload(pann_index* idx, const uint32_t* rows, int on_device);
+int pann_graph_download(pann_index* idx, uint32_t* rows);
+
+/* Read / write the reference's graph file: uint32 n, uint32 maxDeg,
+ * uint32 deg[n], then the edges (Graph(char*) graph.h:151-208, save graph.h:210-237). */
+int pann_graph_load(pann_index* idx, const char* path);
+int pann_graph_save(pann_index* idx, const char* path);
+
+/* ---------------------------------------------------------------- search */
+
+/* Beam search for nq queries from the given start points with one set of
+ * QueryParams; host buffers. Writes the first k frontier entries (ids,
+ * distances) per query, and per-query visited-list size and distance
+ * comparisons (stats<T> counters). Any of out_dists / out_visited / out_cmps /
+ * out_flags may be NULL. out_flags bit 1: the reference's hashset would have
+ * grown on that query (hashset.h:25-38).
+ * Replaces qsearchAll / searchAll / beam_search (beamSearch.h:420-445,
+ * 492-526, 599-646). */
+int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                const uint32_t* starts, uint32_t n_start, uint32_t* out_ids, float* out_dists,
+                uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags);
+
+/* Same, with every buffer in device memory, on `stream` (a cudaStream_t).
+ * Does not synchronise; errors detected on the device are reported by the
+ * next pann_search_status() call. starts is a HOST array. */
+int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
+                       const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
+                       uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
+
+/* ---------------------------------------------------------------- build */
+
+/* Vamana batch-insertion build into the index's graph (knn_index::build_index,
+ * index.h:150-186, batch_insert :188-319). perm (host, length n) is the
+ * insertion order; NULL derives it from bp->perm_seed (points ordered by
+ * splitmix64(seed + i)). stats may be NULL. */
+int pann_build(pann_index* idx, const pann_build_params* bp, const uint32_t* perm, pann_build_stats* stats);
+
+/* ---------------------------------------------------------------- brute force */
+
+/* Exact top-k by full scan (data_tools/compute_groundtruth.cpp:22-60):
+ * integer types in exact integer arithmetic, float in FP64. Ties ordered by id.
+ * Host buffers; out_dists may be NULL. */
+int pann_groundtruth(pann_index* idx, const void* queries, uint32_t nq, uint32_t k, uint32_t* out_ids,
+                     double* out_dists);
+
+/* ---------------------------------------------------------------- misc */
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* pann_last_error(void);
+
+/* Seeded synthetic mixture data (host, deterministic, multi-threaded):
+ * n x d rows from `components` Gaussian centres. dtype PANN_U8: centres
+ * uniform in [lo, hi] per dimension, values rounded and clipped to [0,255];
+ * PANN_F32: centres N(0,1) per dimension, rows L2-normalised when normalize.
+ * stream 0 = base points, 1 = queries (independent draws, same centres). */
+int pann_synth_mixture(int dtype, uint64_t n, uint32_t d, uint32_t components, uint64_t seed,
+                       uint32_t stream, double lo, double hi, double sigma, int normalize, void* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PARLAYANN_B200_H_ */

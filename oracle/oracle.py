@@ -1,0 +1,224 @@
+"""ctypes bindings of the oracle libraries (TEST INFRASTRUCTURE ONLY).
+
+  libpann_oracle.so   the C restatement of the reference's hot path (pann_oracle.c)
+  _ref/libpann_ref.so the reference's own headers compiled in place (ref_driver.cpp)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker / the timed reference. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libpann_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libpann_ref.so")
+_DT = {np.dtype(np.uint8): 0, np.dtype(np.int8): 1, np.dtype(np.float32): 2}
+
+_P = ctypes.c_void_p
+_U32, _U64, _I, _D = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+
+
+def build():
+    """Compile the oracle (and the in-place reference where its checkout exists)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+_olib = None
+_rlib = None
+
+
+def olib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.oracle_search.restype = _I
+        L.oracle_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _U32, _P,
+                                    _P, _P, _P, _P, _P, _P, _P, _P, _U32, _P, _P]
+        L.oracle_robust_prune.restype = _I
+        L.oracle_robust_prune.argtypes = [_I, _I, _U32, _P, _U32, _P, _U32, _U32, _P, _P, _D, _I, _P, _P, _P]
+        L.oracle_build.restype = _I
+        L.oracle_build.argtypes = [_I, _I, _U32, _U32, _P, _U32, _U32, _D, _I, _D, _P, _U64, _I, _P, _P]
+        L.oracle_groundtruth.restype = _I
+        L.oracle_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _P]
+        L.oracle_permutation.restype = None
+        L.oracle_permutation.argtypes = [_U32, _U64, _P]
+        L.oracle_batch_schedule.restype = _U32
+        L.oracle_batch_schedule.argtypes = [_U64, _U64, _D, _D, _P, _P, _U32]
+        L.oracle_distance.restype = ctypes.c_float
+        L.oracle_distance.argtypes = [_I, _I, ctypes.c_uint, _P, _P]
+        _olib = L
+    return _olib
+
+
+def have_ref() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def rlib():
+    global _rlib
+    if _rlib is None:
+        L = ctypes.CDLL(REF_SO)
+        L.ref_search.restype = _I
+        L.ref_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _U32, _P, _P,
+                                 _P, _P, _P, _P, _P, _P, _U32, _P, _P]
+        L.ref_qsearch_time.restype = _D
+        L.ref_qsearch_time.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _D, _P, _P, _P]
+        L.ref_robust_prune.restype = _I
+        L.ref_robust_prune.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _U32, _P, _P, _D, _I, _P, _P, _P]
+        L.ref_build.restype = _I
+        L.ref_build.argtypes = [_I, _I, _U32, _U32, _P, _U32, _U32, _D, _I, _D, _P, _P, _P, _P]
+        L.ref_num_workers.restype = _I
+        L.ref_num_workers.argtypes = []
+        _rlib = L
+    return _rlib
+
+
+def search(impl: str, base, queries, graph, k, L, limit=None, degree_limit=None, batch_factor=0.125, starts=(0,),
+           metric=0, full=False, visited_cap=None):
+    """Beam search per query through the oracle ('oracle') or the in-place reference ('ref').
+    graph: n x (R+1) uint32 reference rows. Returns a dict of arrays."""
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    nq = queries.shape[0]
+    limit = n if limit is None else limit
+    degree_limit = R if degree_limit is None else degree_limit
+    st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+    ids = np.zeros((nq, k), np.uint32)
+    dists = np.zeros((nq, k), np.float32)
+    vis = np.zeros(nq, np.uint32)
+    cmps = np.zeros(nq, np.uint32)
+    out = dict(ids=ids, dists=dists, visited=vis, cmps=cmps)
+    fn = fi = fd = vi = vd = None
+    vcap = 0
+    if full:
+        fn = np.zeros(nq, np.uint32)
+        fi = np.zeros((nq, L), np.uint32)
+        fd = np.zeros((nq, L), np.float32)
+        vcap = visited_cap or 4 * L + 64
+        vi = np.zeros((nq, vcap), np.uint32)
+        vd = np.zeros((nq, vcap), np.float32)
+        out.update(frontier_n=fn, frontier_ids=fi, frontier_d=fd, visited_ids=vi, visited_d=vd)
+    dt = _DT[base.dtype]
+    if impl == "oracle":
+        grew = np.zeros(nq, np.int32)
+        rc = olib().oracle_search(dt, metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit,
+                                  degree_limit, batch_factor, len(st), _p(st), _p(ids), _p(dists), _p(vis), _p(cmps),
+                                  _p(grew), _p(fn), _p(fi), _p(fd), vcap, _p(vi), _p(vd))
+        out["hash_grew"] = grew
+    else:
+        rc = rlib().ref_search(dt, metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit, degree_limit,
+                               batch_factor, len(st), _p(st), _p(ids), _p(dists), _p(vis), _p(cmps), _p(fn), _p(fi),
+                               _p(fd), vcap, _p(vi), _p(vd))
+    out["rc"] = rc
+    return out
+
+
+def robust_prune(impl, base, graph, p, cand_ids, cand_d, alpha, add=True, metric=0):
+    base = np.ascontiguousarray(base)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    ci = np.ascontiguousarray(cand_ids, dtype=np.uint32)
+    cd = np.ascontiguousarray(cand_d, dtype=np.float32)
+    out = np.zeros(R + 1, np.uint32)
+    nout = np.zeros(1, np.uint32)
+    cm = np.zeros(1, np.int64)
+    dt = _DT[base.dtype]
+    if impl == "oracle":
+        olib().oracle_robust_prune(dt, metric, d, _p(base), R, _p(graph), p, len(ci), _p(ci), _p(cd), alpha, int(add),
+                                   _p(out), _p(nout), _p(cm))
+    else:
+        rlib().ref_robust_prune(dt, metric, n, d, _p(base), R, _p(graph), p, len(ci), _p(ci), _p(cd), alpha, int(add),
+                                _p(out), _p(nout), _p(cm))
+    return out[: int(nout[0])].copy(), int(cm[0])
+
+
+def build_graph(impl, base, R, L, alpha, passes, batch_factor=0.125, perm=None, perm_seed=0x5EED5EED5EED,
+                sort_neighbors=True, metric=0):
+    """Vamana build; returns (n x (R+1) reference rows, total distance comparisons)."""
+    base = np.ascontiguousarray(base)
+    n, d = base.shape
+    g = np.zeros((n, R + 1), np.uint32)
+    dt = _DT[base.dtype]
+    tot = np.zeros(1, np.uint64)
+    if impl == "oracle":
+        pm = None if perm is None else np.ascontiguousarray(perm, dtype=np.uint32)
+        rc = olib().oracle_build(dt, metric, n, d, _p(base), R, L, alpha, passes, batch_factor, _p(pm), perm_seed,
+                                 int(sort_neighbors), _p(g), _p(tot))
+    else:
+        secs = np.zeros(1, np.float64)
+        vis = np.zeros(n, np.uint32)
+        rc = rlib().ref_build(dt, metric, n, d, _p(base), R, L, alpha, passes, batch_factor, _p(g), _p(secs), _p(tot),
+                              _p(vis))
+    assert rc == 0, rc
+    return g, int(tot[0])
+
+
+def groundtruth(base, queries, k, metric=0):
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    n, d = base.shape
+    ids = np.zeros((queries.shape[0], k), np.uint32)
+    dd = np.zeros((queries.shape[0], k), np.float64)
+    olib().oracle_groundtruth(_DT[base.dtype], metric, n, d, _p(base), queries.shape[0], _p(queries), k, _p(ids),
+                              _p(dd))
+    return ids, dd
+
+
+def permutation(n, seed=0x5EED5EED5EED):
+    out = np.zeros(n, np.uint32)
+    olib().oracle_permutation(n, seed, _p(out))
+    return out
+
+
+def batch_schedule(n, m=None):
+    m = n if m is None else m
+    fl = np.zeros(8192, np.uint64)
+    ce = np.zeros(8192, np.uint64)
+    nb = olib().oracle_batch_schedule(n, m, 2.0, 0.02, _p(fl), _p(ce), 8192)
+    return list(zip(fl[:nb].tolist(), ce[:nb].tolist()))
+
+
+def qsearch_time(base, queries, graph, k, L, batch_factor=0.125, metric=0):
+    """The reference's qsearchAll timed as checkRecall times it (check_nn_recall.h:46-59)."""
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    nq = queries.shape[0]
+    ids = np.zeros((nq, k), np.uint32)
+    vis = np.zeros(nq, np.uint32)
+    cmps = np.zeros(nq, np.uint32)
+    secs = rlib().ref_qsearch_time(_DT[base.dtype], metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L,
+                                   batch_factor, _p(ids), _p(vis), _p(cmps))
+    return secs, ids, vis, cmps
+
+
+def random_graph(n, R, seed, min_deg=1):
+    """Seeded random graph in the reference layout (degree slot + padded rows)."""
+    rng = np.random.default_rng(seed)
+    g = np.zeros((n, R + 1), np.uint32)
+    for i in range(n):
+        deg = int(rng.integers(min_deg, R + 1))
+        nb = rng.choice(n, size=deg, replace=False)
+        g[i, 0] = deg
+        g[i, 1:1 + deg] = nb
+    return g

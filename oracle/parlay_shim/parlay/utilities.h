@@ -1,0 +1,3 @@
+// Part of the ParlayLib-API shim (test infrastructure for the oracle only).
+#pragma once
+#include "internal/shim_core.h"

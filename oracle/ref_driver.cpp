@@ -1,0 +1,244 @@
+// Oracle driver around the REFERENCE's own code, compiled in place.
+//
+// TEST INFRASTRUCTURE ONLY. This file includes ParlayANN's headers from the
+// reference checkout (algorithms/utils/*.h, algorithms/vamana/index.h) and
+// wraps them in a C ABI so that tests and the CPU baseline can run the
+// reference's beam search, robustPrune and Vamana build on in-memory data.
+// It is built by oracle/Makefile into oracle/_ref/libpann_ref.so, against the
+// project's own ParlayLib-API shim (oracle/parlay_shim), because ParlayLib is
+// not vendored with the reference. Nothing in the product links or loads it.
+//
+// Entry points (dtype 0=uint8, 1=int8, 2=float32; metric 0=Euclidian, 1=mips):
+//   ref_search       beam_search() per query          (beamSearch.h:420-427)
+//   ref_qsearch_time qsearchAll() timed as checkRecall (check_nn_recall.h:46-59)
+//   ref_robust_prune knn_index::robustPrune()          (index.h:63-120)
+//   ref_build        knn_index::build_index()          (index.h:150-186)
+//   ref_num_workers  threads used by parallel_for
+#include <cstdint>
+#include <cstring>
+#include <chrono>
+
+#include "utils/euclidian_point.h"
+#include "utils/mips_point.h"
+#include "utils/point_range.h"
+#include "utils/graph.h"
+#include "utils/beamSearch.h"
+#include "utils/stats.h"
+#include "vamana/index.h"
+
+using namespace parlayANN;
+
+namespace {
+
+template <typename T>
+struct MemRow {
+  const T* p;
+  T operator[](long j) const { return p[j]; }
+};
+template <typename T>
+struct MemRows {
+  const T* base; size_t n; size_t d;
+  size_t size() const { return n; }
+  long dimension() const { return (long)d; }
+  MemRow<T> operator[](long i) const { return MemRow<T>{base + (size_t)i * d}; }
+};
+
+template <typename Point>
+PointRange<Point> make_points(const void* data, size_t n, size_t d) {
+  using T = typename Point::T;
+  MemRows<T> rows{static_cast<const T*>(data), n, d};
+  typename Point::parameters params((int)d);
+  return PointRange<Point>(rows, params);
+}
+
+Graph<unsigned int> make_graph(const uint32_t* rows, size_t n, uint32_t R) {
+  Graph<unsigned int> G((long)R, n);
+  for (size_t i = 0; i < n; i++) {
+    const uint32_t* r = rows + i * (size_t)(R + 1);
+    uint32_t deg = r[0];
+    if (deg > R) deg = R;
+    auto s = parlay::make_slice(const_cast<uint32_t*>(r + 1), const_cast<uint32_t*>(r + 1 + deg));
+    G[(unsigned)i].update_neighbors(s);
+  }
+  return G;
+}
+
+void export_graph(const Graph<unsigned int>& G, uint32_t* out, uint32_t R) {
+  for (size_t i = 0; i < G.size(); i++) {
+    uint32_t* r = out + i * (size_t)(R + 1);
+    auto e = G[(unsigned)i];
+    r[0] = (uint32_t)e.size();
+    for (size_t j = 0; j < R; j++) r[1 + j] = j < e.size() ? e[(unsigned)j] : 0u;
+  }
+}
+
+template <typename Point>
+int search_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries,
+             uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit,
+             uint32_t degree_limit, double batch_factor, uint32_t n_start, const uint32_t* starts,
+             uint32_t* out_ids, float* out_dists, uint32_t* out_visited, uint32_t* out_cmps,
+             uint32_t* out_frontier_n, uint32_t* out_frontier_ids, float* out_frontier_d,
+             uint32_t visited_cap, uint32_t* out_visited_ids, float* out_visited_d) {
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto G = make_graph(graph, n, R);
+  QueryParams QP((long)k, (long)L, (long)limit, (long)degree_limit, 100.0, batch_factor);
+  parlay::sequence<unsigned int> sp(starts, starts + n_start);
+  int bad = 0;
+  parlay::parallel_for(0, (long)nq, [&](long i) {
+    auto [pairElts, cmps] = beam_search(Q[i], G, B, sp, QP);
+    auto& fr = pairElts.first;
+    auto& vis = pairElts.second;
+    if (fr.size() < k) { __atomic_store_n(&bad, 1, __ATOMIC_RELAXED); }
+    for (uint32_t j = 0; j < k; j++) {
+      out_ids[(size_t)i * k + j] = j < fr.size() ? fr[j].first : 0xFFFFFFFFu;
+      out_dists[(size_t)i * k + j] = j < fr.size() ? fr[j].second : 0.0f;
+    }
+    out_visited[i] = (uint32_t)vis.size();
+    out_cmps[i] = (uint32_t)cmps;
+    if (out_frontier_n) {
+      out_frontier_n[i] = (uint32_t)fr.size();
+      for (size_t j = 0; j < fr.size() && j < L; j++) {
+        out_frontier_ids[(size_t)i * L + j] = fr[j].first;
+        out_frontier_d[(size_t)i * L + j] = fr[j].second;
+      }
+    }
+    if (out_visited_ids) {
+      for (size_t j = 0; j < vis.size() && j < visited_cap; j++) {
+        out_visited_ids[(size_t)i * visited_cap + j] = vis[j].first;
+        out_visited_d[(size_t)i * visited_cap + j] = vis[j].second;
+      }
+    }
+  });
+  return bad ? 1 : 0;
+}
+
+template <typename Point>
+double qsearch_time_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries,
+                      uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L,
+                      double batch_factor, uint32_t* out_ids, uint32_t* out_visited,
+                      uint32_t* out_cmps) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto G = make_graph(graph, n, R);
+  QueryParams QP((long)k, (long)L, (long)n, (long)R, 10.0, batch_factor);
+  stats<unsigned int> QueryStats(nq);
+  QueryStats.clear();
+  // cache flush then a timer around qsearchAll only, as checkRecall does
+  auto volatile xx = parlay::random_permutation<long>(5000000);
+  (void)xx;
+  auto t0 = std::chrono::steady_clock::now();
+  auto all = qsearchAll<PR, PR, PR, unsigned int>(Q, Q, Q, G, B, B, B, QueryStats, 0u, QP);
+  auto t1 = std::chrono::steady_clock::now();
+  for (uint32_t i = 0; i < nq; i++) {
+    for (uint32_t j = 0; j < k; j++) out_ids[(size_t)i * k + j] = all[i][j];
+    out_visited[i] = QueryStats.visited[i];
+    out_cmps[i] = QueryStats.distances[i];
+  }
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+template <typename Point>
+int prune_t(uint32_t n, uint32_t d, const void* base, uint32_t R, const uint32_t* graph,
+            uint32_t p, uint32_t n_cand, const uint32_t* cand_ids, const float* cand_d,
+            double alpha, int add, uint32_t* out_nbrs, uint32_t* out_n, long* out_cmps) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  auto G = make_graph(graph, n, R);
+  BuildParams BP((long)R, 64, alpha, 1);
+  knn_index<PR, PR, unsigned int> I(BP);
+  parlay::sequence<std::pair<unsigned int, float>> cand;
+  for (uint32_t i = 0; i < n_cand; i++) cand.push_back(std::make_pair(cand_ids[i], cand_d[i]));
+  auto [nb, dc] = I.robustPrune(p, cand, G, B, alpha, add != 0);
+  *out_n = (uint32_t)nb.size();
+  for (size_t i = 0; i < nb.size(); i++) out_nbrs[i] = nb[i];
+  *out_cmps = dc;
+  return 0;
+}
+
+template <typename Point>
+int build_t(uint32_t n, uint32_t d, const void* base, uint32_t R, uint32_t L, double alpha,
+            int passes, double batch_factor, uint32_t* out_graph, double* seconds,
+            uint64_t* out_dist_total, uint32_t* out_visited) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  BuildParams BP((long)R, (long)L, alpha, passes, 0, 0, 0, 0.0, false, 0, false, 0, 0, 0.0,
+                 10.0, batch_factor);
+  Graph<unsigned int> G((long)R, n);
+  knn_index<PR, PR, unsigned int> I(BP);
+  stats<unsigned int> BuildStats(G.size());
+  auto t0 = std::chrono::steady_clock::now();
+  I.build_index(G, B, B, BuildStats);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  export_graph(G, out_graph, R);
+  if (out_dist_total) {
+    uint64_t s = 0;
+    for (size_t i = 0; i < n; i++) s += BuildStats.distances[i];
+    *out_dist_total = s;
+  }
+  if (out_visited) for (size_t i = 0; i < n; i++) out_visited[i] = BuildStats.visited[i];
+  return 0;
+}
+
+}  // namespace
+
+#define DISPATCH(dtype, metric, FN, ...)                                                  \
+  do {                                                                                    \
+    if (metric == 0) {                                                                    \
+      if (dtype == 0) return FN<Euclidian_Point<uint8_t>>(__VA_ARGS__);                   \
+      if (dtype == 1) return FN<Euclidian_Point<int8_t>>(__VA_ARGS__);                    \
+      if (dtype == 2) return FN<Euclidian_Point<float>>(__VA_ARGS__);                     \
+    } else {                                                                              \
+      if (dtype == 0) return FN<Mips_Point<uint8_t>>(__VA_ARGS__);                        \
+      if (dtype == 1) return FN<Mips_Point<int8_t>>(__VA_ARGS__);                         \
+      if (dtype == 2) return FN<Mips_Point<float>>(__VA_ARGS__);                          \
+    }                                                                                     \
+  } while (0)
+
+extern "C" {
+
+int ref_num_workers(void) { return (int)parlay::num_workers(); }
+
+int ref_search(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+               const void* queries, uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L,
+               uint64_t limit, uint32_t degree_limit, double batch_factor, uint32_t n_start,
+               const uint32_t* starts, uint32_t* out_ids, float* out_dists, uint32_t* out_visited,
+               uint32_t* out_cmps, uint32_t* out_frontier_n, uint32_t* out_frontier_ids,
+               float* out_frontier_d, uint32_t visited_cap, uint32_t* out_visited_ids,
+               float* out_visited_d) {
+  DISPATCH(dtype, metric, search_t, n, d, base, nq, queries, R, graph, k, L, limit, degree_limit,
+           batch_factor, n_start, starts, out_ids, out_dists, out_visited, out_cmps,
+           out_frontier_n, out_frontier_ids, out_frontier_d, visited_cap, out_visited_ids,
+           out_visited_d);
+  return -1;
+}
+
+double ref_qsearch_time(int dtype, int metric, uint32_t n, uint32_t d, const void* base,
+                        uint32_t nq, const void* queries, uint32_t R, const uint32_t* graph,
+                        uint32_t k, uint32_t L, double batch_factor, uint32_t* out_ids,
+                        uint32_t* out_visited, uint32_t* out_cmps) {
+  DISPATCH(dtype, metric, qsearch_time_t, n, d, base, nq, queries, R, graph, k, L, batch_factor,
+           out_ids, out_visited, out_cmps);
+  return -1.0;
+}
+
+int ref_robust_prune(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t R,
+                     const uint32_t* graph, uint32_t p, uint32_t n_cand, const uint32_t* cand_ids,
+                     const float* cand_d, double alpha, int add, uint32_t* out_nbrs,
+                     uint32_t* out_n, long* out_cmps) {
+  DISPATCH(dtype, metric, prune_t, n, d, base, R, graph, p, n_cand, cand_ids, cand_d, alpha, add,
+           out_nbrs, out_n, out_cmps);
+  return -1;
+}
+
+int ref_build(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t R,
+              uint32_t L, double alpha, int passes, double batch_factor, uint32_t* out_graph,
+              double* seconds, uint64_t* out_dist_total, uint32_t* out_visited) {
+  DISPATCH(dtype, metric, build_t, n, d, base, R, L, alpha, passes, batch_factor, out_graph,
+           seconds, out_dist_total, out_visited);
+  return -1;
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+"""parlayann_b200: B200 (sm_100a) beam search and Vamana build behind
+ParlayANN's interfaces.
+
+The product is the C ABI in ``include/parlayann_b200.h``, implemented by
+``parlayann_b200/libparlayann_b200.so`` (CUDA kernels + host orchestration).
+This module is a thin ctypes binding of that ABI, shaped like the reference's
+Python surface (``GraphIndex.batch_search``, ``build_vamana_index``;
+python/graph_index.cpp:192-216, python/builder.cpp:36-99) and its C++ types
+(``QueryParams`` / ``BuildParams``, algorithms/utils/types.h:155-268).
+
+There is no CPU fallback: if the shared library is missing, importing the
+binding raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libparlayann_b200.so")
+
+PANN_OK, PANN_EINVAL, PANN_ENOMEM, PANN_ETIMEOUT, PANN_EDEVICE, PANN_EOVERFLOW, PANN_ESHORT = range(7)
+U8, I8, F32 = 0, 1, 2
+L2, MIPS = 0, 1
+_DTYPES = {np.dtype(np.uint8): U8, np.dtype(np.int8): I8, np.dtype(np.float32): F32}
+_NP_OF = {U8: np.uint8, I8: np.int8, F32: np.float32}
+
+
+class PannError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"parlayann_b200 error {code}: {msg}")
+        self.code = code
+
+
+class QueryParams(ctypes.Structure):
+    """QueryParams (types.h:233-252): k, beamSize, limit, degree_limit, batch_factor."""
+
+    _fields_ = [
+        ("k", ctypes.c_uint32),
+        ("beam", ctypes.c_uint32),
+        ("limit", ctypes.c_uint64),
+        ("degree_limit", ctypes.c_uint32),
+        ("batch_factor", ctypes.c_double),
+    ]
+
+
+class BuildParams(ctypes.Structure):
+    """BuildParams fields of the Vamana build (types.h:155-230)."""
+
+    _fields_ = [
+        ("R", ctypes.c_uint32),
+        ("L", ctypes.c_uint32),
+        ("alpha", ctypes.c_double),
+        ("num_passes", ctypes.c_int32),
+        ("batch_factor", ctypes.c_double),
+        ("perm_seed", ctypes.c_uint64),
+        ("sort_neighbors", ctypes.c_int32),
+    ]
+
+
+class BuildStats(ctypes.Structure):
+    _fields_ = [
+        ("seconds", ctypes.c_double),
+        ("search_seconds", ctypes.c_double),
+        ("prune_seconds", ctypes.c_double),
+        ("reverse_seconds", ctypes.c_double),
+        ("dist_cmps", ctypes.c_uint64),
+        ("visited_total", ctypes.c_uint64),
+        ("batches", ctypes.c_uint32),
+        ("flagged", ctypes.c_uint32),
+    ]
+
+
+# Every symbol include/parlayann_b200.h declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_U32, _U64, _I = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+SIGNATURES = {
+    "pann_index_create": (_I, [ctypes.POINTER(_P), _I, _I, _U64, _U32, _U32]),
+    "pann_index_destroy": (_I, [_P]),
+    "pann_index_set_points": (_I, [_P, _P, _I]),
+    "pann_graph_upload": (_I, [_P, _P, _I]),
+    "pann_graph_download": (_I, [_P, _P]),
+    "pann_graph_load": (_I, [_P, ctypes.c_char_p]),
+    "pann_graph_save": (_I, [_P, ctypes.c_char_p]),
+    "pann_search": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P]),
+    "pann_search_device": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P, _P]),
+    "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
+    "pann_groundtruth": (_I, [_P, _P, _U32, _U32, _P, _P]),
+    "pann_last_error": (ctypes.c_char_p, []),
+    "pann_synth_mixture": (_I, [_I, _U64, _U32, _U32, _U64, _U32, ctypes.c_double, ctypes.c_double,
+                                ctypes.c_double, _I, _P]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libparlayann_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run python -c 'import __graft_entry__ as g; g.build()'")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != PANN_OK:
+        raise PannError(rc, lib().pann_last_error().decode())
+
+
+def _ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays must be C-contiguous"
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def synth_mixture(dtype: int, n: int, d: int, components: int, seed: int, stream: int,
+                  lo: float = 32.0, hi: float = 224.0, sigma: float = 20.0, normalize: bool = False) -> np.ndarray:
+    """Seeded Gaussian-mixture rows (see pann_synth_mixture)."""
+    out = np.empty((n, d), dtype=_NP_OF[dtype])
+    _check(lib().pann_synth_mixture(dtype, n, d, components, seed, stream, lo, hi, sigma, int(normalize), _ptr(out)))
+    return out
+
+
+def batch_schedule(n: int, m: int | None = None, base: float = 2.0, max_fraction: float = 0.02):
+    """Prefix-doubling batch bounds of batch_insert (algorithms/vamana/index.h:206-240)."""
+    m = n if m is None else m
+    max_batch = min(int(max_fraction * float(np.float32(n))), 1000000)
+    if max_batch == 0:
+        max_batch = n
+    out, count, inc = [], 0, 0
+    while count < m:
+        if base ** inc <= max_batch:
+            f = int(base ** inc) - 1
+            c = min(int(base ** (inc + 1)) - 1, m)
+            count = c
+        else:
+            f = count
+            c = min(count + max_batch, m)
+            count += max_batch
+        out.append((f, c))
+        inc += 1
+    return out
+
+
+def permutation(n: int, seed: int = 0x5EED5EED5EED) -> np.ndarray:
+    """Insertion order used when no permutation is given: indices ordered by splitmix64(seed + i)."""
+    x = (np.arange(n, dtype=np.uint64) + np.uint64(seed)).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+    return np.argsort(x, kind="stable").astype(np.uint32)
+
+
+@dataclass
+class SearchResult:
+    ids: np.ndarray
+    dists: np.ndarray
+    visited: np.ndarray
+    cmps: np.ndarray
+    flags: np.ndarray
+
+
+class Index:
+    """Device-resident PointRange + Graph (point_range.h, graph.h) on one GPU."""
+
+    def __init__(self, points: np.ndarray, R: int, metric: int = L2):
+        points = np.ascontiguousarray(points)
+        self.dtype = _DTYPES[points.dtype]
+        self.n, self.d = points.shape
+        self.R = R
+        self.metric = metric
+        h = ctypes.c_void_p()
+        _check(lib().pann_index_create(ctypes.byref(h), self.dtype, metric, self.n, self.d, R))
+        self._h = h
+        _check(lib().pann_index_set_points(self._h, _ptr(points), 0))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pann_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # graph in the reference layout: n x (R+1), slot 0 = degree
+    def set_graph(self, rows: np.ndarray):
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        assert rows.shape == (self.n, self.R + 1)
+        _check(lib().pann_graph_upload(self._h, _ptr(rows), 0))
+
+    def get_graph(self) -> np.ndarray:
+        out = np.empty((self.n, self.R + 1), dtype=np.uint32)
+        _check(lib().pann_graph_download(self._h, _ptr(out)))
+        return out
+
+    def save_graph(self, path: str):
+        _check(lib().pann_graph_save(self._h, path.encode()))
+
+    def load_graph(self, path: str):
+        _check(lib().pann_graph_load(self._h, path.encode()))
+
+    def build(self, L: int, alpha: float, num_passes: int = 1, batch_factor: float = 0.125,
+              perm: np.ndarray | None = None, perm_seed: int = 0x5EED5EED5EED, sort_neighbors: bool = True) -> BuildStats:
+        bp = BuildParams(self.R, L, alpha, num_passes, batch_factor, perm_seed, int(sort_neighbors))
+        st = BuildStats()
+        p = None if perm is None else np.ascontiguousarray(perm, dtype=np.uint32)
+        _check(lib().pann_build(self._h, ctypes.byref(bp), _ptr(p), ctypes.byref(st)))
+        return st
+
+    def search(self, queries: np.ndarray, k: int, L: int, limit: int | None = None, degree_limit: int | None = None,
+               batch_factor: float = 0.125, starts=(0,), allow_short: bool = False) -> SearchResult:
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        nq = queries.shape[0]
+        qp = QueryParams(k, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
+                         batch_factor)
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+        ids = np.empty((nq, k), np.uint32)
+        dists = np.empty((nq, k), np.float32)
+        vis = np.empty(nq, np.uint32)
+        cmps = np.empty(nq, np.uint32)
+        flags = np.empty(nq, np.uint32)
+        rc = lib().pann_search(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(ids),
+                               _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags))
+        if not (allow_short and rc == PANN_ESHORT):
+            _check(rc)
+        return SearchResult(ids, dists, vis, cmps, flags)
+
+    def groundtruth(self, queries: np.ndarray, k: int):
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        ids = np.empty((queries.shape[0], k), np.uint32)
+        dd = np.empty((queries.shape[0], k), np.float64)
+        _check(lib().pann_groundtruth(self._h, _ptr(queries), queries.shape[0], k, _ptr(ids), _ptr(dd)))
+        return ids, dd
+
+
+def recall_at_k(ids: np.ndarray, gt_ids: np.ndarray, k: int) -> float:
+    """recall@k = |result[:k] ∩ gt[:k]| / k averaged over queries (check_nn_recall.h:86-112,
+    without the tie extension; see recall_with_ties)."""
+    hit = 0
+    for a, b in zip(ids[:, :k], gt_ids[:, :k]):
+        hit += len(set(a.tolist()) & set(b.tolist()))
+    return hit / float(k * ids.shape[0])
+
+
+def recall_with_ties(ids: np.ndarray, gt_ids: np.ndarray, gt_d: np.ndarray, k: int) -> float:
+    """checkRecall's recall (check_nn_recall.h:86-112): the groundtruth set is the first k ids plus
+    every later groundtruth id tied with the k-th distance."""
+    hit = 0
+    for i in range(ids.shape[0]):
+        last = gt_d[i, k - 1]
+        extra = [int(x) for x, dd in zip(gt_ids[i, k:], gt_d[i, k:]) if dd == last]
+        truth = [int(x) for x in gt_ids[i, :k]] + extra
+        rep = set(ids[i, :k].tolist())
+        hit += sum(1 for t in truth if t in rep)
+    return hit / float(k * ids.shape[0])

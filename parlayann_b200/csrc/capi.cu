@@ -1,0 +1,556 @@
+// C ABI: index lifetime, data upload, graph formats, and the search entry
+// points (include/parlayann_b200.h).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "index.cuh"
+#include "search.cuh"
+
+namespace pann {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  g_last_error = m;
+  return e == cudaErrorMemoryAllocation ? PANN_ENOMEM : PANN_EDEVICE;
+}
+
+// ------------------------------------------------------------ graph layout kernels
+// reference rows (deg, e0..e_{R-1}) -> flat rows (e0..e_{deg-1}, PAD...)
+__global__ void graph_from_ref_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t rows,
+                                      uint32_t R, uint64_t n_total, uint32_t* bad) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t total = rows * R;
+  for (; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t r = t / R;
+    uint32_t j = (uint32_t)(t - r * R);
+    const uint32_t* src = in + r * (R + 1);
+    uint32_t deg = src[0];
+    if (deg > R) { atomicOr(bad, 1u); deg = R; }
+    uint32_t v = PANN_PAD;
+    if (j < deg) {
+      v = src[1 + j];
+      if ((uint64_t)v >= n_total) { atomicOr(bad, 2u); v = PANN_PAD; }
+    }
+    out[t] = v;
+  }
+}
+// flat rows -> reference rows
+__global__ void graph_to_ref_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint64_t rows,
+                                    uint32_t R) {
+  uint64_t r = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  for (; r < rows; r += (uint64_t)gridDim.x * (blockDim.x / 32)) {
+    const uint32_t* src = in + r * R;
+    uint32_t deg = 0;
+    for (uint32_t b = 0; b < R; b += 32) {
+      uint32_t j = b + lane;
+      uint32_t v = j < R ? src[j] : PANN_PAD;
+      deg += __popc(__ballot_sync(0xFFFFFFFFu, v != PANN_PAD));
+      if (j < R) out[r * (R + 1) + 1 + j] = (v != PANN_PAD) ? v : 0u;
+    }
+    if (lane == 0) out[r * (R + 1)] = deg;
+  }
+}
+
+int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan) {
+  if (!qp) return fail(PANN_EINVAL, "query params are NULL");
+  if (qp->beam == 0) return fail(PANN_EINVAL, "beam (L) must be positive");
+  if (qp->k > qp->beam)
+    return fail(PANN_EINVAL, "beam search parameter Q = " + std::to_string(qp->beam) +
+                                 " same size or smaller than k = " + std::to_string(qp->k));
+  if (qp->degree_limit == 0) return fail(PANN_EINVAL, "degree_limit must be positive");
+  if (n_start == 0) return fail(PANN_EINVAL, "beam search expects at least one start point");
+  if (n_start > qp->beam) return fail(PANN_EINVAL, "beam search has more starting points than beam size");
+  if (!(qp->batch_factor >= 0.0) || qp->batch_factor > 64.0) return fail(PANN_EINVAL, "batch_factor out of range");
+  if (qp->beam > 4096) return fail(PANN_EINVAL, "beam (L) above 4096 is not supported");
+  plan->k = qp->k;
+  plan->L = qp->beam;
+  plan->dl = qp->degree_limit;
+  plan->limit = qp->limit;
+  plan->bf = qp->batch_factor;
+  plan->n_start = n_start;
+  // hashset<indexType> has_been_seen(2 * (10 + beamSize) * max_degree) (beamSearch.h:66):
+  // capacity 2^ceil(log2(n)) (hashset.h:50-54); it grows above capacity/2 entries.
+  double cap_n = 2.0 * (10.0 + (double)qp->beam) * (double)qp->degree_limit;
+  int bits = (int)std::ceil(std::log2(cap_n));
+  uint64_t cap = 1ull << bits;
+  plan->ref_half = (uint32_t)std::min<uint64_t>(cap / 2, 0xFFFFFFFFull);
+  uint32_t nel = std::min(qp->degree_limit, idx->R);
+  uint64_t defer = (uint64_t)std::floor(qp->batch_factor * (double)qp->beam);
+  if (qp->limit < 2ull * qp->beam) defer = 0;  // no deferral: candidates are merged every step
+  plan->Ccap = (uint32_t)(defer + nel + 1);
+  return PANN_OK;
+}
+
+static uint32_t pow2_at_least(uint64_t x) {
+  uint32_t p = 1;
+  while (p < x && p < (1u << 30)) p <<= 1;
+  return p;
+}
+
+template <int DT, int MT, bool G>
+static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
+  auto k = search_kernel<DT, MT, G>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<blocks, threads, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
+                                 int threads, size_t smem, cudaStream_t st) {
+#define PANN_SEARCH_CASE(DT, MT)                                                        \
+  if (dtype == DT && metric == MT)                                                      \
+    return global_table ? launch_search_t<DT, MT, true>(a, blocks, threads, smem, st)   \
+                        : launch_search_t<DT, MT, false>(a, blocks, threads, smem, st);
+  PANN_SEARCH_CASE(DT_U8, MT_L2)
+  PANN_SEARCH_CASE(DT_U8, MT_IP)
+  PANN_SEARCH_CASE(DT_I8, MT_L2)
+  PANN_SEARCH_CASE(DT_I8, MT_IP)
+  PANN_SEARCH_CASE(DT_F32, MT_L2)
+  PANN_SEARCH_CASE(DT_F32, MT_IP)
+#undef PANN_SEARCH_CASE
+  return cudaErrorInvalidValue;
+}
+
+template <int DT, int MT, bool G>
+static int occupancy_t(int threads, size_t smem) {
+  int nb = 0;
+  auto k = search_kernel<DT, MT, G>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
+  return nb;
+}
+static int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem) {
+#define PANN_OCC_CASE(DT, MT) \
+  if (dtype == DT && metric == MT) return g ? occupancy_t<DT, MT, true>(threads, smem) : occupancy_t<DT, MT, false>(threads, smem);
+  PANN_OCC_CASE(DT_U8, MT_L2)
+  PANN_OCC_CASE(DT_U8, MT_IP)
+  PANN_OCC_CASE(DT_I8, MT_L2)
+  PANN_OCC_CASE(DT_I8, MT_IP)
+  PANN_OCC_CASE(DT_F32, MT_L2)
+  PANN_OCC_CASE(DT_F32, MT_IP)
+#undef PANN_OCC_CASE
+  return 0;
+}
+
+// Seen-table size of the first tier: the PANN_SEEN_SLOTS environment variable,
+// else about twice the distinct ids a search touches (visits x new neighbours).
+static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
+  if (const char* e = std::getenv("PANN_SEEN_SLOTS")) {
+    long v = std::atol(e);
+    if (v > 0) return std::max<uint32_t>(pow2_at_least((uint64_t)v), pow2_at_least(4ull * (R + 1)));
+  }
+  uint32_t nel = std::min(p.dl, R);
+  uint64_t est = (uint64_t)(p.L + 24) * nel;
+  uint32_t s = pow2_at_least(est);
+  s = std::min<uint32_t>(s, 8192);
+  s = std::max<uint32_t>(s, pow2_at_least(4ull * (R + 1)));
+  return s;
+}
+
+// Three tiers: (0) many warps per SM with a modest shared-memory seen table;
+// (1) queries whose table filled up, one warp per block with the largest
+// shared-memory table; (2) the rest with a table in global memory.
+int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
+               uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
+               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st) {
+  if (nq == 0) return PANN_OK;
+  // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1
+  PANN_CUDA(idx->counters.ensure(64));
+  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 2 * (size_t)nq));
+  uint32_t* cnt = idx->counters.as<uint32_t>();
+  uint32_t* redo0 = idx->redo.as<uint32_t>();
+  uint32_t* redo1 = redo0 + nq;
+  PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
+
+  SearchArgs a{};
+  a.points = idx->d_points;
+  a.stride = idx->stride;
+  a.d = idx->d;
+  a.nchunks = idx->nchunks;
+  a.graph = idx->d_graph;
+  a.R = idx->R;
+  a.queries = d_queries;
+  a.self_ids = d_self_ids;
+  a.nq = nq;
+  a.k = plan.k;
+  a.L = plan.L;
+  a.dl = plan.dl;
+  a.limit = plan.limit;
+  a.batch_factor = plan.bf;
+  a.ref_half = plan.ref_half;
+  a.starts = d_starts;
+  a.n_start = plan.n_start;
+  a.Ccap = plan.Ccap;
+  a.out_ids = d_ids;
+  a.out_dists = d_dists;
+  a.out_visited = d_vis;
+  a.out_cmps = d_cmps;
+  a.out_status = d_status;
+  a.vis_keys = d_vis_keys;
+  a.vis_cap = vis_cap;
+
+  const size_t smem_cap = idx->smem_optin;
+  // ---- tier 0
+  {
+    uint32_t S = tier0_slots(plan, idx->R);
+    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
+    int wpb = 4;
+    while (wpb > 1 && (size_t)wb * wpb > smem_cap) wpb >>= 1;
+    if ((size_t)wb * wpb > smem_cap) {
+      S = 0;  // cannot fit: everything goes to the next tiers
+    }
+    if (S) {
+      SearchArgs t = a;
+      t.S = S;
+      t.warp_bytes = wb;
+      t.job_counter = cnt + 0;
+      t.redo_list = redo0;
+      t.redo_count = cnt + 3;
+      int occ = search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb);
+      if (occ <= 0) occ = 1;
+      uint64_t want = (nq + wpb - 1) / wpb;
+      int blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
+      PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st));
+    } else {
+      // route every query to tier 1: job list = identity
+      std::vector<uint32_t> ident(nq);
+      for (uint32_t i = 0; i < nq; i++) ident[i] = i;
+      PANN_CUDA(cudaMemcpyAsync(redo0, ident.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
+      PANN_CUDA(cudaMemcpyAsync(cnt + 3, &nq, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      PANN_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  // ---- tier 1: one warp per block, largest shared table
+  {
+    uint32_t base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, false);
+    uint32_t S = 1u << 15;
+    while (S > 512 && base + 4ull * S > smem_cap) S >>= 1;
+    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
+    if ((size_t)wb <= smem_cap) {
+      SearchArgs t = a;
+      t.S = S;
+      t.warp_bytes = wb;
+      t.job_list = redo0;
+      t.njobs_dev = cnt + 3;
+      t.job_counter = cnt + 1;
+      t.redo_list = redo1;
+      t.redo_count = cnt + 4;
+      int occ = search_occupancy(idx->dtype, idx->metric, false, 32, wb);
+      if (occ <= 0) occ = 1;
+      int blocks = std::max(1, occ * idx->sm_count);
+      PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32, wb, st));
+    } else {
+      return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
+    }
+  }
+  // ---- tier 2: global-memory seen table, sized above the reference's own capacity
+  {
+    uint32_t S = std::max<uint32_t>(1u << 16, pow2_at_least(4ull * plan.ref_half));
+    S = std::min<uint32_t>(S, 1u << 24);
+    int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * idx->sm_count, (256ull << 20) / (4ull * S)));
+    PANN_CUDA(idx->gtables.ensure((size_t)slots * S * 4));
+    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, true);
+    SearchArgs t = a;
+    t.S = S;
+    t.warp_bytes = wb;
+    t.gtables = idx->gtables.as<uint32_t>();
+    t.job_list = redo1;
+    t.njobs_dev = cnt + 4;
+    t.job_counter = cnt + 2;
+    t.redo_list = nullptr;
+    t.redo_count = nullptr;
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, slots, 32, wb, st));
+  }
+  return PANN_OK;
+}
+
+static int check_index(const pann_index* idx, bool need_graph) {
+  if (!idx) return fail(PANN_EINVAL, "index is NULL");
+  if (!idx->points_set) return fail(PANN_EINVAL, "index has no points (pann_index_set_points)");
+  (void)need_graph;
+  return PANN_OK;
+}
+
+static int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st) {
+  if (!starts) return fail(PANN_EINVAL, "start points are NULL");
+  for (uint32_t i = 0; i < n_start; i++) {
+    if ((uint64_t)starts[i] >= idx->n) return fail(PANN_EINVAL, "start point id out of range");
+    for (uint32_t j = 0; j < i; j++)
+      if (starts[j] == starts[i]) return fail(PANN_EINVAL, "duplicate start point");
+  }
+  bool same = n_start == idx->starts_cached_n && n_start <= 64 &&
+              std::memcmp(starts, idx->starts_cached, sizeof(uint32_t) * n_start) == 0;
+  if (same) return PANN_OK;
+  PANN_CUDA(idx->starts.ensure(sizeof(uint32_t) * std::max<uint32_t>(n_start, 16)));
+  PANN_CUDA(cudaMemcpyAsync(idx->starts.p, starts, sizeof(uint32_t) * n_start, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaStreamSynchronize(st));  // starts may live on the caller's stack
+  if (n_start <= 64) {
+    std::memcpy(idx->starts_cached, starts, sizeof(uint32_t) * n_start);
+    idx->starts_cached_n = n_start;
+  } else {
+    idx->starts_cached_n = 0;
+  }
+  return PANN_OK;
+}
+
+// status bits -> caller flags: bit0 = reference hashset would grow
+static int summarize_status(const uint32_t* status, uint32_t nq, uint32_t* out_flags) {
+  int rc = PANN_OK;
+  for (uint32_t i = 0; i < nq; i++) {
+    uint32_t s = status[i];
+    if (out_flags) out_flags[i] = (s & QS_REF_WOULD_GROW) ? 1u : 0u;
+    if (s & (QS_TABLE_FULL | QS_INTERNAL)) rc = PANN_EOVERFLOW;
+    else if ((s & QS_SHORT) && rc == PANN_OK) rc = PANN_ESHORT;
+  }
+  if (rc == PANN_EOVERFLOW) set_error("a query's seen-set outgrew the largest table");
+  if (rc == PANN_ESHORT) set_error("beam search returned fewer than k results");
+  return rc;
+}
+
+}  // namespace pann
+
+using namespace pann;
+
+extern "C" {
+
+const char* pann_last_error(void) { return g_last_error.c_str(); }
+
+int pann_index_create(pann_index** out, int dtype, int metric, uint64_t n, uint32_t d, uint32_t R) {
+  if (!out) return fail(PANN_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (dtype < 0 || dtype > 2) return fail(PANN_EINVAL, "dtype must be PANN_U8, PANN_I8 or PANN_F32");
+  if (metric < 0 || metric > 1) return fail(PANN_EINVAL, "metric must be PANN_L2 or PANN_MIPS");
+  if (n == 0 || n >= 0x7FFFFFFFull) return fail(PANN_EINVAL, "n must be in [1, 2^31-1)");
+  if (d == 0 || d > 8192) return fail(PANN_EINVAL, "dimension must be in [1, 8192]");
+  if (R == 0 || R > 1024) return fail(PANN_EINVAL, "max degree R must be in [1, 1024]");
+  int dev = 0;
+  PANN_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  PANN_CUDA(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) return fail(PANN_EDEVICE, "this library is built for sm_100a (B200); device is sm_" +
+                                                     std::to_string(prop.major) + std::to_string(prop.minor));
+  pann_index* idx = new pann_index();
+  idx->dtype = dtype;
+  idx->metric = metric;
+  idx->n = n;
+  idx->d = d;
+  idx->R = R;
+  idx->esize = dtype == PANN_F32 ? 4 : 1;
+  idx->stride = ((uint64_t)d * idx->esize + 15) & ~15ull;
+  idx->nchunks = (uint32_t)(idx->stride / 16);
+  idx->device = dev;
+  idx->sm_count = prop.multiProcessorCount;
+  idx->smem_optin = prop.sharedMemPerBlockOptin;
+  cudaError_t e = cudaStreamCreateWithFlags(&idx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&idx->d_points, idx->stride * n);
+  if (e == cudaSuccess) e = cudaMalloc(&idx->d_graph, sizeof(uint32_t) * (size_t)R * n);
+  if (e == cudaSuccess) e = cudaMemset(idx->d_graph, 0xFF, sizeof(uint32_t) * (size_t)R * n);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(e, "index allocation");
+    pann_index_destroy(idx);
+    return rc;
+  }
+  *out = idx;
+  return PANN_OK;
+}
+
+int pann_index_destroy(pann_index* idx) {
+  if (!idx) return PANN_OK;
+  if (idx->stream) cudaStreamSynchronize(idx->stream);
+  if (idx->d_points) cudaFree(idx->d_points);
+  if (idx->d_graph) cudaFree(idx->d_graph);
+  for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
+                    &idx->counters, &idx->gtables, &idx->starts, &idx->tmp})
+    b->release();
+  if (idx->stream) cudaStreamDestroy(idx->stream);
+  delete idx;
+  return PANN_OK;
+}
+
+int pann_index_set_points(pann_index* idx, const void* vectors, int on_device) {
+  if (!idx || !vectors) return fail(PANN_EINVAL, "index or vectors is NULL");
+  size_t rb = (size_t)idx->d * idx->esize;
+  PANN_CUDA(cudaMemsetAsync(idx->d_points, 0, idx->stride * idx->n, idx->stream));
+  PANN_CUDA(cudaMemcpy2DAsync(idx->d_points, idx->stride, vectors, rb, rb, idx->n,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, idx->stream));
+  PANN_CUDA(cudaStreamSynchronize(idx->stream));
+  idx->points_set = true;
+  return PANN_OK;
+}
+
+int pann_graph_upload(pann_index* idx, const uint32_t* rows, int on_device) {
+  if (!idx || !rows) return fail(PANN_EINVAL, "index or rows is NULL");
+  const uint64_t R = idx->R, n = idx->n;
+  const uint64_t chunk = std::max<uint64_t>(1, (256ull << 20) / (4 * (R + 1)));
+  PANN_CUDA(idx->tmp.ensure(4 * (R + 1) * std::min(chunk, n) + 64));
+  uint32_t* bad = reinterpret_cast<uint32_t*>(idx->tmp.as<uint8_t>() + 4 * (R + 1) * std::min(chunk, n));
+  PANN_CUDA(cudaMemsetAsync(bad, 0, 4, idx->stream));
+  for (uint64_t r0 = 0; r0 < n; r0 += chunk) {
+    uint64_t rows_here = std::min(chunk, n - r0);
+    PANN_CUDA(cudaMemcpyAsync(idx->tmp.p, rows + r0 * (R + 1), 4 * (R + 1) * rows_here,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, idx->stream));
+    int blocks = (int)std::min<uint64_t>((rows_here * R + 255) / 256, 65535ull * 4);
+    graph_from_ref_kernel<<<blocks, 256, 0, idx->stream>>>(idx->tmp.as<uint32_t>(), idx->d_graph + r0 * R,
+                                                            rows_here, (uint32_t)R, n, bad);
+    PANN_CUDA(cudaGetLastError());
+  }
+  uint32_t hbad = 0;
+  PANN_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, idx->stream));
+  PANN_CUDA(cudaStreamSynchronize(idx->stream));
+  if (hbad & 1u) return fail(PANN_EINVAL, "graph row degree exceeds max degree");
+  if (hbad & 2u) return fail(PANN_EINVAL, "graph neighbour id out of range");
+  return PANN_OK;
+}
+
+int pann_graph_download(pann_index* idx, uint32_t* rows) {
+  if (!idx || !rows) return fail(PANN_EINVAL, "index or rows is NULL");
+  const uint64_t R = idx->R, n = idx->n;
+  const uint64_t chunk = std::max<uint64_t>(1, (256ull << 20) / (4 * (R + 1)));
+  PANN_CUDA(idx->tmp.ensure(4 * (R + 1) * std::min(chunk, n) + 64));
+  PANN_CUDA(cudaMemsetAsync(idx->tmp.p, 0, 4 * (R + 1) * std::min(chunk, n), idx->stream));
+  for (uint64_t r0 = 0; r0 < n; r0 += chunk) {
+    uint64_t rows_here = std::min(chunk, n - r0);
+    int blocks = (int)std::min<uint64_t>((rows_here + 7) / 8, 65535ull * 4);
+    graph_to_ref_kernel<<<blocks, 256, 0, idx->stream>>>(idx->d_graph + r0 * R, idx->tmp.as<uint32_t>(), rows_here,
+                                                          (uint32_t)R);
+    PANN_CUDA(cudaGetLastError());
+    PANN_CUDA(cudaMemcpyAsync(rows + r0 * (R + 1), idx->tmp.p, 4 * (R + 1) * rows_here, cudaMemcpyDeviceToHost,
+                              idx->stream));
+  }
+  PANN_CUDA(cudaStreamSynchronize(idx->stream));
+  return PANN_OK;
+}
+
+int pann_graph_save(pann_index* idx, const char* path) {
+  if (!idx || !path) return fail(PANN_EINVAL, "index or path is NULL");
+  const uint64_t R = idx->R, n = idx->n;
+  std::vector<uint32_t> rows((size_t)(n * (R + 1)));
+  int rc = pann_graph_download(idx, rows.data());
+  if (rc) return rc;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(PANN_EINVAL, std::string("cannot open graph file for writing: ") + path);
+  uint32_t pre[2] = {(uint32_t)n, (uint32_t)R};
+  bool ok = std::fwrite(pre, 4, 2, f) == 2;
+  std::vector<uint32_t> deg((size_t)n);
+  for (uint64_t i = 0; i < n; i++) deg[i] = rows[i * (R + 1)];
+  ok = ok && std::fwrite(deg.data(), 4, (size_t)n, f) == (size_t)n;
+  for (uint64_t i = 0; i < n && ok; i++)
+    if (deg[i]) ok = std::fwrite(&rows[i * (R + 1) + 1], 4, deg[i], f) == deg[i];
+  std::fclose(f);
+  if (!ok) return fail(PANN_EINVAL, std::string("short write to graph file: ") + path);
+  return PANN_OK;
+}
+
+int pann_graph_load(pann_index* idx, const char* path) {
+  if (!idx || !path) return fail(PANN_EINVAL, "index or path is NULL");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(PANN_EINVAL, std::string("graph file ") + path + " not found");
+  uint32_t pre[2];
+  if (std::fread(pre, 4, 2, f) != 2) { std::fclose(f); return fail(PANN_EINVAL, "graph file too short"); }
+  const uint64_t n = pre[0], R = pre[1];
+  if (n != idx->n || R > idx->R) {
+    std::fclose(f);
+    return fail(PANN_EINVAL, "graph file has n=" + std::to_string(n) + ", maxDeg=" + std::to_string(R) +
+                                 " but the index has n=" + std::to_string(idx->n) + ", R=" + std::to_string(idx->R));
+  }
+  const uint64_t RI = idx->R;
+  std::vector<uint32_t> deg((size_t)n);
+  if (std::fread(deg.data(), 4, (size_t)n, f) != (size_t)n) { std::fclose(f); return fail(PANN_EINVAL, "graph file truncated"); }
+  std::vector<uint32_t> rows((size_t)(n * (RI + 1)), 0);
+  for (uint64_t i = 0; i < n; i++) {
+    if (deg[i] > R) { std::fclose(f); return fail(PANN_EINVAL, "graph file degree exceeds maxDeg"); }
+    rows[i * (RI + 1)] = deg[i];
+    if (deg[i] && std::fread(&rows[i * (RI + 1) + 1], 4, deg[i], f) != deg[i]) {
+      std::fclose(f);
+      return fail(PANN_EINVAL, "graph file truncated");
+    }
+  }
+  std::fclose(f);
+  return pann_graph_upload(idx, rows.data(), 0);
+}
+
+int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
+                       const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
+                       uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream) {
+  int rc = check_index(idx, true);
+  if (rc) return rc;
+  if (nq && (!d_queries || !d_out_ids)) return fail(PANN_EINVAL, "queries or out_ids is NULL");
+  SearchPlan plan;
+  rc = make_plan(idx, qp, n_start, &plan);
+  if (rc) return rc;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : idx->stream;
+  rc = stage_starts(idx, starts, n_start, st);
+  if (rc) return rc;
+  const uint8_t* q = static_cast<const uint8_t*>(d_queries);
+  size_t rb = (size_t)idx->d * idx->esize;
+  if (rb != idx->stride) {
+    PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
+    PANN_CUDA(cudaMemsetAsync(idx->q.p, 0, idx->stride * (size_t)nq, st));
+    PANN_CUDA(cudaMemcpy2DAsync(idx->q.p, idx->stride, d_queries, rb, rb, nq, cudaMemcpyDeviceToDevice, st));
+    q = idx->q.as<uint8_t>();
+  }
+  uint32_t* status = d_out_flags;
+  if (!status) {
+    PANN_CUDA(idx->status.ensure(sizeof(uint32_t) * (size_t)std::max<uint32_t>(nq, 1)));
+    status = idx->status.as<uint32_t>();
+  }
+  return run_search(idx, plan, q, nullptr, nq, idx->starts.as<uint32_t>(), d_out_ids, d_out_dists, d_out_visited,
+                    d_out_cmps, status, nullptr, 0, st);
+}
+
+int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                const uint32_t* starts, uint32_t n_start, uint32_t* out_ids, float* out_dists,
+                uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags) {
+  int rc = check_index(idx, true);
+  if (rc) return rc;
+  if (nq && (!queries || !out_ids)) return fail(PANN_EINVAL, "queries or out_ids is NULL");
+  SearchPlan plan;
+  rc = make_plan(idx, qp, n_start, &plan);
+  if (rc) return rc;
+  if (nq == 0) return PANN_OK;
+  cudaStream_t st = idx->stream;
+  rc = stage_starts(idx, starts, n_start, st);
+  if (rc) return rc;
+  const size_t k = plan.k;
+  size_t rb = (size_t)idx->d * idx->esize;
+  PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
+  PANN_CUDA(idx->ids.ensure(4 * std::max<size_t>(1, k * nq)));
+  PANN_CUDA(idx->dists.ensure(4 * std::max<size_t>(1, k * nq)));
+  PANN_CUDA(idx->vis.ensure(4 * (size_t)nq));
+  PANN_CUDA(idx->cmps.ensure(4 * (size_t)nq));
+  PANN_CUDA(idx->status.ensure(4 * (size_t)nq));
+  if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(idx->q.p, 0, idx->stride * (size_t)nq, st));
+  PANN_CUDA(cudaMemcpy2DAsync(idx->q.p, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
+  rc = run_search(idx, plan, idx->q.as<uint8_t>(), nullptr, nq, idx->starts.as<uint32_t>(), idx->ids.as<uint32_t>(),
+                  idx->dists.as<float>(), idx->vis.as<uint32_t>(), idx->cmps.as<uint32_t>(),
+                  idx->status.as<uint32_t>(), nullptr, 0, st);
+  if (rc) return rc;
+  if (k) {
+    PANN_CUDA(cudaMemcpyAsync(out_ids, idx->ids.p, 4 * k * nq, cudaMemcpyDeviceToHost, st));
+    if (out_dists) PANN_CUDA(cudaMemcpyAsync(out_dists, idx->dists.p, 4 * k * nq, cudaMemcpyDeviceToHost, st));
+  }
+  if (out_visited) PANN_CUDA(cudaMemcpyAsync(out_visited, idx->vis.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  if (out_cmps) PANN_CUDA(cudaMemcpyAsync(out_cmps, idx->cmps.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  std::vector<uint32_t> status(nq);
+  PANN_CUDA(cudaMemcpyAsync(status.data(), idx->status.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  return summarize_status(status.data(), nq, out_flags);
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Internal definition of the index handle behind the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include "../../include/parlayann_b200.h"
+
+namespace pann {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PANN_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t _e = (call);                              \
+    if (_e != cudaSuccess) return ::pann::cuda_fail(_e, #call); \
+  } while (0)
+
+// Device scratch buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace pann
+
+struct pann_index {
+  int dtype = 0, metric = 0;
+  uint64_t n = 0;
+  uint32_t d = 0, R = 0;
+  uint32_t esize = 1;
+  uint64_t stride = 0;  // bytes per device row
+  uint32_t nchunks = 0;
+  int device = 0;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  uint8_t* d_points = nullptr;
+  uint32_t* d_graph = nullptr;
+  bool points_set = false;
+  cudaStream_t stream = nullptr;
+  // search scratch
+  pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, starts, tmp;
+  uint32_t starts_cached_n = 0;
+  uint32_t starts_cached[64] = {};
+};
+
+namespace pann {
+
+struct SearchPlan {
+  uint32_t k, L, dl;
+  uint64_t limit;
+  double bf;
+  uint32_t n_start;
+  uint32_t ref_half;
+  uint32_t Ccap;
+};
+
+int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan);
+
+// Run the tiered search on device buffers (queries already in index row layout).
+// self_ids (device, nullable) selects build mode: query j is point self_ids[j].
+int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
+               uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
+               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st);
+
+}  // namespace pann

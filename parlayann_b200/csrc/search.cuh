@@ -1,0 +1,295 @@
+// Warp-per-query beam search: the device form of ParlayANN's
+// filtered_beam_search with use_filtering = false and no early stopping
+// (algorithms/utils/beamSearch.h:33-228).
+//
+// One warp owns one query at a time and keeps all of its search state in
+// shared memory:
+//   qs    the query vector (row stride bytes)
+//   fr    the frontier, <= L 64-bit (dist, id) keys, sorted; bit 31 of the id
+//         word marks a visited entry. The reference's separate sorted
+//         `visited` list and `unvisited_frontier` (set_difference, :217-222)
+//         are represented by that flag: the next node to expand is the first
+//         unflagged frontier entry, exactly unvisited_frontier[offset] (:119),
+//         because between merges the frontier is unchanged and the flagged
+//         entries are precisely unvisited_frontier[0..offset).
+//   cand  candidates accumulated since the last merge (deferred batching,
+//         :185-192); sorted by rank into cand2 and merged into the frontier
+//         (set_union + trim to L, :197-214).
+//   table the seen-set (:66, hashset.h). The reference's hashset is exact
+//         until it grows; this table is exact, and the kernel counts inserts
+//         against the reference's growth threshold (capacity/2) to flag
+//         queries on which the reference's growth could change its result.
+// Lanes split the adjacency row (one id per lane), test-and-insert ids with
+// shared-memory CAS, compact the new ids, and compute one distance per lane
+// (so float sums keep the reference's sequential order).
+#pragma once
+#include "common.cuh"
+
+namespace pann {
+
+struct SearchArgs {
+  // index
+  const uint8_t* points;
+  uint64_t stride;  // bytes per row (multiple of 16)
+  uint32_t d;
+  uint32_t nchunks;  // stride / 16
+  const uint32_t* graph;
+  uint32_t R;
+  // queries
+  const uint8_t* queries;  // nq rows of `stride` bytes; null in build mode
+  const uint32_t* self_ids;  // build mode: query j is point self_ids[j] and skips itself
+  uint32_t nq;
+  const uint32_t* job_list;   // optional: job j is query job_list[j]
+  const uint32_t* njobs_dev;  // optional: number of jobs read from device memory
+  uint32_t* job_counter;      // dynamic work distribution (zeroed before launch)
+  // query parameters (QueryParams, types.h:233-252)
+  uint32_t k, L, dl;
+  uint64_t limit;
+  double batch_factor;
+  uint32_t ref_half;  // the reference hashset's growth threshold: capacity/2
+  const uint32_t* starts;
+  uint32_t n_start;
+  // per-warp shared-memory layout
+  uint32_t Ccap;  // candidate buffer capacity
+  uint32_t S;     // seen-table slots (power of two)
+  uint32_t warp_bytes;
+  uint32_t* gtables;  // global seen tables (TABLE_GLOBAL form), S slots per resident warp
+  // outputs
+  uint32_t* out_ids;
+  float* out_dists;
+  uint32_t* out_visited;
+  uint32_t* out_cmps;
+  uint32_t* out_status;
+  uint64_t* vis_keys;  // build mode: visited (dist,id) keys, vis_cap per query
+  uint32_t vis_cap;
+  uint32_t* redo_list;  // queries whose seen table filled up
+  uint32_t* redo_count;
+};
+
+__host__ __device__ inline uint32_t search_warp_bytes(uint64_t stride, uint32_t L, uint32_t Ccap, uint32_t R,
+                                                      uint32_t S, bool table_global) {
+  uint64_t b = stride;                 // query
+  b += 16ull * L;                      // fr + fr2
+  b += 16ull * Ccap;                   // cand + cand2
+  b += 4ull * ((R + 3) & ~3u);         // compacted new ids
+  if (!table_global) b += 4ull * S;    // seen table
+  return (uint32_t)((b + 15) & ~15ull);
+}
+
+// Sort n distinct keys from `in` into `out` by rank (warp-cooperative).
+__device__ __forceinline__ void warp_rank_sort(const uint64_t* in, uint64_t* out, int n, int lane) {
+  for (int i = lane; i < n; i += 32) {
+    uint64_t ki = in[i] & PANN_KEYMASK;
+    int r = 0;
+    for (int j = 0; j < n; j++) {
+      uint64_t kj = in[j] & PANN_KEYMASK;
+      r += (kj < ki) | ((kj == ki) & (j < i));
+    }
+    out[r] = in[i];
+  }
+}
+
+// Merge sorted frontier fr[0..fn) with sorted candidates c[0..cn) into out,
+// keeping the first L (std::set_union then trim, beamSearch.h:202-214). Keys
+// of the two inputs are disjoint (the seen-set admits each id once).
+__device__ __forceinline__ int warp_merge(const uint64_t* fr, int fn, const uint64_t* c, int cn, uint64_t* out,
+                                          int L, int lane) {
+  for (int i = lane; i < fn; i += 32) {
+    uint64_t k = fr[i] & PANN_KEYMASK;
+    int lo = 0, hi = cn;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if ((c[mid] & PANN_KEYMASK) < k) lo = mid + 1; else hi = mid; }
+    int pos = i + lo;
+    if (pos < L) out[pos] = fr[i];
+  }
+  for (int j = lane; j < cn; j += 32) {
+    uint64_t k = c[j] & PANN_KEYMASK;
+    int lo = 0, hi = fn;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if ((fr[mid] & PANN_KEYMASK) < k) lo = mid + 1; else hi = mid; }
+    int pos = j + lo;
+    if (pos < L) out[pos] = c[j];
+  }
+  int t = fn + cn;
+  return t < L ? t : L;
+}
+
+// Test-and-insert into an open-addressing table (linear probing). Returns 1 if
+// id was inserted (first sighting), 0 if it was already present. The caller
+// keeps the load below 1 so the probe always ends.
+__device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint32_t id) {
+  uint32_t h = hash_slot(id, mask);
+  for (uint32_t probe = 0; probe <= mask; probe++) {
+    uint32_t old = atomicCAS(table + h, PANN_PAD, id);
+    if (old == PANN_PAD) return 1;
+    if (old == id) return 0;
+    h = (h + 1) & mask;
+  }
+  return 0;
+}
+
+template <int DT, int MT, bool TABLE_GLOBAL>
+__global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const unsigned FULL = 0xFFFFFFFFu;
+
+  uint8_t* wbase = smem + (size_t)warp * a.warp_bytes;
+  uint8_t* qs = wbase;
+  uint64_t* frA = reinterpret_cast<uint64_t*>(wbase + a.stride);
+  uint64_t* frB = frA + a.L;
+  uint64_t* cand = frB + a.L;
+  uint64_t* cand2 = cand + a.Ccap;
+  uint32_t* nbuf = reinterpret_cast<uint32_t*>(cand2 + a.Ccap);
+  uint32_t* table;
+  if (TABLE_GLOBAL) {
+    table = a.gtables + ((size_t)blockIdx.x * wpb + warp) * a.S;
+  } else {
+    table = nbuf + ((a.R + 3) & ~3u);
+  }
+  const uint32_t mask = a.S - 1;
+  const uint32_t table_limit = (a.S >> 2) * 3;  // abort above 3/4 load
+  const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
+  const uint32_t L = a.L;
+
+  for (;;) {
+    uint32_t job = 0;
+    if (lane == 0) job = atomicAdd(a.job_counter, 1u);
+    job = __shfl_sync(FULL, job, 0);
+    if (job >= njobs) break;
+    const uint32_t qi = a.job_list ? a.job_list[job] : job;
+    const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
+    const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
+
+    // stage the query, clear the seen table
+    for (uint32_t c = lane; c < a.nchunks; c += 32)
+      reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(qsrc) + c);
+    {
+      uint4 e = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+      for (uint32_t c = lane; c < (a.S >> 2); c += 32) reinterpret_cast<uint4*>(table)[c] = e;
+    }
+    if (TABLE_GLOBAL) __threadfence_block();
+    __syncwarp();
+    int32_t qq = 0;
+    if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), a.nchunks);
+
+    // starting points (:73-77); n_start <= L, staged in frB then sorted into frA
+    for (uint32_t s = lane; s < a.n_start; s += 32) {
+      uint32_t id = a.starts[s];
+      float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
+      frB[s] = make_key(dd, id);
+      table_insert(table, mask, id);
+    }
+    __syncwarp();
+    uint64_t* fr = frA;
+    uint64_t* fr2 = frB;
+    warp_rank_sort(frB, fr, (int)a.n_start, lane);
+    __syncwarp();
+    int fn = (int)a.n_start;
+    int cn = 0;
+    uint32_t entries = a.n_start;
+    uint32_t cmps = a.n_start;
+    uint64_t nvis = 0;
+    uint32_t status = 0;
+
+    for (;;) {
+      __syncwarp();
+      // first unvisited frontier entry and the number of unvisited entries
+      int first = -1, cnt = 0;
+      for (int b = 0; b < fn; b += 32) {
+        int i = b + lane;
+        bool unv = (i < fn) && !(fr[i] & PANN_VFLAG);
+        unsigned m = __ballot_sync(FULL, unv);
+        if (first < 0 && m) first = b + __ffs(m) - 1;
+        cnt += __popc(m);
+      }
+      if (first < 0 || nvis >= a.limit) break;  // :116
+      const uint64_t cur = fr[first];
+      __syncwarp();
+      if (lane == 0) fr[first] = cur | PANN_VFLAG;
+      nvis++;
+      if (a.vis_keys && lane == 0) {
+        if (nvis <= a.vis_cap) a.vis_keys[(uint64_t)qi * a.vis_cap + (nvis - 1)] = cur & PANN_KEYMASK;
+      }
+      if (nvis > a.vis_cap && a.vis_keys) status |= QS_VISIT_OVERFLOW;
+      const bool full = (fn == (int)L);
+      const float cutoff = full ? key_dist(fr[fn - 1]) : 3.40282346638528859812e+38F;  // :173-175
+      const uint32_t cid = key_id(cur);
+
+      // neighbours not seen before (:151-160), compacted into nbuf
+      const uint32_t nel = a.dl < a.R ? a.dl : a.R;
+      const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
+      int nnew = 0;
+      uint32_t ins = 0;
+      for (uint32_t b = 0; b < nel; b += 32) {
+        uint32_t j = b + lane;
+        uint32_t v = (j < nel) ? __ldg(grow + j) : PANN_PAD;
+        int inserted = 0;
+        if (v != PANN_PAD) inserted = table_insert(table, mask, v);
+        bool isnew = inserted && (v != self);
+        unsigned mi = __ballot_sync(FULL, inserted);
+        unsigned mn = __ballot_sync(FULL, isnew);
+        ins += __popc(mi);
+        if (isnew) nbuf[nnew + __popc(mn & ((1u << lane) - 1))] = v;
+        nnew += __popc(mn);
+      }
+      entries += ins;
+      if (entries > a.ref_half) status |= QS_REF_WOULD_GROW;
+      if (entries > table_limit) { status |= QS_TABLE_FULL; break; }
+      __syncwarp();
+
+      // distances; keep those below the cutoff (:176-182)
+      cmps += (uint32_t)nnew;
+      if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
+      for (int b = 0; b < nnew; b += 32) {
+        int i = b + lane;
+        bool keep = false;
+        uint64_t key = 0;
+        if (i < nnew) {
+          uint32_t v = nbuf[i];
+          float dd = point_dist<DT, MT>(a.points + (uint64_t)v * a.stride, qs, a.d, a.nchunks, qq);
+          keep = !(dd >= cutoff);
+          key = make_key(dd, v);
+        }
+        unsigned mk = __ballot_sync(FULL, keep);
+        if (keep) cand[cn + __popc(mk & ((1u << lane) - 1))] = key;
+        cn += __popc(mk);
+      }
+      // deferred batching (:185-192): cnt - 1 unvisited entries remain after this one
+      if (cn == 0 || (a.limit >= 2ull * L && (double)cn < a.batch_factor * (double)L && cnt - 1 >= 1)) continue;
+      __syncwarp();
+      warp_rank_sort(cand, cand2, cn, lane);
+      __syncwarp();
+      fn = warp_merge(fr, fn, cand2, cn, fr2, (int)L, lane);
+      uint64_t* t = fr; fr = fr2; fr2 = t;
+      cn = 0;
+      __syncwarp();
+    }
+
+    if (status & (QS_TABLE_FULL | QS_INTERNAL)) {
+      if (status & QS_INTERNAL) {
+        if (lane == 0 && a.out_status) a.out_status[qi] = status;
+        __syncwarp();
+        continue;
+      }
+      if (lane == 0 && a.redo_list) a.redo_list[atomicAdd(a.redo_count, 1u)] = qi;
+      if (lane == 0 && a.out_status) a.out_status[qi] = status;
+      __syncwarp();
+      continue;
+    }
+    if ((uint32_t)fn < a.k) status |= QS_SHORT;
+    for (uint32_t j = lane; j < a.k; j += 32) {
+      bool ok = j < (uint32_t)fn;
+      a.out_ids[(uint64_t)qi * a.k + j] = ok ? key_id(fr[j]) : PANN_PAD;
+      if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = ok ? key_dist(fr[j]) : 0.0f;
+    }
+    if (lane == 0) {
+      if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;
+      if (a.out_cmps) a.out_cmps[qi] = cmps;
+      if (a.out_status) a.out_status[qi] = status;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace pann
