@@ -199,7 +199,7 @@ __global__ void reverse_classify_kernel(uint32_t* graph, uint32_t R, const uint3
                                         const uint32_t* __restrict__ counts, const uint32_t* __restrict__ offs,
                                         const uint32_t* __restrict__ num_runs, const uint32_t* __restrict__ vals,
                                         uint32_t* job_pts, uint32_t* job_off, uint32_t* job_n, uint32_t* job_begin,
-                                        uint32_t* njobs) {
+                                        uint32_t* njobs, unsigned long long* seg_total) {
   const int lane = threadIdx.x & 31;
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t runs = *num_runs;
@@ -239,11 +239,12 @@ __global__ void reverse_classify_kernel(uint32_t* graph, uint32_t R, const uint3
       for (uint32_t j = m + keep_cnt + lane; j < R; j += 32) row[j] = PANN_PAD;
       __syncwarp();
     } else if (lane == 0) {
+      // a segment of exactly m candidates + deg current neighbours, packed by an atomic cursor
       uint32_t t = atomicAdd(njobs, 1u);
       job_pts[t] = tgt;
       job_off[t] = off;
       job_n[t] = m;
-      job_begin[t] = off + r * R;  // room for m candidates + up to R current neighbours
+      job_begin[t] = (uint32_t)atomicAdd(seg_total, (unsigned long long)(m + deg));
     }
   }
 }
@@ -429,13 +430,14 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
   BCUDA(cudaMemcpyAsync(bb.start.p, &start0, 4, cudaMemcpyHostToDevice, st));
   BCUDA(bb.counters.ensure(256));
   uint32_t* c32 = bb.counters.as<uint32_t>();  // [0] status or, [1] njobs, [2] flagged count
-  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(c32 + 8);  // [0] dist cmps, [1] visited
+  // [0] dist cmps, [1] visited, [2] reverse prune segment cursor
+  unsigned long long* c64 = reinterpret_cast<unsigned long long*>(c32 + 8);
   BCUDA(cudaMemsetAsync(bb.counters.p, 0, 256, st));
 
   const uint64_t pairs_cap = maxB * R;
   auto alloc_batch = [&](uint32_t vcap) -> int {
     uint64_t segcap = vcap + R;
-    uint64_t seg_items = std::max<uint64_t>(maxB * segcap, 2 * pairs_cap);
+    uint64_t seg_items = maxB * segcap;
     BCUDA(bb.vis_keys.ensure(8 * maxB * vcap));
     BCUDA(bb.vis_n.ensure(4 * maxB));
     BCUDA(bb.cmps.ensure(4 * maxB));
@@ -566,19 +568,37 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
                                             (int)np, st));
       }
       BCUDA(cudaMemsetAsync(c32 + 1, 0, 4, st));
+      BCUDA(cudaMemsetAsync(c64 + 2, 0, 8, st));
       {
         int blocks = (int)std::min<uint64_t>((np * 32 + 255) / 256, 65535);
         reverse_classify_kernel<<<blocks, 256, 0, st>>>(idx->d_graph, R, bb.uniq.as<uint32_t>(),
                                                         bb.counts.as<uint32_t>(), bb.offs.as<uint32_t>(),
                                                         bb.nruns.as<uint32_t>(), bb.pv_b.as<uint32_t>(),
                                                         bb.jobs.as<uint32_t>(), bb.job_off.as<uint32_t>(),
-                                                        bb.job_n.as<uint32_t>(), bb.seg_begin.as<uint32_t>(), c32 + 1);
+                                                        bb.job_n.as<uint32_t>(), bb.seg_begin.as<uint32_t>(), c32 + 1,
+                                                        c64 + 2);
         BCUDA(cudaGetLastError());
       }
       uint32_t njobs = 0;
+      unsigned long long seg_total = 0;
       BCUDA(cudaMemcpyAsync(&njobs, c32 + 1, 4, cudaMemcpyDeviceToHost, st));
+      BCUDA(cudaMemcpyAsync(&seg_total, c64 + 2, 8, cudaMemcpyDeviceToHost, st));
       BCUDA(cudaStreamSynchronize(st));
       if (njobs) {
+        if (seg_total >= 0x7FFFFFFFull) {
+          cleanup();
+          return fail(PANN_ENOMEM, "reverse-edge prune segments exceed 2^31 keys");
+        }
+        // scratch for exactly seg_total keys (grown if this batch needs more)
+        BCUDA(bb.seg_a.ensure(8 * seg_total + 8));
+        BCUDA(bb.seg_b.ensure(8 * seg_total + 8));
+        {
+          size_t need = 0;
+          cub::DeviceSegmentedSort::SortKeys(nullptr, need, bb.seg_a.as<uint64_t>(), bb.seg_b.as<uint64_t>(),
+                                             (int)seg_total, (int)njobs, bb.seg_begin.as<uint32_t>(),
+                                             bb.seg_end.as<uint32_t>(), st);
+          BCUDA(bb.cub_tmp.ensure(need + 256));
+        }
         BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
           constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
           int blocks = (int)std::min<uint32_t>((njobs + wpb - 1) / wpb, 65535);
@@ -591,7 +611,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
         {
           size_t tb = bb.cub_tmp.bytes;
           BCUDA(cub::DeviceSegmentedSort::SortKeys(bb.cub_tmp.p, tb, bb.seg_a.as<uint64_t>(), bb.seg_b.as<uint64_t>(),
-                                                   (int)(2 * np), (int)njobs, bb.seg_begin.as<uint32_t>(),
+                                                   (int)seg_total, (int)njobs, bb.seg_begin.as<uint32_t>(),
                                                    bb.seg_end.as<uint32_t>(), st));
         }
         BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
