@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: beam-search QPS at recall@10 >= 0.95 on one B200 (per GPU replica).
+
+Workload (the plain float32 path at scale): 1,000,000 base + 10,000 query
+vectors, 96-d float32, 256-component Gaussian mixture (centres N(0,1),
+per-dimension sigma 0.3), every vector L2-normalised, seed 1 (synthetic,
+seeded; stands in for the public datasets). Vamana graph built on the GPU
+with R=64, L=128, alpha=1.2, two passes, prefix-doubling batches. Beam search
+k=10 from start point 0 with degree_limit=R, limit=n, batch_factor=0.125, at
+the smallest beam in the reference's sweep list (check_nn_recall.h:214-216)
+whose recall@10 against FP64 brute force is >= 0.95.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one batched beam search over the 10,000 queries. `value` is
+device-timed (CUDA events on the launching stream, inputs resident in HBM,
+L2 flushed between steps); `e2e` is the same metric through the host-buffer
+C-ABI call (pinned host queries in, ids/distances/counters out, copies inside
+the timed region). `--impl reference` times the reference's own qsearchAll
+(compiled in place, oracle/_ref) on the host cores. Under torchrun every rank
+runs an independent replica (no data-path collective); the timed region is
+bracketed by barriers and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BEAMS = [10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 22, 24, 26, 28, 30, 32, 34, 36, 38, 40, 45, 50, 55, 60, 65,
+         70, 80, 90, 100, 120, 140, 160, 180, 200]
+METRIC = "QPS at recall@10>=0.95 (beam search, 1M x 96-d f32, 10K queries)"
+W = dict(n=1_000_000, nq=10_000, d=96, comps=256, seed=1, sigma=0.3, R=64, Lb=128, alpha=1.2, passes=2, k=10,
+         bf=0.125)
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_data():
+    import parlayann_b200 as P
+
+    base = P.synth_mixture(P.F32, W["n"], W["d"], W["comps"], W["seed"], 0, sigma=W["sigma"], normalize=True)
+    q = P.synth_mixture(P.F32, W["nq"], W["d"], W["comps"], W["seed"], 1, sigma=W["sigma"], normalize=True)
+    return base, q
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(mp["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per query of the search kernel from the committed ncu summary (profiles/)."""
+    try:
+        s = json.load(open(os.path.join(ROOT, "profiles", "search_f32_c1.json")))
+        return float(s["dram_bytes_per_query"]), s
+    except Exception:
+        return None, None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import parlayann_b200 as P
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    lib = P.lib()
+    base, q = make_data()
+    idx = P.Index(base, W["R"])
+    t0 = time.time()
+    build_dev = None
+    if args.load_graph:
+        idx.load_graph(args.load_graph)
+    else:
+        bst = idx.build(W["Lb"], W["alpha"], num_passes=W["passes"], batch_factor=W["bf"])
+        build_dev = round(bst.seconds, 3)
+        if args.save_graph:
+            idx.save_graph(args.save_graph)
+    build_wall = time.time() - t0
+    g = idx.get_graph()
+    avg_deg = float(g[:, 0].mean())
+    gt, gd = idx.groundtruth(q, 20)
+    k = W["k"]
+    # smallest beam of the reference's sweep with recall@10 >= 0.95
+    beam, recall, sweep, res = None, None, [], None
+    for L in ([] if args.beam else BEAMS):
+        r = idx.search(q, k, L, batch_factor=W["bf"])
+        rec = P.recall_with_ties(r.ids, gt, gd, k)
+        sweep.append((L, round(rec, 4)))
+        if rec >= 0.95:
+            beam, recall, res = L, rec, r
+            break
+    if res is None:
+        beam = args.beam or BEAMS[-1]
+        res = idx.search(q, k, beam, batch_factor=W["bf"])
+        recall = P.recall_with_ties(res.ids, gt, gd, k)
+    nq = q.shape[0]
+    mean_vis = float(res.visited.mean())
+    mean_cmps = float(res.cmps.mean())
+    row_bytes = W["d"] * 4
+    bytes_per_query = 4.0 * mean_vis * (1.0 + avg_deg) + mean_cmps * row_bytes + row_bytes
+
+    # device-resident timed loop
+    qp = P.QueryParams(k, beam, W["n"], W["R"], W["bf"])
+    starts = np.zeros(1, np.uint32)
+    dq = torch.from_numpy(q).to(dev)
+    d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+    d_dists = torch.empty((nq, k), dtype=torch.float32, device=dev)
+    d_vis = torch.empty(nq, dtype=torch.int32, device=dev)
+    d_cmps = torch.empty(nq, dtype=torch.int32, device=dev)
+    d_flags = torch.empty(nq, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+    stream = torch.cuda.current_stream(dev)
+
+    def step_device():
+        rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(dq.data_ptr()), nq, ctypes.byref(qp),
+                                    starts.ctypes.data_as(ctypes.c_void_p), 1, ctypes.c_void_p(d_ids.data_ptr()),
+                                    ctypes.c_void_p(d_dists.data_ptr()), ctypes.c_void_p(d_vis.data_ptr()),
+                                    ctypes.c_void_p(d_cmps.data_ptr()), ctypes.c_void_p(d_flags.data_ptr()),
+                                    ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise P.PannError(rc, lib.pann_last_error().decode())
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        step_device()
+    torch.cuda.synchronize()
+    assert np.array_equal(d_ids.cpu().numpy().astype(np.uint32), res.ids), "device path differs from host path"
+    times = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)  # L2 flush outside the timed span
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_device()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_dev = sum(times)
+    if world > 1:
+        tt = torch.tensor([t_dev], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    qps = world * nq * args.steps / t_dev
+
+    # end-to-end through the host-buffer C-ABI call (pinned buffers, copies timed)
+    hq = torch.from_numpy(q).pin_memory()
+    h_ids = torch.empty((nq, k), dtype=torch.int32).pin_memory()
+    h_d = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    h_v = torch.empty(nq, dtype=torch.int32).pin_memory()
+    h_c = torch.empty(nq, dtype=torch.int32).pin_memory()
+    h_f = torch.empty(nq, dtype=torch.int32).pin_memory()
+
+    def step_e2e():
+        rc = lib.pann_search(idx.handle, ctypes.c_void_p(hq.data_ptr()), nq, ctypes.byref(qp),
+                             starts.ctypes.data_as(ctypes.c_void_p), 1, ctypes.c_void_p(h_ids.data_ptr()),
+                             ctypes.c_void_p(h_d.data_ptr()), ctypes.c_void_p(h_v.data_ptr()),
+                             ctypes.c_void_p(h_c.data_ptr()), ctypes.c_void_p(h_f.data_ptr()))
+        if rc != 0:
+            raise P.PannError(rc, lib.pann_last_error().decode())
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        step_e2e()
+    e2e_times = []
+    if world > 1:
+        dist.barrier()
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        step_e2e()
+        e2e_times.append(time.perf_counter() - t)
+    t_e2e = sum(e2e_times)
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    assert np.array_equal(h_ids.numpy().astype(np.uint32), res.ids), "e2e path differs"
+
+    peak, peak_kind = measured_peak()
+    per_launch_s = t_dev / args.steps
+    achieved = bytes_per_query * nq / per_launch_s / 1e9
+    traffic_pq, prof = profiled_traffic()
+    line = None
+    if rank == 0:
+        cpu = cpu_baseline(base, q, g, beam, args) if not args.no_cpu_baseline else None
+        line = {
+            "metric": METRIC,
+            "value": round(qps, 1),
+            "unit": "queries/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t_dev / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded 256-component Gaussian mixture, L2-normalised)",
+            "config": {"workload": "plain beam search, 1M x 96-d f32, 10K queries, Vamana R=64 L=128 alpha=1.2 2 passes",
+                       "n": W["n"], "nq": nq, "d": W["d"], "k": k, "beam": beam, "recall_at_10": round(recall, 4),
+                       "degree_limit": W["R"], "batch_factor": W["bf"], "l2_flush": "256 MB write between steps",
+                       "parallelism": f"replicas x{world}", "build_seconds_device": build_dev,
+                       "build_seconds_wall": round(build_wall, 3), "mean_visited": round(mean_vis, 2),
+                       "mean_cmps": round(mean_cmps, 2), "flagged_queries": int(res.flags.sum()),
+                       "recall_sweep": sweep},
+            "e2e": {"value": round(world * nq * args.steps / t_e2e, 1), "unit": "queries/s",
+                    "h2d_bytes_per_step": int(q.nbytes),
+                    "d2h_bytes_per_step": int(nq * k * 8 + nq * 12)},
+            "gpu_launches": 5 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (hbm_gbs)",
+                         "algorithmic_bytes_per_query": round(bytes_per_query, 1),
+                         "traffic": (round(traffic_pq * nq / 1e9, 4) if traffic_pq else None),
+                         "traffic_unit": "GB per launch (ncu dram read+write, scaled from profiles/)"},
+            "cpu_baseline": cpu,
+        }
+        c = clk.summary()
+        if c:
+            line["clocks"] = c
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    idx.close()
+    return line
+
+
+def cpu_baseline(base, q, graph, beam, args):
+    """The reference's qsearchAll (compiled in place) on the host cores, as a
+    reported baseline: a bounded sample of the same workload."""
+    try:
+        from oracle import oracle as O
+
+        if not O.have_ref():
+            return None
+        nq = min(q.shape[0], args.cpu_queries)
+        secs, ids, vis, cmps = O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        return {"value": round(nq / secs, 1), "unit": "queries/s", "cores": int(O.rlib().ref_num_workers()),
+                "kind": "reference",
+                "sample": f"{nq} of the {q.shape[0]} queries, one qsearchAll pass after a cache flush "
+                          f"({secs:.2f} s), same graph and beam {beam}"}
+    except Exception as ex:  # noqa: BLE001
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own build_index and qsearchAll on the host cores."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+
+    if not O.have_ref():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libpann_ref.so was not built (reference checkout absent at build time)"}
+    base, q = make_data()
+    t0 = time.time()
+    graph, _ = O.build_graph("ref", base, W["R"], W["Lb"], W["alpha"], W["passes"], batch_factor=W["bf"])
+    build_s = time.time() - t0
+    beam = args.beam or 45
+    nq = min(q.shape[0], args.cpu_queries)
+    for _ in range(args.warmup):
+        O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+    times = []
+    ids = None
+    for _ in range(args.steps):
+        secs, ids, vis, cmps = O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        times.append(secs)
+    t = sum(times)
+    qps = nq * args.steps / t
+    # recall on a query subsample against FP64 brute force (numpy, float64)
+    sub = min(200, nq)
+    qq = q[:sub].astype(np.float64)
+    bb = base.astype(np.float64)
+    d2 = (qq * qq).sum(1)[:, None] + (bb * bb).sum(1)[None, :] - 2.0 * qq @ bb.T
+    gt = np.argsort(d2, axis=1, kind="stable")[:, :10]
+    rec = float(np.mean([len(set(ids[i].tolist()) & set(gt[i].tolist())) / 10.0 for i in range(sub)]))
+    cores = int(O.rlib().ref_num_workers())
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(qps, 1),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * t / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded 256-component Gaussian mixture, L2-normalised)",
+        "config": {"workload": "plain beam search, 1M x 96-d f32, 10K queries, Vamana R=64 L=128 alpha=1.2 2 passes",
+                   "n": W["n"], "nq": nq, "d": W["d"], "k": W["k"], "beam": beam,
+                   "recall_at_10_sample": round(rec, 4), "build_seconds_cpu": round(build_s, 2),
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
+                         "sample": f"{nq} queries per step (qsearchAll after a cache flush, check_nn_recall.h:46-59)"},
+        "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--beam", type=int, default=0, help="fix the beam instead of sweeping for recall 0.95")
+    ap.add_argument("--cpu-queries", type=int, default=10000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
+    ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

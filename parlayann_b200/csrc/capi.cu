@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "index.cuh"
 #include "search.cuh"
+#include "search_emu.cuh"
 
 namespace pann {
 
@@ -127,6 +128,30 @@ static cudaError_t launch_search(int dtype, int metric, bool global_table, const
   return cudaErrorInvalidValue;
 }
 
+template <int DT, int MT, bool SM>
+static cudaError_t launch_emulate_t(const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem, cudaStream_t st) {
+  auto k = search_emulate_kernel<DT, MT, SM>;
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return err;
+  k<<<blocks, 32, smem, st>>>(a, e);
+  return cudaGetLastError();
+}
+static cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
+                                  int blocks, size_t smem, cudaStream_t st) {
+#define PANN_EMU_CASE(DT, MT)                                                              \
+  if (dtype == DT && metric == MT)                                                         \
+    return smem_tables ? launch_emulate_t<DT, MT, true>(a, e, blocks, smem, st)            \
+                       : launch_emulate_t<DT, MT, false>(a, e, blocks, smem, st);
+  PANN_EMU_CASE(DT_U8, MT_L2)
+  PANN_EMU_CASE(DT_U8, MT_IP)
+  PANN_EMU_CASE(DT_I8, MT_L2)
+  PANN_EMU_CASE(DT_I8, MT_IP)
+  PANN_EMU_CASE(DT_F32, MT_L2)
+  PANN_EMU_CASE(DT_F32, MT_IP)
+#undef PANN_EMU_CASE
+  return cudaErrorInvalidValue;
+}
+
 template <int DT, int MT, bool G>
 static int occupancy_t(int threads, size_t smem) {
   int nb = 0;
@@ -170,12 +195,16 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st) {
   if (nq == 0) return PANN_OK;
-  // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1
+  // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
+  // [5] shared-memory emulation job counter, [6] emulation list length,
+  // [7] global emulation job counter, [8] emulation overflow count
   PANN_CUDA(idx->counters.ensure(64));
-  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 2 * (size_t)nq));
+  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 4 * (size_t)nq));
   uint32_t* cnt = idx->counters.as<uint32_t>();
   uint32_t* redo0 = idx->redo.as<uint32_t>();
   uint32_t* redo1 = redo0 + nq;
+  uint32_t* emu = redo1 + nq;
+  uint32_t* ovf = emu + nq;
   PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
 
   SearchArgs a{};
@@ -204,6 +233,8 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.out_status = d_status;
   a.vis_keys = d_vis_keys;
   a.vis_cap = vis_cap;
+  a.emu_list = emu;
+  a.emu_count = cnt + 6;
 
   const size_t smem_cap = idx->smem_optin;
   // ---- tier 0
@@ -276,6 +307,55 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     t.redo_list = nullptr;
     t.redo_count = nullptr;
     PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, slots, 32, wb, st));
+  }
+  // ---- tier E: exact emulation of the reference's hashset for flagged queries,
+  // first with the emulated table in shared memory (capacities 4 S0 / 2 S0),
+  // then, for queries that outgrow it, in global memory (16 S0 / 8 S0)
+  {
+    double cap_n = 2.0 * (10.0 + (double)plan.L) * (double)plan.dl;
+    uint32_t bits0 = (uint32_t)std::ceil(std::log2(cap_n));
+    uint64_t S0 = 1ull << bits0;
+    uint32_t vs = pow2_at_least(8ull * plan.L + 64);
+    uint32_t base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, true);
+    SearchArgs t = a;
+    t.redo_list = nullptr;
+    t.redo_count = nullptr;
+    t.emu_list = nullptr;
+    t.emu_count = nullptr;
+    EmuArgs e{};
+    e.bits0 = bits0;
+    e.vs_slots = vs;
+    e.base_bytes = base;
+    size_t smem_need = emu_smem_bytes(base, vs, (uint32_t)(4 * S0), (uint32_t)(2 * S0), true);
+    const uint32_t* glist = emu;
+    uint32_t* gcount = cnt + 6;
+    if (smem_need <= smem_cap && 4 * S0 < (1ull << 31)) {
+      e.capA = (uint32_t)(4 * S0);
+      e.capB = (uint32_t)(2 * S0);
+      e.overflow_list = ovf;
+      e.overflow_count = cnt + 8;
+      t.job_list = emu;
+      t.njobs_dev = cnt + 6;
+      t.job_counter = cnt + 5;
+      PANN_CUDA(launch_emulate(idx->dtype, idx->metric, true, t, e, 2 * idx->sm_count, smem_need, st));
+      glist = ovf;
+      gcount = cnt + 8;
+    }
+    uint64_t capA = 16 * S0, capB = 8 * S0;
+    size_t per_slot = 4ull * (capA + capB);
+    int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(idx->sm_count, (1ull << 30) / per_slot));
+    PANN_CUDA(idx->emu.ensure(per_slot * slots));
+    e.gA = idx->emu.as<uint32_t>();
+    e.gB = e.gA + (size_t)slots * capA;
+    e.capA = (uint32_t)capA;
+    e.capB = (uint32_t)capB;
+    e.overflow_list = nullptr;
+    e.overflow_count = nullptr;
+    t.job_list = glist;
+    t.njobs_dev = gcount;
+    t.job_counter = cnt + 7;
+    PANN_CUDA(launch_emulate(idx->dtype, idx->metric, false, t, e, slots,
+                             emu_smem_bytes(base, vs, 0, 0, false), st));
   }
   return PANN_OK;
 }
@@ -376,7 +456,7 @@ int pann_index_destroy(pann_index* idx) {
   if (idx->d_points) cudaFree(idx->d_points);
   if (idx->d_graph) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
-                    &idx->counters, &idx->gtables, &idx->starts, &idx->tmp})
+                    &idx->counters, &idx->gtables, &idx->emu, &idx->starts, &idx->tmp})
     b->release();
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;

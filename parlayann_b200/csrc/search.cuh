@@ -64,6 +64,8 @@ struct SearchArgs {
   uint32_t vis_cap;
   uint32_t* redo_list;  // queries whose seen table filled up
   uint32_t* redo_count;
+  uint32_t* emu_list;   // queries on which the reference's hashset would grow
+  uint32_t* emu_count;
 };
 
 __host__ __device__ inline uint32_t search_warp_bytes(uint64_t stride, uint32_t L, uint32_t Ccap, uint32_t R,
@@ -274,6 +276,12 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
       }
       if (lane == 0 && a.redo_list) a.redo_list[atomicAdd(a.redo_count, 1u)] = qi;
       if (lane == 0 && a.out_status) a.out_status[qi] = status;
+      __syncwarp();
+      continue;
+    }
+    if ((status & QS_REF_WOULD_GROW) && a.emu_list) {
+      // re-run by the exact-emulation tier, which writes this query's outputs
+      if (lane == 0) a.emu_list[atomicAdd(a.emu_count, 1u)] = qi;
       __syncwarp();
       continue;
     }
