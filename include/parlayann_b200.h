@@ -105,17 +105,21 @@ int pann_graph_save(pann_index* idx, const char* path);
  * QueryParams; host buffers. Writes the first k frontier entries (ids,
  * distances) per query, and per-query visited-list size and distance
  * comparisons (stats<T> counters). Any of out_dists / out_visited / out_cmps /
- * out_flags may be NULL. out_flags bit 1: the reference's hashset would have
- * grown on that query (hashset.h:25-38).
+ * out_flags may be NULL. out_flags[i] is 1 where the reference's hashset grows
+ * on query i (hashset.h:25-38); those queries are reproduced by an exact
+ * emulation of that hashset, so results still equal the reference's.
  * Replaces qsearchAll / searchAll / beam_search (beamSearch.h:420-445,
  * 492-526, 599-646). */
 int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
                 const uint32_t* starts, uint32_t n_start, uint32_t* out_ids, float* out_dists,
                 uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags);
 
-/* Same, with every buffer in device memory, on `stream` (a cudaStream_t).
- * Does not synchronise; errors detected on the device are reported by the
- * next pann_search_status() call. starts is a HOST array. */
+/* Same, with every buffer in device memory, on `stream` (a cudaStream_t;
+ * 0 is the legacy default stream).
+ * Does not synchronise. d_out_flags (may be NULL) receives per-query status
+ * bits: 1 = the reference's hashset grows on this query (result reproduced
+ * exactly), 2 or 16 = the query's state outgrew every buffer (result invalid),
+ * 4 = fewer than k results. starts is a HOST array. */
 int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
                        uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);

@@ -63,8 +63,7 @@ __global__ void __launch_bounds__(128) assemble_kernel(const uint8_t* __restrict
   uint8_t* qs = smem + (size_t)warp * stride;
   for (uint32_t job = blockIdx.x * wpb + warp; job < njobs; job += gridDim.x * wpb) {
     const uint32_t p = pts[job];
-    for (int c = lane; c < nchunks; c += 32)
-      reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(points + (uint64_t)p * stride) + c);
+    stage_query<DT, MT>(qs, points + (uint64_t)p * stride, nchunks, lane);
     __syncwarp();
     int32_t qq = 0;
     if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);
@@ -152,8 +151,7 @@ __global__ void __launch_bounds__(128) greedy_prune_kernel(const uint8_t* __rest
       if (pstar == p) continue;  // :99-101
       if (lane == 0) row[nsel] = pstar;
       nsel++;
-      for (int c = lane; c < nchunks; c += 32)
-        reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(points + (uint64_t)pstar * stride) + c);
+      stage_query<DT, MT>(qs, points + (uint64_t)pstar * stride, nchunks, lane);
       __syncwarp();
       int32_t qq = 0;
       if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);
@@ -259,8 +257,7 @@ __global__ void __launch_bounds__(128) sort_neighbors_kernel(const uint8_t* __re
   uint64_t* kin = reinterpret_cast<uint64_t*>(qs + stride);
   uint64_t* kout = kin + R;
   for (uint64_t v = (uint64_t)blockIdx.x * wpb + warp; v < n; v += (uint64_t)gridDim.x * wpb) {
-    for (int c = lane; c < nchunks; c += 32)
-      reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(points + v * stride) + c);
+    stage_query<DT, MT>(qs, points + v * stride, nchunks, lane);
     __syncwarp();
     int32_t qq = 0;
     if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);

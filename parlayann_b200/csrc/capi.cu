@@ -173,24 +173,27 @@ static int search_occupancy(int dtype, int metric, bool g, int threads, size_t s
   return 0;
 }
 
-// Seen-table size of the first tier: the PANN_SEEN_SLOTS environment variable,
-// else about twice the distinct ids a search touches (visits x new neighbours).
+// Shared-memory seen-table slots of tier 0: the PANN_SEEN_SLOTS environment
+// variable, else room (at 3/4 load) for about (L + 16) * min(dl, R) * 3/4
+// distinct ids, between 4 (R + 1) and 8192 slots; queries that need more
+// continue in the per-warp global spill table.
 static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
+  uint32_t floor_s = pow2_at_least(4ull * (R + 1));
   if (const char* e = std::getenv("PANN_SEEN_SLOTS")) {
     long v = std::atol(e);
-    if (v > 0) return std::max<uint32_t>(pow2_at_least((uint64_t)v), pow2_at_least(4ull * (R + 1)));
+    if (v > 0) return std::max<uint32_t>(pow2_at_least((uint64_t)v), floor_s);
   }
   uint32_t nel = std::min(p.dl, R);
-  uint64_t est = (uint64_t)(p.L + 24) * nel;
+  uint64_t est = (uint64_t)(p.L + 16) * nel;  // (3/4 of the ids) / (3/4 load)
   uint32_t s = pow2_at_least(est);
   s = std::min<uint32_t>(s, 8192);
-  s = std::max<uint32_t>(s, pow2_at_least(4ull * (R + 1)));
-  return s;
+  return std::max<uint32_t>(s, floor_s);
 }
 
-// Three tiers: (0) many warps per SM with a modest shared-memory seen table;
-// (1) queries whose table filled up, one warp per block with the largest
-// shared-memory table; (2) the rest with a table in global memory.
+// Tiers: (0) every query, many warps per SM, shared-memory seen table with a
+// global spill table; (2) queries whose tables still filled up, with one large
+// global table per warp; (E) queries on which the reference's hashset grows,
+// re-run with that hashset emulated exactly.
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st) {
@@ -237,72 +240,55 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.emu_count = cnt + 6;
 
   const size_t smem_cap = idx->smem_optin;
-  // ---- tier 0
+  // ---- tier 0: many warps per SM, a modest shared-memory seen table that
+  // spills into a per-warp global table for the queries that outgrow it
   {
     uint32_t S = tier0_slots(plan, idx->R);
     uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
     int wpb = 4;
     while (wpb > 1 && (size_t)wb * wpb > smem_cap) wpb >>= 1;
-    if ((size_t)wb * wpb > smem_cap) {
-      S = 0;  // cannot fit: everything goes to the next tiers
+    while ((size_t)wb * wpb > smem_cap && S > pow2_at_least(4ull * (idx->R + 1))) {
+      S >>= 1;
+      wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
     }
-    if (S) {
-      SearchArgs t = a;
-      t.S = S;
-      t.warp_bytes = wb;
-      t.job_counter = cnt + 0;
-      t.redo_list = redo0;
-      t.redo_count = cnt + 3;
-      int occ = search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb);
-      if (occ <= 0) occ = 1;
-      uint64_t want = (nq + wpb - 1) / wpb;
-      int blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
-      PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st));
+    if ((size_t)wb * wpb > smem_cap) return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
+    int occ = search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb);
+    if (occ <= 0) occ = 1;
+    uint64_t want = (nq + wpb - 1) / wpb;
+    int blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
+    uint32_t Sg = std::max<uint32_t>(4 * S, pow2_at_least(2ull * plan.ref_half));
+    size_t slots = (size_t)blocks * wpb;
+    while (Sg > 4 * S && slots * Sg * 4 > (1ull << 30)) Sg >>= 1;
+    SearchArgs t = a;
+    t.S = S;
+    t.warp_bytes = wb;
+    t.job_counter = cnt + 0;
+    t.redo_list = redo0;
+    t.redo_count = cnt + 3;
+    if (idx->gtables.ensure(slots * Sg * 4) == cudaSuccess) {
+      t.gspill = idx->gtables.as<uint32_t>();
+      t.Sg = Sg;
     } else {
-      // route every query to tier 1: job list = identity
-      std::vector<uint32_t> ident(nq);
-      for (uint32_t i = 0; i < nq; i++) ident[i] = i;
-      PANN_CUDA(cudaMemcpyAsync(redo0, ident.data(), sizeof(uint32_t) * nq, cudaMemcpyHostToDevice, st));
-      PANN_CUDA(cudaMemcpyAsync(cnt + 3, &nq, sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-      PANN_CUDA(cudaStreamSynchronize(st));
+      cudaGetLastError();
+      t.gspill = nullptr;
+      t.Sg = 0;
     }
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st));
   }
-  // ---- tier 1: one warp per block, largest shared table
-  {
-    uint32_t base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, false);
-    uint32_t S = 1u << 15;
-    while (S > 512 && base + 4ull * S > smem_cap) S >>= 1;
-    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
-    if ((size_t)wb <= smem_cap) {
-      SearchArgs t = a;
-      t.S = S;
-      t.warp_bytes = wb;
-      t.job_list = redo0;
-      t.njobs_dev = cnt + 3;
-      t.job_counter = cnt + 1;
-      t.redo_list = redo1;
-      t.redo_count = cnt + 4;
-      int occ = search_occupancy(idx->dtype, idx->metric, false, 32, wb);
-      if (occ <= 0) occ = 1;
-      int blocks = std::max(1, occ * idx->sm_count);
-      PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32, wb, st));
-    } else {
-      return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
-    }
-  }
-  // ---- tier 2: global-memory seen table, sized above the reference's own capacity
+  // ---- tier 2: queries whose tables still filled up, with one global-memory
+  // seen table per warp sized above the reference's own capacity
   {
     uint32_t S = std::max<uint32_t>(1u << 16, pow2_at_least(4ull * plan.ref_half));
     S = std::min<uint32_t>(S, 1u << 24);
     int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * idx->sm_count, (256ull << 20) / (4ull * S)));
-    PANN_CUDA(idx->gtables.ensure((size_t)slots * S * 4));
+    PANN_CUDA(idx->gtables2.ensure((size_t)slots * S * 4));
     uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, true);
     SearchArgs t = a;
     t.S = S;
     t.warp_bytes = wb;
-    t.gtables = idx->gtables.as<uint32_t>();
-    t.job_list = redo1;
-    t.njobs_dev = cnt + 4;
+    t.gtables = idx->gtables2.as<uint32_t>();
+    t.job_list = redo0;
+    t.njobs_dev = cnt + 3;
     t.job_counter = cnt + 2;
     t.redo_list = nullptr;
     t.redo_count = nullptr;
@@ -456,7 +442,7 @@ int pann_index_destroy(pann_index* idx) {
   if (idx->d_points) cudaFree(idx->d_points);
   if (idx->d_graph) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
-                    &idx->counters, &idx->gtables, &idx->emu, &idx->starts, &idx->tmp})
+                    &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->starts, &idx->tmp})
     b->release();
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;
@@ -574,7 +560,7 @@ int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, cons
   SearchPlan plan;
   rc = make_plan(idx, qp, n_start, &plan);
   if (rc) return rc;
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : idx->stream;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);  // 0 is the legacy default stream
   rc = stage_starts(idx, starts, n_start, st);
   if (rc) return rc;
   const uint8_t* q = static_cast<const uint8_t*>(d_queries);

@@ -54,6 +54,8 @@ struct SearchArgs {
   uint32_t S;     // seen-table slots (power of two)
   uint32_t warp_bytes;
   uint32_t* gtables;  // global seen tables (TABLE_GLOBAL form), S slots per resident warp
+  uint32_t* gspill;   // shared-memory form: per resident warp, Sg-slot table taking inserts
+  uint32_t Sg;        // once the shared table is 3/4 full (0 = no spill: re-run instead)
   // outputs
   uint32_t* out_ids;
   float* out_dists;
@@ -66,6 +68,7 @@ struct SearchArgs {
   uint32_t* redo_count;
   uint32_t* emu_list;   // queries on which the reference's hashset would grow
   uint32_t* emu_count;
+  uint64_t opaque_zero;  // always 0; see f32_chunk2
 };
 
 __host__ __device__ inline uint32_t search_warp_bytes(uint64_t stride, uint32_t L, uint32_t Ccap, uint32_t R,
@@ -114,6 +117,18 @@ __device__ __forceinline__ int warp_merge(const uint64_t* fr, int fn, const uint
   return t < L ? t : L;
 }
 
+// Lookup without insert (linear probing): 1 if present.
+__device__ __forceinline__ int table_has(const uint32_t* table, uint32_t mask, uint32_t id) {
+  uint32_t h = hash_slot(id, mask);
+  for (uint32_t probe = 0; probe <= mask; probe++) {
+    uint32_t v = table[h];
+    if (v == id) return 1;
+    if (v == PANN_PAD) return 0;
+    h = (h + 1) & mask;
+  }
+  return 0;
+}
+
 // Test-and-insert into an open-addressing table (linear probing). Returns 1 if
 // id was inserted (first sighting), 0 if it was already present. The caller
 // keeps the load below 1 so the probe always ends.
@@ -129,7 +144,7 @@ __device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint
 }
 
 template <int DT, int MT, bool TABLE_GLOBAL>
-__global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -151,6 +166,9 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
   }
   const uint32_t mask = a.S - 1;
   const uint32_t table_limit = (a.S >> 2) * 3;  // abort above 3/4 load
+  uint32_t* spill = (!TABLE_GLOBAL && a.gspill) ? a.gspill + ((size_t)blockIdx.x * wpb + warp) * a.Sg : nullptr;
+  const uint32_t smask = a.Sg - 1;
+  const uint32_t spill_limit = (a.Sg >> 2) * 3;
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
   const uint32_t L = a.L;
 
@@ -164,8 +182,7 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
     const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
 
     // stage the query, clear the seen table
-    for (uint32_t c = lane; c < a.nchunks; c += 32)
-      reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(qsrc) + c);
+    stage_query<DT, MT>(qs, qsrc, (int)a.nchunks, lane);
     {
       uint4 e = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
       for (uint32_t c = lane; c < (a.S >> 2); c += 32) reinterpret_cast<uint4*>(table)[c] = e;
@@ -189,7 +206,9 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
     __syncwarp();
     int fn = (int)a.n_start;
     int cn = 0;
-    uint32_t entries = a.n_start;
+    uint32_t entries = a.n_start;    // distinct ids inserted (the reference's num_entries)
+    uint32_t entries_sh = a.n_start;  // of which in the shared-memory table
+    bool spilled = false;
     uint32_t cmps = a.n_start;
     uint64_t nvis = 0;
     uint32_t status = 0;
@@ -197,16 +216,25 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
     for (;;) {
       __syncwarp();
       // first unvisited frontier entry and the number of unvisited entries
-      int first = -1, cnt = 0;
+      int first = -1, second = -1, cnt = 0;
       for (int b = 0; b < fn; b += 32) {
         int i = b + lane;
         bool unv = (i < fn) && !(fr[i] & PANN_VFLAG);
         unsigned m = __ballot_sync(FULL, unv);
-        if (first < 0 && m) first = b + __ffs(m) - 1;
+        if (first < 0 && m) {
+          first = b + __ffs(m) - 1;
+          m &= m - 1;
+        }
+        if (first >= 0 && second < 0 && m) second = b + __ffs(m) - 1;
         cnt += __popc(m);
       }
+      if (first >= 0) cnt += 1;
       if (first < 0 || nvis >= a.limit) break;  // :116
       const uint64_t cur = fr[first];
+      // the next node to expand is most often the following unvisited entry:
+      // start its adjacency row on its way to L2
+      if (second >= 0 && lane == 0)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[second]) * a.R));
       __syncwarp();
       if (lane == 0) fr[first] = cur | PANN_VFLAG;
       nvis++;
@@ -221,13 +249,26 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
       // neighbours not seen before (:151-160), compacted into nbuf
       const uint32_t nel = a.dl < a.R ? a.dl : a.R;
       const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
+      if (!spilled && entries_sh + nel > table_limit) {
+        if (!spill) { status |= QS_TABLE_FULL; break; }
+        // the shared table is frozen from here on; new ids go to the global spill table
+        spilled = true;
+        uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+        for (uint32_t c = lane; c < (a.Sg >> 2); c += 32) reinterpret_cast<uint4*>(spill)[c] = e4;
+        __threadfence_block();
+        __syncwarp();
+      }
+      if (spilled && entries - entries_sh + nel > spill_limit) { status |= QS_TABLE_FULL; break; }
       int nnew = 0;
       uint32_t ins = 0;
       for (uint32_t b = 0; b < nel; b += 32) {
         uint32_t j = b + lane;
         uint32_t v = (j < nel) ? __ldg(grow + j) : PANN_PAD;
         int inserted = 0;
-        if (v != PANN_PAD) inserted = table_insert(table, mask, v);
+        if (v != PANN_PAD) {
+          if (!spilled) inserted = table_insert(table, mask, v);
+          else if (!table_has(table, mask, v)) inserted = table_insert(spill, smask, v);
+        }
         bool isnew = inserted && (v != self);
         unsigned mi = __ballot_sync(FULL, inserted);
         unsigned mn = __ballot_sync(FULL, isnew);
@@ -236,26 +277,33 @@ __global__ void __launch_bounds__(128) search_kernel(SearchArgs a) {
         nnew += __popc(mn);
       }
       entries += ins;
+      if (!spilled) entries_sh += ins;
       if (entries > a.ref_half) status |= QS_REF_WOULD_GROW;
-      if (entries > table_limit) { status |= QS_TABLE_FULL; break; }
       __syncwarp();
 
       // distances; keep those below the cutoff (:176-182)
       cmps += (uint32_t)nnew;
       if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
-      for (int b = 0; b < nnew; b += 32) {
-        int i = b + lane;
-        bool keep = false;
-        uint64_t key = 0;
-        if (i < nnew) {
-          uint32_t v = nbuf[i];
-          float dd = point_dist<DT, MT>(a.points + (uint64_t)v * a.stride, qs, a.d, a.nchunks, qq);
-          keep = !(dd >= cutoff);
-          key = make_key(dd, v);
+      // two rows per lane per round: rows b+lane and b+32+lane
+      for (int b = 0; b < nnew; b += 64) {
+        const int i0 = b + lane, i1 = b + 32 + lane;
+        float d0 = 0.0f, d1 = 0.0f;
+        uint32_t v0 = 0, v1 = 0;
+        if (i0 < nnew) {
+          v0 = nbuf[i0];
+          v1 = i1 < nnew ? nbuf[i1] : 0u;
+          point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
+                              i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
+                              a.opaque_zero);
         }
-        unsigned mk = __ballot_sync(FULL, keep);
-        if (keep) cand[cn + __popc(mk & ((1u << lane) - 1))] = key;
-        cn += __popc(mk);
+        bool keep0 = i0 < nnew && !(d0 >= cutoff);
+        unsigned m0 = __ballot_sync(FULL, keep0);
+        if (keep0) cand[cn + __popc(m0 & ((1u << lane) - 1))] = make_key(d0, v0);
+        cn += __popc(m0);
+        bool keep1 = i1 < nnew && !(d1 >= cutoff);
+        unsigned m1 = __ballot_sync(FULL, keep1);
+        if (keep1) cand[cn + __popc(m1 & ((1u << lane) - 1))] = make_key(d1, v1);
+        cn += __popc(m1);
       }
       // deferred batching (:185-192): cnt - 1 unvisited entries remain after this one
       if (cn == 0 || (a.limit >= 2ull * L && (double)cn < a.batch_factor * (double)L && cnt - 1 >= 1)) continue;

@@ -42,7 +42,7 @@ __device__ __forceinline__ uint32_t ref_slot(uint32_t k, uint32_t mask) {
   return (uint32_t)(((uint64_t)k * 0xbf58476d1ce4e5b9ull) & (uint64_t)mask);
 }
 
-// State of the emulated hashset; meaningful in lane 0 only.
+// State of the emulated hashset, identical in every lane of the warp.
 struct EmuHash {
   uint32_t* cur;
   uint32_t* other;
@@ -51,100 +51,137 @@ struct EmuHash {
   long long num_entries;
 };
 
-// Lane 0: process keys[j0..n) in order (hashset.h:22-48) until one needs the
-// table to grow. Writes each key reported unseen (and != self) to out[*nout].
-// Returns the index of the key that needs growth, or -1 when all are done.
-__device__ int emu_run(EmuHash& h, const uint32_t* keys, int j0, int n, bool stop_at_pad, uint32_t self,
-                       uint32_t* out, int* nout) {
-  for (int j = j0; j < n; j++) {
-    uint32_t a = keys[j];
-    if (stop_at_pad && a == PANN_PAD) return -1;
-    uint32_t size = 1u << h.bits, mask = size - 1;
-    uint32_t loc = ref_slot(a, mask);
-    if (h.cur[loc] == a) continue;
-    if (h.num_entries > (long long)(size / 2)) return j;
-    bool hit = false;
-    if (h.cur[loc] != PANN_PAD) {
-      loc = (loc + 1) & mask;
-      while (h.cur[loc] != PANN_PAD && h.cur[loc] != a) loc = (loc + 1) & mask;
-      hit = h.cur[loc] == a;
+// Order-preserving parallel linear probing. Lanes in `act` each hold a key;
+// processing them in lane order one at a time ("find the key or the first
+// empty slot from pos, insert there") gives the same table and results as
+// running rounds in which every unfinished lane probes the current table, and
+// among lanes that reach the same empty slot the lowest lane inserts while the
+// others continue past it. (A later key never changes an earlier key's
+// outcome: an empty slot on an earlier key's path before its own stop would
+// have been that key's stop.) Returns, per lane, whether it inserted (*ins)
+// and the slot where it stopped (*pos).
+__device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, uint32_t key, bool act, uint32_t start,
+                                                 int lane, bool* ins, uint32_t* pos) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  uint32_t p = start;
+  bool done = !act;
+  bool inserted = false;
+  for (;;) {
+    if (!done) {
+      uint32_t v = tab[p];
+      while (v != PANN_PAD && v != key) { p = (p + 1) & mask; v = tab[p]; }
+      if (v == key) done = true;
     }
-    if (hit) continue;
-    h.cur[loc] = a;
-    h.num_entries++;
-    if (out && a != self) out[(*nout)++] = a;
+    unsigned want = __ballot_sync(FULL, !done);
+    if (!want) break;
+    unsigned grp = __match_any_sync(FULL, done ? (0x80000000u | (uint32_t)lane) : p);
+    if (!done && (__ffs(grp & want) - 1) == lane) {
+      tab[p] = key;
+      inserted = true;
+      done = true;
+    }
+    __syncwarp();
   }
-  return -1;
+  *ins = inserted;
+  *pos = p;
 }
 
-// Warp: grow the table (re-insert in old-slot order), then lane 0 finishes the
-// call for key a from its old-mask slot. Returns false if the new table does
-// not fit this tier's capacity.
-__device__ bool emu_grow_and_insert(EmuHash& h, uint32_t a, uint32_t self, uint32_t* out, int* nout, int lane) {
+// Warp: grow the table (hashset.h:25-38): every key of the old table is
+// re-inserted in old-slot order (num_entries counts each re-insertion), then
+// the key that triggered the growth continues from its old-mask slot
+// (:39-47). Returns false if the grown table does not fit this tier.
+__device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool* a_seen) {
   const unsigned FULL = 0xFFFFFFFFu;
-  uint32_t size = 0, other_cap = 0;
-  uint32_t* other = nullptr;
-  if (lane == 0) { size = 1u << h.bits; other_cap = h.other_cap; other = h.other; }
-  size = __shfl_sync(FULL, size, 0);
-  other_cap = __shfl_sync(FULL, other_cap, 0);
-  other = reinterpret_cast<uint32_t*>(__shfl_sync(FULL, reinterpret_cast<unsigned long long>(other), 0));
-  const uint32_t nsize = size * 2;
-  if (nsize > other_cap) return false;
-  for (uint32_t i = lane; i < nsize; i += 32) other[i] = PANN_PAD;
+  const uint32_t size = 1u << h.bits, nsize = size * 2;
+  if (nsize > h.other_cap) return false;
+  uint32_t* other = h.other;
+  const uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+  for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
   __syncwarp();
-  __threadfence_block();
+  const uint32_t oldmask = size - 1, nmask = nsize - 1;
+  long long added = 0;
+  // re-insert in old-slot order: lane order within a 32-slot chunk is slot
+  // order, so the lanes holding keys go straight into the ordered rounds
+  for (uint32_t base = 0; base < size; base += 32) {
+    uint32_t k = h.cur[base + lane];
+    bool v = k != PANN_PAD;
+    unsigned m = __ballot_sync(FULL, v);
+    if (!m) continue;
+    bool ins;
+    uint32_t pos;
+    emu_probe_rounds(other, nmask, k, v, ref_slot(k, nmask), lane, &ins, &pos);
+    added += __popc(m);
+  }
+  h.num_entries += added;
+  uint32_t* t = h.cur; h.cur = h.other; h.other = t;
+  uint32_t c = h.cur_cap; h.cur_cap = h.other_cap; h.other_cap = c;
+  h.bits += 1;
+  // the call that grew the table: probe from the old-mask slot
+  int hit = 0;
   if (lane == 0) {
-    const uint32_t oldmask = size - 1, nmask = nsize - 1;
-    long long added = 0;
-    for (uint32_t i = 0; i < size; i++) {
-      uint32_t k = h.cur[i];
-      if (k != PANN_PAD) {
-        uint32_t l2 = ref_slot(k, nmask);
-        while (other[l2] != PANN_PAD && other[l2] != k) l2 = (l2 + 1) & nmask;
-        other[l2] = k;
-        added++;
-      }
-    }
-    h.num_entries += added;
-    uint32_t* t = h.cur; h.cur = h.other; h.other = t;
-    uint32_t c = h.cur_cap; h.cur_cap = h.other_cap; h.other_cap = c;
-    h.bits += 1;
-    // the call that grew the table continues with its old-mask slot (hashset.h:23,39-45)
     uint32_t loc = ref_slot(a, oldmask);
-    bool hit = false;
     if (h.cur[loc] != PANN_PAD) {
       loc = (loc + 1) & nmask;
       while (h.cur[loc] != PANN_PAD && h.cur[loc] != a) loc = (loc + 1) & nmask;
       hit = h.cur[loc] == a;
     }
-    if (!hit) {
-      h.cur[loc] = a;
-      h.num_entries++;
-      if (out && a != self) out[(*nout)++] = a;
-    }
+    if (!hit) h.cur[loc] = a;
   }
+  hit = __shfl_sync(FULL, hit, 0);
   __syncwarp();
+  __threadfence_block();
+  if (!hit) h.num_entries++;
+  *a_seen = hit != 0;
   return true;
 }
 
-// Run the emulated hashset over keys[0..n) (warp-uniform call). Returns false
-// on capacity overflow. *nout (lane 0) counts keys reported unseen.
-__device__ bool emu_lookup_all(EmuHash& h, const uint32_t* keys, int n, bool stop_at_pad, uint32_t self,
-                               uint32_t* out, int* nout, int lane) {
+// hashset::operator() (hashset.h:22-48) for up to 32 keys, lane i holding the
+// i-th key in call order (valid lanes form a prefix). *seen gets each call's
+// result. Returns false if the table would outgrow this tier.
+__device__ __forceinline__ bool emu_batch(EmuHash& h, uint32_t key, bool valid, int lane, bool* seen) {
   const unsigned FULL = 0xFFFFFFFFu;
-  int j = 0;
-  for (;;) {
-    int g = -1;
-    if (lane == 0) g = emu_run(h, keys, j, n, stop_at_pad, self, out, nout);
-    g = __shfl_sync(FULL, g, 0);
+  unsigned todo = __ballot_sync(FULL, valid);
+  bool my_seen = false;
+  while (todo) {
+    const bool act = (todo >> lane) & 1u;
+    const uint32_t size = 1u << h.bits, mask = size - 1;
+    const uint32_t home = ref_slot(key, mask);
+    const bool home_hit0 = act && h.cur[home] == key;  // present at its home before this batch
     __syncwarp();
-    if (g < 0) return true;
-    uint32_t a = 0;
-    if (lane == 0) a = keys[g];
-    a = __shfl_sync(FULL, a, 0);
-    if (!emu_grow_and_insert(h, a, self, out, nout, lane)) return false;
-    j = g + 1;
+    bool ins;
+    uint32_t pos;
+    emu_probe_rounds(h.cur, mask, key, act, home, lane, &ins, &pos);
+    // a repeated key whose first copy in this batch was inserted at that home
+    unsigned kgrp = __match_any_sync(FULL, act ? key : (0x80000000u | (uint32_t)lane));
+    int first = __ffs(kgrp & todo) - 1;
+    bool f_ins = __shfl_sync(FULL, ins, first < 0 ? lane : first);
+    uint32_t f_pos = __shfl_sync(FULL, pos, first < 0 ? lane : first);
+    bool home_hit = home_hit0 || (act && first >= 0 && first < lane && f_ins && f_pos == home);
+    // calls that miss their home slot check for growth against num_entries so far
+    unsigned insm = __ballot_sync(FULL, act && ins);
+    long long before = h.num_entries + __popc(insm & ((1u << lane) - 1));
+    bool grows = act && !home_hit && before > (long long)(size / 2);
+    unsigned gm = __ballot_sync(FULL, grows);
+    if (!gm) {
+      if (act) my_seen = !ins;
+      h.num_entries += __popc(insm);
+      break;
+    }
+    const int g = __ffs(gm) - 1;
+    // undo the tentative inserts of calls at or after g, keep the earlier ones
+    if (act && ins && lane >= g) h.cur[pos] = PANN_PAD;
+    __syncwarp();
+    __threadfence_block();
+    if (act && lane < g) my_seen = !ins;
+    h.num_entries += __popc(insm & ((1u << g) - 1));
+    uint32_t ag = __shfl_sync(FULL, key, g);
+    bool gseen = false;
+    if (!emu_grow(h, ag, lane, &gseen)) return false;
+    if (lane == g) my_seen = gseen;
+    todo &= ~((2u << g) - 1u);  // calls after g run against the grown table
   }
+  *seen = my_seen;
+  return true;
 }
 
 __device__ __forceinline__ void vset_insert(uint32_t* t, uint32_t mask, uint32_t id) {
@@ -217,8 +254,7 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     const uint32_t qi = a.job_list ? a.job_list[job] : job;
     const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
     const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
-    for (uint32_t c = lane; c < a.nchunks; c += 32)
-      reinterpret_cast<uint4*>(qs)[c] = __ldg(reinterpret_cast<const uint4*>(qsrc) + c);
+    stage_query<DT, MT>(qs, qsrc, (int)a.nchunks, lane);
     for (uint32_t i = lane; i < (1u << e.bits0); i += 32) tabA[i] = PANN_PAD;
     for (uint32_t i = lane; i < e.vs_slots; i += 32) vset[i] = PANN_PAD;
     __syncwarp();
@@ -227,6 +263,7 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     h.cur = tabA; h.other = tabB; h.cur_cap = e.capA; h.other_cap = e.capB;
     h.bits = e.bits0; h.num_entries = 0;
     bool ok = true;
+    bool sdummy;
     int32_t qq = 0;
     if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), a.nchunks);
 
@@ -236,10 +273,8 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
       frB[s] = make_key(dd, id);
     }
-    {
-      int dummy = 0;
-      ok = emu_lookup_all(h, a.starts, (int)a.n_start, false, PANN_PAD, nullptr, &dummy, lane);
-    }
+    for (uint32_t s0 = 0; s0 < a.n_start && ok; s0 += 32)
+      ok = emu_batch(h, s0 + lane < a.n_start ? a.starts[s0 + lane] : PANN_PAD, s0 + lane < a.n_start, lane, &sdummy);
     __syncwarp();
     uint64_t* fr = frA;
     uint64_t* fr2 = frB;
@@ -275,33 +310,46 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       const float cutoff = full ? key_dist(fr[fn - 1]) : 3.40282346638528859812e+38F;
       const uint32_t cid = key_id(cur_key);
       const uint32_t nel = a.dl < a.R ? a.dl : a.R;
-      // adjacency ids, staged in shared memory (cand2 is free until the merge),
-      // then looked up in order (:153-159)
-      uint32_t* row = reinterpret_cast<uint32_t*>(cand2);
-      for (uint32_t j = lane; j < nel; j += 32) row[j] = __ldg(a.graph + (uint64_t)cid * a.R + j);
-      __syncwarp();
+      // adjacency ids looked up in order, 32 calls per batch (:153-159)
       int nnew = 0;
-      if (!emu_lookup_all(h, row, (int)nel, true, self, nbuf, &nnew, lane)) {
+      bool full_tab = false;
+      for (uint32_t b = 0; b < nel; b += 32) {
+        uint32_t j = b + lane;
+        uint32_t v = j < nel ? __ldg(a.graph + (uint64_t)cid * a.R + j) : PANN_PAD;
+        bool seen = false;
+        if (!emu_batch(h, v, v != PANN_PAD, lane, &seen)) { full_tab = true; break; }
+        bool isnew = v != PANN_PAD && !seen && v != self;
+        unsigned mn = __ballot_sync(FULL, isnew);
+        if (isnew) nbuf[nnew + __popc(mn & ((1u << lane) - 1))] = v;
+        nnew += __popc(mn);
+      }
+      if (full_tab) {
         status |= QS_TABLE_FULL;
         break;
       }
-      nnew = __shfl_sync(FULL, nnew, 0);
       __syncwarp();
       cmps += (uint32_t)nnew;
       if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
-      for (int b = 0; b < nnew; b += 32) {
-        int i = b + lane;
-        bool keep = false;
-        uint64_t key = 0;
-        if (i < nnew) {
-          uint32_t v = nbuf[i];
-          float dd = point_dist<DT, MT>(a.points + (uint64_t)v * a.stride, qs, a.d, a.nchunks, qq);
-          keep = !(dd >= cutoff);
-          key = make_key(dd, v);
+      // two rows per lane per round: rows b+lane and b+32+lane
+      for (int b = 0; b < nnew; b += 64) {
+        const int i0 = b + lane, i1 = b + 32 + lane;
+        float d0 = 0.0f, d1 = 0.0f;
+        uint32_t v0 = 0, v1 = 0;
+        if (i0 < nnew) {
+          v0 = nbuf[i0];
+          v1 = i1 < nnew ? nbuf[i1] : 0u;
+          point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
+                              i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
+                              a.opaque_zero);
         }
-        unsigned mk = __ballot_sync(FULL, keep);
-        if (keep) cand[cn + __popc(mk & ((1u << lane) - 1))] = key;
-        cn += __popc(mk);
+        bool keep0 = i0 < nnew && !(d0 >= cutoff);
+        unsigned m0 = __ballot_sync(FULL, keep0);
+        if (keep0) cand[cn + __popc(m0 & ((1u << lane) - 1))] = make_key(d0, v0);
+        cn += __popc(m0);
+        bool keep1 = i1 < nnew && !(d1 >= cutoff);
+        unsigned m1 = __ballot_sync(FULL, keep1);
+        if (keep1) cand[cn + __popc(m1 & ((1u << lane) - 1))] = make_key(d1, v1);
+        cn += __popc(m1);
       }
       if (cn == 0 || (a.limit >= 2ull * L && (double)cn < a.batch_factor * (double)L && cnt - 1 >= 1)) continue;
       __syncwarp();

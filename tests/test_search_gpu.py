@@ -138,6 +138,27 @@ def test_hashset_growth_is_reproduced(L, bf, lib_built):
     idx.close()
 
 
+@pytest.mark.parametrize("L", [40, 50])
+def test_hashset_growth_with_repeated_neighbours(L, lib_built):
+    """Adjacency lists with repeated ids under hashset growth: the emulation
+    must reproduce the reference's duplicate handling (std::unique, set_union,
+    set_difference) exactly."""
+    base = random_points(np.uint8, 20000, 8, 5)
+    q = random_points(np.uint8, 48, 8, 6)
+    g = O.random_graph(20000, 64, 7, min_deg=60)
+    rng = np.random.default_rng(8)
+    for i in range(0, 20000, 3):          # repeat some ids inside a row
+        deg = g[i, 0]
+        g[i, 1 + rng.integers(0, deg, 4)] = g[i, 1 + rng.integers(0, deg, 4)]
+    idx = P.Index(base, 64)
+    idx.set_graph(g)
+    r = idx.search(q, 10, L, batch_factor=1.0)
+    o = O.search("oracle", base, q, g, 10, L, batch_factor=1.0)
+    assert (o["hash_grew"] > 0).sum() > 0
+    check_same(r, o)
+    idx.close()
+
+
 def test_search_edge_cases(lib_built):
     base = random_points(np.float32, 500, 7, 31)   # odd dimension: padded rows
     g = O.random_graph(500, 5, 32)
