@@ -118,6 +118,23 @@ def profiled_traffic():
         return None, None
 
 
+def max_over_ranks(seconds: float, device) -> float:
+    """The slowest rank's time (all ranks take this collective in the same order)."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return seconds
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_qps(queries_per_rank: int, steps: int, world: int, slowest_seconds: float) -> float:
+    """Whole-job throughput: every rank searches its own replica's queries."""
+    return world * queries_per_rank * steps / slowest_seconds
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -208,12 +225,8 @@ def run_ours(args):
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    t_dev = sum(times)
-    if world > 1:
-        tt = torch.tensor([t_dev], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev = float(tt.item())
-    qps = world * nq * args.steps / t_dev
+    t_dev = max_over_ranks(sum(times), dev)
+    qps = replica_qps(nq, args.steps, world, t_dev)
 
     # end-to-end through the host-buffer C-ABI call (pinned buffers, copies timed)
     hq = torch.from_numpy(q).pin_memory()
@@ -244,11 +257,7 @@ def run_ours(args):
         t = time.perf_counter()
         step_e2e()
         e2e_times.append(time.perf_counter() - t)
-    t_e2e = sum(e2e_times)
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    t_e2e = max_over_ranks(sum(e2e_times), dev)
     assert np.array_equal(h_ids.numpy().astype(np.uint32), res.ids), "e2e path differs"
 
     peak, peak_kind = measured_peak()
@@ -278,7 +287,7 @@ def run_ours(args):
                        "build_seconds_wall": round(build_wall, 3), "mean_visited": round(mean_vis, 2),
                        "mean_cmps": round(mean_cmps, 2), "flagged_queries": int(res.flags.sum()),
                        "recall_sweep": sweep},
-            "e2e": {"value": round(world * nq * args.steps / t_e2e, 1), "unit": "queries/s",
+            "e2e": {"value": round(replica_qps(nq, args.steps, world, t_e2e), 1), "unit": "queries/s",
                     "h2d_bytes_per_step": int(q.nbytes),
                     "d2h_bytes_per_step": int(nq * k * 8 + nq * 12)},
             "gpu_launches": 5 * args.steps,

@@ -1,0 +1,534 @@
+// parlayANN drop-in host API over the parlayann_b200 C ABI.
+//
+// Mirrors the reference's types and free functions for the beam-search /
+// Vamana-build path, with the same names and argument meaning, so code
+// written against ParlayANN's headers compiles against this one:
+//
+//   QueryParams, BuildParams          algorithms/utils/types.h:155-268
+//   Euclidian_Point<T>, Mips_Point<T> algorithms/utils/euclidian_point.h:92-248,
+//                                     algorithms/utils/mips_point.h:68-144
+//   PointRange<Point>                 algorithms/utils/point_range.h:43-141
+//   Graph<indexType>, edgeRange       algorithms/utils/graph.h:45-255
+//   stats<indexType>                  algorithms/utils/stats.h:120-155
+//   groundTruth<T>                    algorithms/utils/types.h:38-107
+//   beam_search, searchAll, qsearchAll algorithms/utils/beamSearch.h:420-646
+//   knn_index<PR,QPR,indexType>::build_index   algorithms/vamana/index.h:42-186
+//
+// Points and graphs live on the host as in the reference; the first search or
+// build on a (Graph, PointRange) pair uploads them to the GPU (a cached device
+// index kept with the Graph, refreshed when the graph or the points change).
+// Errors that make the reference abort() print a message and abort() here too.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "../parlayann_b200.h"
+
+namespace parlayANN {
+
+inline void pann_check(int rc, const char* where) {
+  if (rc != PANN_OK) {
+    std::cout << "ERROR in " << where << ": " << pann_last_error() << std::endl;
+    std::abort();
+  }
+}
+
+// ---------------------------------------------------------------- params
+struct QueryParams {
+  long k;
+  long beamSize;
+  long limit;
+  long degree_limit;
+  double rerank_factor = 100;
+  double batch_factor = .125;
+  QueryParams(long k, long Q, long limit, long dg, double rerank_factor = 100, double batch_factor = .125)
+      : k(k), beamSize(Q), limit(limit), degree_limit(dg), rerank_factor(rerank_factor), batch_factor(batch_factor) {}
+  QueryParams() : k(0), beamSize(0), limit(0), degree_limit(0) {}
+  pann_query_params c() const {
+    pann_query_params q;
+    q.k = (uint32_t)k;
+    q.beam = (uint32_t)beamSize;
+    q.limit = (uint64_t)limit;
+    q.degree_limit = (uint32_t)degree_limit;
+    q.batch_factor = batch_factor;
+    return q;
+  }
+};
+
+struct BuildParams {
+  long R = 0;
+  long L = 0;
+  double alpha = 1.0;
+  int num_passes = 1;
+  double rerank_factor = 100;
+  double batch_factor = 1.0;  // the reference's default for this constructor (types.h:176)
+  int single_batch = 0;
+  bool verbose = false;
+  BuildParams() {}
+  BuildParams(long R, long L, double a, int num_passes, bool verbose = false)
+      : R(R), L(L), alpha(a), num_passes(num_passes), verbose(verbose) {}
+  long max_degree() { return R; }
+};
+
+// ---------------------------------------------------------------- points
+// Host distance functions, restated from euclidian_point.h:54-90 and
+// mips_point.h:44-66 (sequential sums), for callers that score points on the host.
+template <typename T>
+inline float pann_host_distance(const T* p, const T* q, unsigned d, int metric) {
+  if constexpr (std::is_same<T, float>::value) {
+    float r = 0.0f;
+    if (metric == PANN_L2)
+      for (unsigned i = 0; i < d; i++) { float t = q[i] - p[i]; float s = t * t; r = r + s; }
+    else
+      for (unsigned i = 0; i < d; i++) { float s = q[i] * p[i]; r = r + s; }
+    return metric == PANN_L2 ? r : -r;
+  } else {
+    int32_t r = 0;
+    for (unsigned i = 0; i < d; i++) {
+      int32_t a = (int32_t)p[i], b = (int32_t)q[i];
+      r += metric == PANN_L2 ? (a - b) * (a - b) : a * b;
+    }
+    return metric == PANN_L2 ? (float)r : -((float)r);
+  }
+}
+
+template <typename T> struct pann_dtype_of;
+template <> struct pann_dtype_of<uint8_t> { static constexpr int value = PANN_U8; };
+template <> struct pann_dtype_of<int8_t> { static constexpr int value = PANN_I8; };
+template <> struct pann_dtype_of<float> { static constexpr int value = PANN_F32; };
+
+template <typename T_, int METRIC>
+struct PannPoint {
+  using T = T_;
+  using distanceType = float;
+  using byte = uint8_t;
+  static constexpr int pann_metric = METRIC;
+  static constexpr bool is_metric = METRIC == PANN_L2;
+  struct parameters {
+    int dims;
+    parameters() : dims(0) {}
+    parameters(int d) : dims(d) {}
+    int num_bytes() const { return dims * (int)sizeof(T); }
+  };
+  PannPoint() : values(nullptr), id_(-1), params(0) {}
+  PannPoint(byte* v, long id, parameters p) : values((T*)v), id_(id), params(p) {}
+  T operator[](long i) const { return values[i]; }
+  float distance(const PannPoint& x) const { return pann_host_distance(values, x.values, params.dims, METRIC); }
+  bool same_as(const PannPoint& q) const { return values == q.values; }
+  long id() const { return id_; }
+  void prefetch() const {}
+  static distanceType d_min() { return METRIC == PANN_L2 ? 0.0f : -std::numeric_limits<float>::max(); }
+  T* values;
+  long id_;
+  parameters params;
+};
+template <typename T> using Euclidian_Point = PannPoint<T, PANN_L2>;
+template <typename T> using Mips_Point = PannPoint<T, PANN_MIPS>;
+
+template <class Point_>
+struct PointRange {
+  using Point = Point_;
+  using T = typename Point::T;
+  using parameters = typename Point::parameters;
+  parameters params;
+
+  PointRange() : n(0) {}
+  // .bin file: uint32 n, uint32 d, then n*d values (point_range.h:74-117)
+  PointRange(char* filename) : n(0) {
+    if (filename == nullptr) return;
+    std::ifstream reader(filename, std::ios::binary);
+    if (!reader.is_open()) {
+      std::cout << "Data file " << filename << " not found" << std::endl;
+      std::abort();
+    }
+    uint32_t num_points = 0, d = 0;
+    reader.read((char*)&num_points, 4);
+    reader.read((char*)&d, 4);
+    n = num_points;
+    params = parameters((int)d);
+    data_ = std::make_shared<std::vector<T>>((size_t)n * d);
+    reader.read((char*)data_->data(), (std::streamsize)(sizeof(T) * (size_t)n * d));
+    if (!reader) {
+      std::cout << "Data file " << filename << " is truncated" << std::endl;
+      std::abort();
+    }
+  }
+  // from memory (copied)
+  PointRange(const T* rows, size_t num, int dims) : params(dims), n(num) {
+    data_ = std::make_shared<std::vector<T>>(rows, rows + num * (size_t)dims);
+  }
+  size_t size() const { return n; }
+  long dimension() const { return params.dims; }
+  unsigned int get_dims() const { return params.dims; }
+  Point operator[](long i) const {
+    if (i > (long)n) {
+      std::cout << "ERROR: point index out of range: " << i << " from range " << n << ", " << std::endl;
+      std::abort();
+    }
+    return Point((uint8_t*)(data_->data() + (size_t)i * params.dims), i, params);
+  }
+  const T* data() const { return data_ ? data_->data() : nullptr; }
+
+ private:
+  size_t n;
+  std::shared_ptr<std::vector<T>> data_;
+};
+
+// ---------------------------------------------------------------- graph
+struct PannDevice {
+  pann_index* idx = nullptr;
+  const void* points = nullptr;
+  int dtype = -1, metric = -1;
+  ~PannDevice() {
+    if (idx) pann_index_destroy(idx);
+  }
+};
+
+template <typename indexType>
+struct edgeRange {
+  edgeRange(indexType* row, long maxDeg, indexType id, bool* dirty) : e(row), maxDeg(maxDeg), id_(id), dirty(dirty) {}
+  size_t size() const { return e[0]; }
+  indexType id() const { return id_; }
+  indexType operator[](indexType j) const {
+    if (j > e[0]) {
+      std::cout << "ERROR: index exceeds degree while accessing neighbors" << std::endl;
+      std::abort();
+    }
+    return e[j + 1];
+  }
+  template <typename rangeType>
+  void update_neighbors(const rangeType& r) {
+    if ((long)r.size() > maxDeg) {
+      std::cout << "ERROR in update_neighbors: cannot exceed max degree " << maxDeg << std::endl;
+      std::abort();
+    }
+    e[0] = (indexType)r.size();
+    for (size_t i = 0; i < r.size(); i++) e[i + 1] = r[i];
+    *dirty = true;
+  }
+  void append_neighbor(indexType nbh) {
+    if ((long)e[0] == maxDeg) {
+      std::cout << "ERROR in append_neighbor: cannot exceed max degree " << maxDeg << std::endl;
+      std::abort();
+    }
+    e[e[0] + 1] = nbh;
+    e[0] += 1;
+    *dirty = true;
+  }
+  void clear_neighbors() {
+    e[0] = 0;
+    *dirty = true;
+  }
+  template <typename F>
+  void sort(F&& less) {
+    std::sort(e + 1, e + 1 + e[0], less);
+    *dirty = true;
+  }
+  indexType* begin() const { return e + 1; }
+  indexType* end() const { return e + 1 + e[0]; }
+  void prefetch() const {}
+
+ private:
+  indexType* e;
+  long maxDeg;
+  indexType id_;
+  bool* dirty;
+};
+
+template <typename indexType_>
+struct Graph {
+  using indexType = indexType_;
+  static_assert(sizeof(indexType) == 4, "the device graph stores 32-bit ids");
+  Graph() : n(0), maxDeg(0) {}
+  Graph(long maxDeg, size_t n) : n(n), maxDeg(maxDeg), rows(std::make_shared<std::vector<indexType>>(n * (maxDeg + 1), 0)) {}
+  // the reference's graph file (graph.h:151-208)
+  Graph(char* gFile) {
+    std::ifstream reader(gFile, std::ios::binary);
+    if (!reader.is_open()) {
+      std::cout << "graph file " << gFile << " not found" << std::endl;
+      std::abort();
+    }
+    uint32_t pre[2];
+    reader.read((char*)pre, 8);
+    n = pre[0];
+    maxDeg = pre[1];
+    rows = std::make_shared<std::vector<indexType>>(n * (maxDeg + 1), 0);
+    std::vector<uint32_t> deg(n);
+    reader.read((char*)deg.data(), 4 * (std::streamsize)n);
+    for (size_t i = 0; i < n; i++) {
+      indexType* r = rows->data() + i * (maxDeg + 1);
+      r[0] = deg[i];
+      reader.read((char*)(r + 1), 4 * (std::streamsize)deg[i]);
+    }
+    if (!reader) {
+      std::cout << "graph file " << gFile << " is truncated" << std::endl;
+      std::abort();
+    }
+  }
+  long max_degree() const { return maxDeg; }
+  size_t size() const { return n; }
+  edgeRange<indexType> operator[](indexType i) const {
+    if (i > n) {
+      std::cout << "ERROR: graph index out of range: " << i << std::endl;
+      std::abort();
+    }
+    return edgeRange<indexType>(rows->data() + (size_t)i * (maxDeg + 1), maxDeg, i, &dirty_->v);
+  }
+  // graph.h:210-237
+  void save(char* oFile) {
+    std::ofstream w(oFile, std::ios::binary);
+    uint32_t pre[2] = {(uint32_t)n, (uint32_t)maxDeg};
+    w.write((char*)pre, 8);
+    for (size_t i = 0; i < n; i++) w.write((char*)(rows->data() + i * (maxDeg + 1)), 4);
+    for (size_t i = 0; i < n; i++) {
+      const indexType* r = rows->data() + i * (maxDeg + 1);
+      w.write((char*)(r + 1), 4 * (std::streamsize)r[0]);
+    }
+  }
+  const indexType* raw_rows() const { return rows->data(); }
+  indexType* raw_rows() { return rows->data(); }
+
+  // device mirror of (this graph, the given points)
+  template <class PR>
+  pann_index* device(const PR& Points) const {
+    using P = typename PR::Point;
+    const int dt = pann_dtype_of<typename P::T>::value, mt = P::pann_metric;
+    PannDevice& d = *dev_;
+    if (!d.idx || d.points != (const void*)Points.data() || d.dtype != dt || d.metric != mt) {
+      if (d.idx) pann_index_destroy(d.idx);
+      d.idx = nullptr;
+      pann_check(pann_index_create(&d.idx, dt, mt, n, (uint32_t)Points.dimension(), (uint32_t)maxDeg),
+                 "pann_index_create");
+      pann_check(pann_index_set_points(d.idx, Points.data(), 0), "pann_index_set_points");
+      d.points = Points.data();
+      d.dtype = dt;
+      d.metric = mt;
+      dirty_->v = true;
+    }
+    if (dirty_->v) {
+      pann_check(pann_graph_upload(d.idx, (const uint32_t*)rows->data(), 0), "pann_graph_upload");
+      dirty_->v = false;
+    }
+    return d.idx;
+  }
+  void pull_from_device() {
+    pann_check(pann_graph_download(dev_->idx, (uint32_t*)rows->data()), "pann_graph_download");
+    dirty_->v = false;
+  }
+
+ private:
+  struct Flag { bool v = true; };
+  size_t n;
+  long maxDeg;
+  std::shared_ptr<std::vector<indexType>> rows;
+  std::shared_ptr<PannDevice> dev_ = std::make_shared<PannDevice>();
+  std::shared_ptr<Flag> dirty_ = std::make_shared<Flag>();
+};
+
+// ---------------------------------------------------------------- stats, groundtruth
+template <typename indexType>
+struct stats {
+  stats() {}
+  stats(size_t n) : visited(n, 0), distances(n, 0) {}
+  std::vector<indexType> visited;
+  std::vector<indexType> distances;
+  void increment_dist(indexType i, indexType j) { distances[i] += j; }
+  void increment_visited(indexType i, indexType j) { visited[i] += j; }
+  std::vector<indexType> visited_stats() { return statistics(visited); }
+  std::vector<indexType> dist_stats() { return statistics(distances); }
+  void clear() {
+    std::fill(visited.begin(), visited.end(), 0);
+    std::fill(distances.begin(), distances.end(), 0);
+  }
+  // mean and the 0.99 quantile (stats.h:147-153)
+  static std::vector<indexType> statistics(std::vector<indexType> s) {
+    long sum = 0;
+    for (auto x : s) sum += (long)x;
+    indexType avg = (indexType)(sum / (long)s.size());
+    std::sort(s.begin(), s.end());
+    indexType tail = s[(size_t)(.99 * ((float)s.size()))];
+    return {avg, tail};
+  }
+};
+
+// .ibin groundtruth: int32 n, int32 k, ids[n*k], float dists[n*k] (types.h:38-107)
+template <typename T>
+struct groundTruth {
+  std::vector<T> coords;
+  std::vector<float> dists;
+  long dim = 0;
+  size_t n = 0;
+  groundTruth() {}
+  groundTruth(char* gtFile) {
+    if (!gtFile) return;
+    std::ifstream r(gtFile, std::ios::binary);
+    if (!r.is_open()) {
+      std::cout << "groundtruth file " << gtFile << " not found" << std::endl;
+      std::abort();
+    }
+    int32_t pre[2];
+    r.read((char*)pre, 8);
+    n = pre[0];
+    dim = pre[1];
+    coords.resize(n * dim);
+    dists.resize(n * dim);
+    r.read((char*)coords.data(), sizeof(T) * n * dim);
+    r.read((char*)dists.data(), 4 * n * dim);
+  }
+  T coordinates(long i, long j) const { return coords[i * dim + j]; }
+  float distances(long i, long j) const { return dists[i * dim + j]; }
+  size_t size() const { return n; }
+  long dimension() const { return dim; }
+};
+
+// ---------------------------------------------------------------- search
+template <typename indexType>
+using pann_pairs = std::vector<std::pair<indexType, float>>;
+
+// beam_search (beamSearch.h:420-427): ((frontier, visited), full_dist_cmps)
+template <typename Point, typename PointRange_, typename indexType>
+std::pair<std::pair<pann_pairs<indexType>, pann_pairs<indexType>>, size_t>
+beam_search(const Point p, const Graph<indexType>& G, const PointRange_& Points,
+            const std::vector<indexType> starting_points, const QueryParams& QP) {
+  pann_index* idx = G.device(Points);
+  pann_query_params q = QP.c();
+  const uint32_t L = (uint32_t)QP.beamSize;
+  uint32_t vcap = 4 * L + 256;
+  for (;;) {
+    std::vector<uint32_t> fi(L), vi(vcap);
+    std::vector<float> fd(L), vd(vcap);
+    uint32_t fn = 0, vn = 0, cm = 0;
+    std::vector<uint32_t> st(starting_points.begin(), starting_points.end());
+    int rc = pann_search_lists(idx, p.values, 1, &q, st.data(), (uint32_t)st.size(), fi.data(), fd.data(), &fn, vcap,
+                               vi.data(), vd.data(), &vn, &cm);
+    if (rc == PANN_EOVERFLOW && vcap < (1u << 24)) {
+      vcap *= 4;
+      continue;
+    }
+    pann_check(rc, "beam_search");
+    pann_pairs<indexType> fr, vis;
+    for (uint32_t j = 0; j < fn; j++) fr.push_back({fi[j], fd[j]});
+    for (uint32_t j = 0; j < vn; j++) vis.push_back({vi[j], vd[j]});
+    return {{fr, vis}, (size_t)cm};
+  }
+}
+
+template <typename Point, typename PointRange_, typename indexType>
+std::pair<std::pair<pann_pairs<indexType>, pann_pairs<indexType>>, size_t>
+beam_search(const Point p, const Graph<indexType>& G, const PointRange_& Points, const indexType starting_point,
+            const QueryParams& QP) {
+  return beam_search(p, G, Points, std::vector<indexType>{starting_point}, QP);
+}
+
+template <typename PointRange_, typename indexType>
+std::vector<std::vector<indexType>> pann_batch(const PointRange_& Query_Points, const Graph<indexType>& G,
+                                               const PointRange_& Base_Points, stats<indexType>& QueryStats,
+                                               const std::vector<indexType>& starts, const QueryParams& QP,
+                                               const char* who) {
+  if (QP.k > QP.beamSize) {
+    std::cout << "Error: beam search parameter Q = " << QP.beamSize << " same size or smaller than k = " << QP.k
+              << std::endl;
+    std::abort();
+  }
+  pann_index* idx = G.device(Base_Points);
+  pann_query_params q = QP.c();
+  const size_t nq = Query_Points.size(), k = (size_t)QP.k;
+  std::vector<uint32_t> ids(nq * k), vis(nq), cmps(nq);
+  std::vector<uint32_t> st(starts.begin(), starts.end());
+  pann_check(pann_search(idx, Query_Points.data(), (uint32_t)nq, &q, st.data(), (uint32_t)st.size(), ids.data(),
+                         nullptr, vis.data(), cmps.data(), nullptr),
+             who);
+  std::vector<std::vector<indexType>> out(nq);
+  for (size_t i = 0; i < nq; i++) {
+    out[i].assign(ids.begin() + i * k, ids.begin() + (i + 1) * k);
+    if (QueryStats.visited.size() == nq) {
+      QueryStats.increment_visited((indexType)i, vis[i]);
+      QueryStats.increment_dist((indexType)i, cmps[i]);
+    }
+  }
+  return out;
+}
+
+// searchAll (beamSearch.h:492-526)
+template <typename PointRange_, typename indexType>
+std::vector<std::vector<indexType>> searchAll(PointRange_& Query_Points, Graph<indexType>& G,
+                                              PointRange_& Base_Points, stats<indexType>& QueryStats,
+                                              std::vector<indexType> starting_points, QueryParams& QP) {
+  return pann_batch(Query_Points, G, Base_Points, QueryStats, starting_points, QP, "searchAll");
+}
+template <typename PointRange_, typename indexType>
+std::vector<std::vector<indexType>> searchAll(PointRange_& Query_Points, Graph<indexType>& G,
+                                              PointRange_& Base_Points, stats<indexType>& QueryStats,
+                                              indexType starting_point, QueryParams& QP) {
+  return pann_batch(Query_Points, G, Base_Points, QueryStats, std::vector<indexType>{starting_point}, QP, "searchAll");
+}
+
+// qsearchAll (beamSearch.h:599-646) without quantization: the three point
+// ranges must be the same (the quantized two-level search is not offered).
+template <typename PR, typename QPR, typename QQPR, typename indexType>
+std::vector<std::vector<indexType>> qsearchAll(const PR& Query_Points, const QPR& Q_Query_Points,
+                                               const QQPR& QQ_Query_Points, const Graph<indexType>& G,
+                                               const PR& Base_Points, const QPR& Q_Base_Points,
+                                               const QQPR& QQ_Base_Points, stats<indexType>& QueryStats,
+                                               const indexType starting_point, const QueryParams& QP,
+                                               bool random = false) {
+  if ((const void*)&Q_Base_Points != (const void*)&Base_Points ||
+      (const void*)&QQ_Base_Points != (const void*)&Base_Points || random) {
+    std::cout << "ERROR: qsearchAll supports the unquantized search from a fixed start point" << std::endl;
+    std::abort();
+  }
+  (void)Q_Query_Points;
+  (void)QQ_Query_Points;
+  return pann_batch(Query_Points, G, Base_Points, QueryStats, std::vector<indexType>{starting_point}, QP,
+                    "qsearchAll");
+}
+
+// ---------------------------------------------------------------- build
+template <typename PointRange_, typename QPointRange, typename indexType>
+struct knn_index {
+  BuildParams BP;
+  indexType start_point = 0;
+  knn_index(BuildParams& BP) : BP(BP) {}
+  indexType get_start() { return start_point; }
+  void set_start() { start_point = 0; }
+  // build_index (index.h:150-186): batch insertion with prefix doubling, on the GPU
+  void build_index(Graph<indexType>& G, PointRange_& Points, QPointRange& QPoints, stats<indexType>& BuildStats,
+                   bool sort_neighbors = true) {
+    (void)QPoints;
+    set_start();
+    if (BP.single_batch != 0) {
+      std::cout << "ERROR: single_batch builds are not offered" << std::endl;
+      std::abort();
+    }
+    pann_index* idx = G.device(Points);
+    pann_build_params bp;
+    bp.R = (uint32_t)BP.R;
+    bp.L = (uint32_t)BP.L;
+    bp.alpha = BP.alpha;
+    bp.num_passes = BP.num_passes;
+    bp.batch_factor = BP.batch_factor;
+    bp.perm_seed = 0x5EED5EED5EEDull;
+    bp.sort_neighbors = sort_neighbors ? 1 : 0;
+    pann_build_stats st;
+    pann_check(pann_build(idx, &bp, nullptr, &st), "build_index");
+    G.pull_from_device();
+    if (BP.verbose)
+      std::cout << "build: " << st.seconds << " s (search " << st.search_seconds << ", prune " << st.prune_seconds
+                << ", reverse " << st.reverse_seconds << "), " << st.batches << " batches" << std::endl;
+    (void)BuildStats;
+  }
+};
+
+}  // namespace parlayANN

@@ -124,6 +124,18 @@ int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, cons
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
                        uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
 
+/* Beam search returning the reference's full per-query output: the final
+ * frontier (<= beam entries, sorted by (distance, id)) and the visited list
+ * (sorted by (distance, id)), as filtered_beam_search returns them
+ * (beamSearch.h:225-227), plus full_dist_cmps. Host buffers:
+ * frontier_ids/frontier_d nq x beam, visited_ids/visited_d nq x visited_cap.
+ * A query that visits more than visited_cap nodes fails with PANN_EOVERFLOW.
+ * Replaces beam_search / filtered_beam_search (beamSearch.h:33-228,420-445). */
+int pann_search_lists(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                      const uint32_t* starts, uint32_t n_start, uint32_t* frontier_ids, float* frontier_d,
+                      uint32_t* frontier_n, uint32_t visited_cap, uint32_t* visited_ids, float* visited_d,
+                      uint32_t* visited_n, uint32_t* out_cmps);
+
 /* ---------------------------------------------------------------- build */
 
 /* Vamana batch-insertion build into the index's graph (knn_index::build_index,

@@ -87,6 +87,8 @@ SIGNATURES = {
     "pann_graph_save": (_I, [_P, ctypes.c_char_p]),
     "pann_search": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P]),
     "pann_search_device": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P, _P]),
+    "pann_search_lists": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _U32, _P, _P, _P,
+                               _P]),
     "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
     "pann_groundtruth": (_I, [_P, _P, _U32, _U32, _P, _P]),
     "pann_last_error": (ctypes.c_char_p, []),
@@ -244,6 +246,26 @@ class Index:
         if not (allow_short and rc == PANN_ESHORT):
             _check(rc)
         return SearchResult(ids, dists, vis, cmps, flags)
+
+    def search_lists(self, queries: np.ndarray, L: int, limit: int | None = None, degree_limit: int | None = None,
+                     batch_factor: float = 0.125, starts=(0,), visited_cap: int | None = None):
+        """Full beam_search output: frontier (<= L) and sorted visited list per query."""
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        nq = queries.shape[0]
+        vc = visited_cap or 4 * L + 64
+        qp = QueryParams(L, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
+                         batch_factor)
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+        fi = np.zeros((nq, L), np.uint32)
+        fd = np.zeros((nq, L), np.float32)
+        fn = np.zeros(nq, np.uint32)
+        vi = np.zeros((nq, vc), np.uint32)
+        vd = np.zeros((nq, vc), np.float32)
+        vn = np.zeros(nq, np.uint32)
+        cm = np.zeros(nq, np.uint32)
+        _check(lib().pann_search_lists(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(fi),
+                                       _ptr(fd), _ptr(fn), vc, _ptr(vi), _ptr(vd), _ptr(vn), _ptr(cm)))
+        return dict(frontier_ids=fi, frontier_d=fd, frontier_n=fn, visited_ids=vi, visited_d=vd, visited=vn, cmps=cm)
 
     def groundtruth(self, queries: np.ndarray, k: int):
         queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])

@@ -619,4 +619,70 @@ int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_qu
   return summarize_status(status.data(), nq, out_flags);
 }
 
+int pann_search_lists(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                      const uint32_t* starts, uint32_t n_start, uint32_t* frontier_ids, float* frontier_d,
+                      uint32_t* frontier_n, uint32_t visited_cap, uint32_t* visited_ids, float* visited_d,
+                      uint32_t* visited_n, uint32_t* out_cmps) {
+  int rc = check_index(idx, true);
+  if (rc) return rc;
+  if (nq && (!queries || !frontier_ids || !frontier_n || !visited_n)) return fail(PANN_EINVAL, "NULL output buffer");
+  if (visited_cap && (!visited_ids || !visited_d)) return fail(PANN_EINVAL, "NULL visited buffer");
+  if (!qp) return fail(PANN_EINVAL, "query params are NULL");
+  pann_query_params q2 = *qp;
+  q2.k = qp->beam;  // the whole frontier
+  SearchPlan plan;
+  rc = make_plan(idx, &q2, n_start, &plan);
+  if (rc) return rc;
+  if (nq == 0) return PANN_OK;
+  cudaStream_t st = idx->stream;
+  rc = stage_starts(idx, starts, n_start, st);
+  if (rc) return rc;
+  const size_t L = plan.L, vc = std::max<uint32_t>(visited_cap, 1);
+  size_t rb = (size_t)idx->d * idx->esize;
+  PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
+  PANN_CUDA(idx->ids.ensure(4 * L * nq));
+  PANN_CUDA(idx->dists.ensure(4 * L * nq));
+  PANN_CUDA(idx->vis.ensure(4 * (size_t)nq));
+  PANN_CUDA(idx->cmps.ensure(4 * (size_t)nq));
+  PANN_CUDA(idx->status.ensure(4 * (size_t)nq));
+  PANN_CUDA(idx->tmp.ensure(8 * vc * nq));
+  if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(idx->q.p, 0, idx->stride * (size_t)nq, st));
+  PANN_CUDA(cudaMemcpy2DAsync(idx->q.p, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
+  rc = run_search(idx, plan, idx->q.as<uint8_t>(), nullptr, nq, idx->starts.as<uint32_t>(), idx->ids.as<uint32_t>(),
+                  idx->dists.as<float>(), idx->vis.as<uint32_t>(), idx->cmps.as<uint32_t>(),
+                  idx->status.as<uint32_t>(), idx->tmp.as<uint64_t>(), (uint32_t)vc, st);
+  if (rc) return rc;
+  std::vector<uint32_t> fid(L * nq), status(nq), vn(nq);
+  std::vector<float> fd(L * nq);
+  std::vector<uint64_t> vk(vc * nq);
+  PANN_CUDA(cudaMemcpyAsync(fid.data(), idx->ids.p, 4 * L * nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(fd.data(), idx->dists.p, 4 * L * nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(vn.data(), idx->vis.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(status.data(), idx->status.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(vk.data(), idx->tmp.p, 8 * vc * nq, cudaMemcpyDeviceToHost, st));
+  if (out_cmps) PANN_CUDA(cudaMemcpyAsync(out_cmps, idx->cmps.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < nq; i++) {
+    if (status[i] & (QS_TABLE_FULL | QS_INTERNAL)) return fail(PANN_EOVERFLOW, "a query's seen-set outgrew the largest table");
+    if (vn[i] > visited_cap) return fail(PANN_EOVERFLOW, "a query visited more nodes than visited_cap");
+    uint32_t fn = 0;
+    for (size_t j = 0; j < L; j++) {
+      uint32_t id = fid[i * L + j];
+      frontier_ids[i * L + j] = id;
+      frontier_d[i * L + j] = fd[i * L + j];
+      if (id != PANN_PAD) fn = (uint32_t)j + 1;
+    }
+    frontier_n[i] = fn;
+    visited_n[i] = vn[i];
+    // the reference keeps `visited` sorted by (distance, id) (beamSearch.h:125-126)
+    uint64_t* v = &vk[(size_t)i * vc];
+    std::sort(v, v + vn[i]);
+    for (uint32_t j = 0; j < vn[i]; j++) {
+      visited_ids[(size_t)i * visited_cap + j] = key_id(v[j]);
+      visited_d[(size_t)i * visited_cap + j] = key_dist(v[j]);
+    }
+  }
+  return PANN_OK;
+}
+
 }  // extern "C"

@@ -1,0 +1,58 @@
+// A ParlayANN-style program (the shape of neighborsTime.C + ANN_Quantized:
+// build a Vamana index, save/load the graph, search, check recall) written
+// against include/parlayANN/parlayann.hpp. Exit status 0 when recall@10 of
+// qsearchAll is >= 0.9 and beam_search agrees with qsearchAll.
+#include <cstdio>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "parlayANN/parlayann.hpp"
+
+using namespace parlayANN;
+
+int main(int argc, char** argv) {
+  std::string graph_path = argc > 1 ? argv[1] : "/tmp/pann_dropin.graph";
+  const size_t n = 20000, nq = 200;
+  const int d = 32;
+  std::vector<uint8_t> base(n * d), q(nq * d);
+  pann_check(pann_synth_mixture(PANN_U8, n, d, 16, 0, 0, 32.0, 224.0, 20.0, 0, base.data()), "synth");
+  pann_check(pann_synth_mixture(PANN_U8, nq, d, 16, 0, 1, 32.0, 224.0, 20.0, 0, q.data()), "synth");
+  using Point = Euclidian_Point<uint8_t>;
+  using PR = PointRange<Point>;
+  PR Points(base.data(), n, d), Query_Points(q.data(), nq, d);
+
+  Graph<unsigned int> G(32, n);
+  BuildParams BP(32, 64, 1.2, 2);
+  BP.batch_factor = .125;
+  knn_index<PR, PR, unsigned int> I(BP);
+  stats<unsigned int> BuildStats(n);
+  I.build_index(G, Points, Points, BuildStats);
+  G.save((char*)graph_path.c_str());
+  Graph<unsigned int> G2((char*)graph_path.c_str());
+
+  QueryParams QP(10, 64, (long)n, 32, 10, .125);
+  stats<unsigned int> QueryStats(nq);
+  auto all = qsearchAll(Query_Points, Query_Points, Query_Points, G2, Points, Points, Points, QueryStats, 0u, QP);
+
+  // recall@10 against an exact host scan
+  long hit = 0;
+  for (size_t i = 0; i < nq; i++) {
+    std::vector<std::pair<float, unsigned>> ds;
+    for (size_t j = 0; j < n; j++) ds.push_back({Query_Points[i].distance(Points[j]), (unsigned)j});
+    std::partial_sort(ds.begin(), ds.begin() + 10, ds.end());
+    std::set<unsigned> truth;
+    for (int t = 0; t < 10; t++) truth.insert(ds[t].second);
+    for (auto id : all[i]) hit += truth.count(id);
+  }
+  double recall = hit / (10.0 * nq);
+  auto vs = QueryStats.visited_stats(), cs = QueryStats.dist_stats();
+
+  // single-query beam_search agrees with the batch
+  auto [lists, cmps] = beam_search(Query_Points[0], G2, Points, std::vector<unsigned int>{0u}, QP);
+  bool same = lists.first.size() >= 10 && cmps == QueryStats.distances[0] && lists.second.size() == QueryStats.visited[0];
+  for (int t = 0; t < 10 && same; t++) same = lists.first[t].first == all[0][t];
+  std::printf("recall@10 %.4f  visited avg %u p99 %u  cmps avg %u p99 %u  beam_search agrees %d\n", recall, vs[0], vs[1],
+              cs[0], cs[1], (int)same);
+  return (recall >= 0.9 && same) ? 0 : 1;
+}

@@ -78,6 +78,32 @@ def test_search_matches_golden(path, lib_built):
     idx.close()
 
 
+@pytest.mark.parametrize("dtype,metric", [(np.uint8, P.L2), (np.float32, P.MIPS), (np.int8, P.L2)])
+def test_search_lists_match_oracle(dtype, metric, lib_built):
+    """Full beam_search output (frontier and sorted visited list), as
+    filtered_beam_search returns it (beamSearch.h:225-227)."""
+    base = random_points(dtype, 2000, 24, 91)
+    q = random_points(dtype, 60, 24, 92)
+    g = O.random_graph(2000, 12, 93)
+    idx = P.Index(base, 12, metric)
+    idx.set_graph(g)
+    for (L, lim, bf, st) in [(20, None, 0.125, (0,)), (8, 12, 0.5, (1, 2)), (40, None, 1.0, (5,))]:
+        r = idx.search_lists(q, L, limit=lim, batch_factor=bf, starts=st, visited_cap=512)
+        o = O.search("oracle", base, q, g, 1, L, limit=lim, batch_factor=bf, starts=st, metric=metric, full=True,
+                     visited_cap=512)
+        np.testing.assert_array_equal(r["frontier_n"], o["frontier_n"])
+        np.testing.assert_array_equal(r["visited"], o["visited"])
+        np.testing.assert_array_equal(r["cmps"], o["cmps"])
+        for i in range(q.shape[0]):
+            f = int(o["frontier_n"][i])
+            np.testing.assert_array_equal(r["frontier_ids"][i, :f], o["frontier_ids"][i, :f])
+            np.testing.assert_array_equal(r["frontier_d"][i, :f], o["frontier_d"][i, :f])
+            v = int(o["visited"][i])
+            np.testing.assert_array_equal(r["visited_ids"][i, :v], o["visited_ids"][i, :v])
+            np.testing.assert_array_equal(r["visited_d"][i, :v], o["visited_d"][i, :v])
+    idx.close()
+
+
 def test_search_vamana_graph_u8(lib_built):
     """A Vamana graph on a seeded uint8 mixture (the reference's own build
     restated by the oracle), queried across beams."""
