@@ -200,14 +200,17 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   if (nq == 0) return PANN_OK;
   // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
   // [5] shared-memory emulation job counter, [6] emulation list length,
-  // [7] global emulation job counter, [8] emulation overflow count
+  // [7] global emulation job counter, [8] emulation overflow count,
+  // [9] resume records taken
   PANN_CUDA(idx->counters.ensure(64));
-  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 4 * (size_t)nq));
+  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)nq));
   uint32_t* cnt = idx->counters.as<uint32_t>();
   uint32_t* redo0 = idx->redo.as<uint32_t>();
   uint32_t* redo1 = redo0 + nq;
   uint32_t* emu = redo1 + nq;
   uint32_t* ovf = emu + nq;
+  uint32_t* emu_rec = ovf + nq;
+  uint32_t* ovf_rec = emu_rec + nq;
   PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
 
   SearchArgs a{};
@@ -237,6 +240,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.vis_keys = d_vis_keys;
   a.vis_cap = vis_cap;
   a.emu_list = emu;
+  a.emu_rec = emu_rec;
   a.emu_count = cnt + 6;
 
   const size_t smem_cap = idx->smem_optin;
@@ -265,6 +269,30 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     t.job_counter = cnt + 0;
     t.redo_list = redo0;
     t.redo_count = cnt + 3;
+    // hand-off buffers: per-warp insertion/visit logs and the resume records
+    {
+      const uint32_t logcap = plan.ref_half;
+      const uint32_t viscap = pow2_at_least(8ull * plan.L + 64);
+      const ResumeLayout ly = resume_layout(plan.L, plan.Ccap, logcap, viscap);
+      uint64_t rec_cap = std::min<uint64_t>(nq, std::max<uint64_t>(64, (256ull << 20) / (4ull * ly.words)));
+      size_t need = 4ull * (slots * (size_t)(logcap + viscap) + rec_cap * ly.words);
+      if (idx->handoff.ensure(need) == cudaSuccess) {
+        t.inslog = idx->handoff.as<uint32_t>();
+        t.logcap = logcap;
+        t.vislog = t.inslog + slots * (size_t)logcap;
+        t.viscap = viscap;
+        t.rec_pool = t.vislog + slots * (size_t)viscap;
+        t.rec_cap = (uint32_t)rec_cap;
+        t.rec_words = ly.words;
+        t.rec_count = cnt + 9;
+        a.logcap = logcap;  // the emulation tiers read the record layout
+        a.viscap = viscap;
+        a.rec_pool = t.rec_pool;
+        a.rec_words = ly.words;
+      } else {
+        cudaGetLastError();
+      }
+    }
     if (idx->gtables.ensure(slots * Sg * 4) == cudaSuccess) {
       t.gspill = idx->gtables.as<uint32_t>();
       t.Sg = Sg;
@@ -287,6 +315,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     t.S = S;
     t.warp_bytes = wb;
     t.gtables = idx->gtables2.as<uint32_t>();
+    t.inslog = nullptr;
     t.job_list = redo0;
     t.njobs_dev = cnt + 3;
     t.job_counter = cnt + 2;
@@ -315,16 +344,20 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     size_t smem_need = emu_smem_bytes(base, vs, (uint32_t)(4 * S0), (uint32_t)(2 * S0), true);
     const uint32_t* glist = emu;
     uint32_t* gcount = cnt + 6;
+    const uint32_t* grec = emu_rec;
     if (smem_need <= smem_cap && 4 * S0 < (1ull << 31)) {
       e.capA = (uint32_t)(4 * S0);
       e.capB = (uint32_t)(2 * S0);
       e.overflow_list = ovf;
+      e.overflow_rec = ovf_rec;
       e.overflow_count = cnt + 8;
+      e.job_rec = emu_rec;
       t.job_list = emu;
       t.njobs_dev = cnt + 6;
       t.job_counter = cnt + 5;
       PANN_CUDA(launch_emulate(idx->dtype, idx->metric, true, t, e, 2 * idx->sm_count, smem_need, st));
       glist = ovf;
+      grec = ovf_rec;
       gcount = cnt + 8;
     }
     uint64_t capA = 16 * S0, capB = 8 * S0;
@@ -336,7 +369,9 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     e.capA = (uint32_t)capA;
     e.capB = (uint32_t)capB;
     e.overflow_list = nullptr;
+    e.overflow_rec = nullptr;
     e.overflow_count = nullptr;
+    e.job_rec = grec;
     t.job_list = glist;
     t.njobs_dev = gcount;
     t.job_counter = cnt + 7;
@@ -442,7 +477,8 @@ int pann_index_destroy(pann_index* idx) {
   if (idx->d_points) cudaFree(idx->d_points);
   if (idx->d_graph) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
-                    &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->starts, &idx->tmp})
+                    &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->handoff, &idx->starts,
+                    &idx->tmp})
     b->release();
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;

@@ -206,9 +206,11 @@ __device__ __forceinline__ float dist_f32_row(const float4* __restrict__ row, co
 // two dependency chains overlap. rowB may be null (then db is not written).
 // Loads go in batches of PAIR_CHUNKS 16-byte chunks per row (the rows' other
 // lines are prefetched into L2 first), which keeps the register footprint
-// small enough for five resident 128-thread blocks per SM.
-constexpr int PAIR_CHUNKS = 4;
-template <int DT, int MT>
+// within the 168-register budget of three resident 128-thread blocks per SM
+// (the shared-memory seen tables allow three anyway); measured faster than
+// 4-chunk batches at four blocks and than 12- or 24-chunk batches, which spill.
+constexpr int PAIR_CHUNKS = 8;
+template <int DT, int MT, int CH = PAIR_CHUNKS>
 __device__ __forceinline__ void point_dist2(const uint8_t* __restrict__ rowA, const uint8_t* __restrict__ rowB,
                                             const uint8_t* qs, int nchunks, int32_t qq, float& da, float& db,
                                             uint64_t opq) {
@@ -220,16 +222,16 @@ __device__ __forceinline__ void point_dist2(const uint8_t* __restrict__ rowA, co
   if (DT == DT_F32) {
     const float4* q = reinterpret_cast<const float4*>(qs);
     uint64_t r = 0;  // two +0.0f
-    for (int c0 = 0; c0 < nchunks; c0 += PAIR_CHUNKS) {
-      float4 ba[PAIR_CHUNKS], bb[PAIR_CHUNKS];
+    for (int c0 = 0; c0 < nchunks; c0 += CH) {
+      float4 ba[CH], bb[CH];
 #pragma unroll
-      for (int c = 0; c < PAIR_CHUNKS; c++)
+      for (int c = 0; c < CH; c++)
         if (c0 + c < nchunks) {
           ba[c] = __ldg(reinterpret_cast<const float4*>(ra) + c0 + c);
           bb[c] = two ? __ldg(reinterpret_cast<const float4*>(rb) + c0 + c) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
-      for (int c = 0; c < PAIR_CHUNKS; c++)
+      for (int c = 0; c < CH; c++)
         if (c0 + c < nchunks) r = f32_chunk2<MT>(r, ba[c], bb[c], q[c0 + c], opq);
     }
     const float rx = __uint_as_float((uint32_t)r), ry = __uint_as_float((uint32_t)(r >> 32));
@@ -238,16 +240,16 @@ __device__ __forceinline__ void point_dist2(const uint8_t* __restrict__ rowA, co
   } else {
     const uint4* q = reinterpret_cast<const uint4*>(qs);
     int32_t pa = 0, qa = 0, pb = 0, qb = 0;
-    for (int c0 = 0; c0 < nchunks; c0 += PAIR_CHUNKS) {
-      uint4 ba[PAIR_CHUNKS], bb[PAIR_CHUNKS];
+    for (int c0 = 0; c0 < nchunks; c0 += CH) {
+      uint4 ba[CH], bb[CH];
 #pragma unroll
-      for (int c = 0; c < PAIR_CHUNKS; c++)
+      for (int c = 0; c < CH; c++)
         if (c0 + c < nchunks) {
           ba[c] = __ldg(ra + c0 + c);
           if (two) bb[c] = __ldg(rb + c0 + c);
         }
 #pragma unroll
-      for (int c = 0; c < PAIR_CHUNKS; c++)
+      for (int c = 0; c < CH; c++)
         if (c0 + c < nchunks) {
           uint4 qc = q[c0 + c];
           int_chunk<DT, MT>(ba[c], qc, qa, pa);

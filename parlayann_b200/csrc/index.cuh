@@ -55,7 +55,7 @@ struct pann_index {
   bool points_set = false;
   cudaStream_t stream = nullptr;
   // search scratch
-  pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, gtables2, emu, starts, tmp;
+  pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, gtables2, emu, handoff, starts, tmp;
   uint32_t starts_cached_n = 0;
   uint32_t starts_cached[64] = {};
 };

@@ -67,9 +67,38 @@ struct SearchArgs {
   uint32_t* redo_list;  // queries whose seen table filled up
   uint32_t* redo_count;
   uint32_t* emu_list;   // queries on which the reference's hashset would grow
+  uint32_t* emu_rec;    // per emu_list entry: resume record index, or PAD to re-run from scratch
   uint32_t* emu_count;
   uint64_t opaque_zero;  // always 0; see f32_chunk2
+  // Hand-off to the emulation tier. Before the visit in which a query could
+  // push the reference's seen-set past its growth threshold, tier 0 stops the
+  // query and saves its exact state in a resume record; the emulation tier
+  // rebuilds the reference's table from the insertion log and continues.
+  uint32_t* inslog;     // per resident warp: logcap ids, inserted in call order
+  uint32_t logcap;
+  uint32_t* vislog;     // per resident warp: viscap visited ids, in visit order
+  uint32_t viscap;
+  uint32_t* rec_pool;   // rec_cap records of rec_words words (layout: resume_layout)
+  uint32_t rec_cap;
+  uint32_t rec_words;
+  uint32_t* rec_count;
 };
+
+// Resume record: 8-word header (query, fn, cn, visits, cmps, entries), the
+// frontier (2L words), the candidates (2 Ccap words), the insertion log
+// (logcap words) and the visited ids (viscap words).
+struct ResumeLayout {
+  uint32_t fr, cand, log, vis, words;
+};
+__host__ __device__ inline ResumeLayout resume_layout(uint32_t L, uint32_t Ccap, uint32_t logcap, uint32_t viscap) {
+  ResumeLayout r;
+  r.fr = 8;
+  r.cand = r.fr + 2 * L;
+  r.log = r.cand + 2 * Ccap;
+  r.vis = r.log + logcap;
+  r.words = (r.vis + viscap + 3) & ~3u;
+  return r;
+}
 
 __host__ __device__ inline uint32_t search_warp_bytes(uint64_t stride, uint32_t L, uint32_t Ccap, uint32_t R,
                                                       uint32_t S, bool table_global) {
@@ -144,7 +173,7 @@ __device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint
 }
 
 template <int DT, int MT, bool TABLE_GLOBAL>
-__global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
+__global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -171,6 +200,9 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
   const uint32_t spill_limit = (a.Sg >> 2) * 3;
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
   const uint32_t L = a.L;
+  const bool handoff = a.inslog != nullptr && a.emu_list != nullptr;
+  uint32_t* const wlog = handoff ? a.inslog + ((size_t)blockIdx.x * wpb + warp) * a.logcap : nullptr;
+  uint32_t* const wvis = handoff ? a.vislog + ((size_t)blockIdx.x * wpb + warp) * a.viscap : nullptr;
 
   for (;;) {
     uint32_t job = 0;
@@ -198,6 +230,7 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
       float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
       frB[s] = make_key(dd, id);
       table_insert(table, mask, id);
+      if (handoff) wlog[s] = id;
     }
     __syncwarp();
     uint64_t* fr = frA;
@@ -212,6 +245,8 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
     uint32_t cmps = a.n_start;
     uint64_t nvis = 0;
     uint32_t status = 0;
+    bool hand_over = false;
+    const uint32_t nel = a.dl < a.R ? a.dl : a.R;
 
     for (;;) {
       __syncwarp();
@@ -230,6 +265,12 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
       }
       if (first >= 0) cnt += 1;
       if (first < 0 || nvis >= a.limit) break;  // :116
+      if (handoff && entries + nel > a.ref_half) {
+        // this visit could cross the reference's growth threshold
+        status |= QS_REF_WOULD_GROW;
+        hand_over = true;
+        break;
+      }
       const uint64_t cur = fr[first];
       // the next node to expand is most often the following unvisited entry:
       // start its adjacency row on its way to L2
@@ -245,9 +286,9 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
       const bool full = (fn == (int)L);
       const float cutoff = full ? key_dist(fr[fn - 1]) : 3.40282346638528859812e+38F;  // :173-175
       const uint32_t cid = key_id(cur);
+      if (handoff && lane == 0 && nvis <= a.viscap) wvis[nvis - 1] = cid;
 
       // neighbours not seen before (:151-160), compacted into nbuf
-      const uint32_t nel = a.dl < a.R ? a.dl : a.R;
       const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
       if (!spilled && entries_sh + nel > table_limit) {
         if (!spill) { status |= QS_TABLE_FULL; break; }
@@ -272,6 +313,7 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
         bool isnew = inserted && (v != self);
         unsigned mi = __ballot_sync(FULL, inserted);
         unsigned mn = __ballot_sync(FULL, isnew);
+        if (handoff && inserted) wlog[entries + ins + __popc(mi & ((1u << lane) - 1))] = v;  // call order
         ins += __popc(mi);
         if (isnew) nbuf[nnew + __popc(mn & ((1u << lane) - 1))] = v;
         nnew += __popc(mn);
@@ -328,8 +370,35 @@ __global__ void __launch_bounds__(128, 4) search_kernel(SearchArgs a) {
       continue;
     }
     if ((status & QS_REF_WOULD_GROW) && a.emu_list) {
-      // re-run by the exact-emulation tier, which writes this query's outputs
-      if (lane == 0) a.emu_list[atomicAdd(a.emu_count, 1u)] = qi;
+      // continued (or re-run) by the exact-emulation tier, which writes this query's outputs
+      uint32_t r = PANN_PAD;
+      if (hand_over) {
+        if (lane == 0) r = atomicAdd(a.rec_count, 1u);
+        r = __shfl_sync(FULL, r, 0);
+        if (r < a.rec_cap && nvis <= a.viscap) {
+          const ResumeLayout ly = resume_layout(L, a.Ccap, a.logcap, a.viscap);
+          uint32_t* rec = a.rec_pool + (size_t)r * a.rec_words;
+          if (lane == 0) {
+            rec[0] = qi; rec[1] = (uint32_t)fn; rec[2] = (uint32_t)cn; rec[3] = (uint32_t)nvis;
+            rec[4] = cmps; rec[5] = entries;
+          }
+          uint64_t* rfr = reinterpret_cast<uint64_t*>(rec + ly.fr);
+          uint64_t* rcand = reinterpret_cast<uint64_t*>(rec + ly.cand);
+          for (int i = lane; i < fn; i += 32) rfr[i] = fr[i];
+          for (int i = lane; i < cn; i += 32) rcand[i] = cand[i];
+          __syncwarp();
+          for (uint32_t i = lane; i < entries; i += 32) rec[ly.log + i] = wlog[i];
+          for (uint32_t i = lane; i < (uint32_t)nvis; i += 32) rec[ly.vis + i] = wvis[i];
+        } else {
+          r = PANN_PAD;  // no room: the emulation re-runs the query from the start
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        uint32_t pos = atomicAdd(a.emu_count, 1u);
+        a.emu_list[pos] = qi;
+        a.emu_rec[pos] = r;
+      }
       __syncwarp();
       continue;
     }

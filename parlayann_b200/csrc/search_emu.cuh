@@ -35,12 +35,14 @@ struct EmuArgs {
   uint32_t vs_slots; // exact visited-id set, in shared memory (power of two)
   uint32_t base_bytes;  // search state bytes before the visited set
   uint32_t* overflow_list;  // queries whose emulated table outgrew this tier
+  uint32_t* overflow_rec;
   uint32_t* overflow_count;
+  const uint32_t* job_rec;  // per job: resume record (tier 0's saved state) or PAD
 };
 
-__device__ __forceinline__ uint32_t ref_slot(uint32_t k, uint32_t mask) {
-  return (uint32_t)(((uint64_t)k * 0xbf58476d1ce4e5b9ull) & (uint64_t)mask);
-}
+// (k * 0xbf58476d1ce4e5b9) & mask for mask < 2^32: the product's low 32 bits
+// depend only on the multiplier's low 32 bits, so 32-bit arithmetic suffices.
+__device__ __forceinline__ uint32_t ref_slot(uint32_t k, uint32_t mask) { return (k * 0x1ce4e5b9u) & mask; }
 
 // State of the emulated hashset, identical in every lane of the warp.
 struct EmuHash {
@@ -75,12 +77,15 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
     unsigned want = __ballot_sync(FULL, !done);
     if (!want) break;
     unsigned grp = __match_any_sync(FULL, done ? (0x80000000u | (uint32_t)lane) : p);
-    if (!done && (__ffs(grp & want) - 1) == lane) {
+    const bool win = !done && (__ffs(grp & want) - 1) == lane;
+    if (win) {
       tab[p] = key;
       inserted = true;
       done = true;
     }
+    const unsigned won = __ballot_sync(FULL, win);
     __syncwarp();
+    if (won == want) break;  // nobody lost a slot: every call is finished
   }
   *ins = inserted;
   *pos = p;
@@ -99,19 +104,27 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
   for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
   __syncwarp();
   const uint32_t oldmask = size - 1, nmask = nsize - 1;
-  long long added = 0;
-  // re-insert in old-slot order: lane order within a 32-slot chunk is slot
-  // order, so the lanes holding keys go straight into the ordered rounds
+  // re-insert in old-slot order: first compact the old table's keys to its
+  // front (order kept; writes never pass the chunk being read), then insert
+  // them 32 at a time with the ordered rounds
+  uint32_t cnt = 0;
   for (uint32_t base = 0; base < size; base += 32) {
     uint32_t k = h.cur[base + lane];
     bool v = k != PANN_PAD;
     unsigned m = __ballot_sync(FULL, v);
-    if (!m) continue;
+    __syncwarp();
+    if (v) h.cur[cnt + __popc(m & ((1u << lane) - 1))] = k;
+    cnt += __popc(m);
+    __syncwarp();
+  }
+  for (uint32_t b = 0; b < cnt; b += 32) {
+    const bool v = b + lane < cnt;
+    const uint32_t k = v ? h.cur[b + lane] : PANN_PAD;
     bool ins;
     uint32_t pos;
     emu_probe_rounds(other, nmask, k, v, ref_slot(k, nmask), lane, &ins, &pos);
-    added += __popc(m);
   }
+  const long long added = cnt;
   h.num_entries += added;
   uint32_t* t = h.cur; h.cur = h.other; h.other = t;
   uint32_t c = h.cur_cap; h.cur_cap = h.other_cap; h.other_cap = c;
@@ -252,6 +265,7 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     job = __shfl_sync(FULL, job, 0);
     if (job >= njobs) break;
     const uint32_t qi = a.job_list ? a.job_list[job] : job;
+    const uint32_t rec_id = e.job_rec ? e.job_rec[job] : PANN_PAD;
     const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
     const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
     stage_query<DT, MT>(qs, qsrc, (int)a.nchunks, lane);
@@ -267,23 +281,53 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     int32_t qq = 0;
     if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), a.nchunks);
 
-    // starting points, inserted in the given order (:73-76)
-    for (uint32_t s = lane; s < a.n_start; s += 32) {
-      uint32_t id = a.starts[s];
-      float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
-      frB[s] = make_key(dd, id);
-    }
-    for (uint32_t s0 = 0; s0 < a.n_start && ok; s0 += 32)
-      ok = emu_batch(h, s0 + lane < a.n_start ? a.starts[s0 + lane] : PANN_PAD, s0 + lane < a.n_start, lane, &sdummy);
-    __syncwarp();
     uint64_t* fr = frA;
     uint64_t* fr2 = frB;
-    warp_rank_sort(frB, fr, (int)a.n_start, lane);
+    int fn, cn;
+    uint32_t cmps;
+    uint64_t nvis;
+    if (rec_id != PANN_PAD) {
+      // resume tier 0's query: its state before the visit that could cross the
+      // growth threshold, and the reference's table rebuilt from the insertion
+      // log (no growth can have happened before that visit)
+      const ResumeLayout ly = resume_layout(a.L, a.Ccap, a.logcap, a.viscap);
+      const uint32_t* rec = a.rec_pool + (size_t)rec_id * a.rec_words;
+      fn = (int)rec[1];
+      cn = (int)rec[2];
+      nvis = rec[3];
+      cmps = rec[4];
+      const uint32_t entries = rec[5];
+      const uint64_t* rfr = reinterpret_cast<const uint64_t*>(rec + ly.fr);
+      const uint64_t* rcand = reinterpret_cast<const uint64_t*>(rec + ly.cand);
+      for (int i = lane; i < fn; i += 32) fr[i] = rfr[i];
+      for (int i = lane; i < cn; i += 32) cand[i] = rcand[i];
+      const uint32_t mask0 = (1u << h.bits) - 1;
+      for (uint32_t b = 0; b < entries; b += 32) {
+        const bool v = b + lane < entries;
+        const uint32_t key = v ? rec[ly.log + b + lane] : PANN_PAD;
+        bool ins;
+        uint32_t pos;
+        emu_probe_rounds(h.cur, mask0, key, v, ref_slot(key, mask0), lane, &ins, &pos);
+      }
+      h.num_entries = entries;
+      for (uint32_t i = lane; i < (uint32_t)nvis; i += 32) vset_insert(vset, vmask, rec[ly.vis + i]);
+    } else {
+      // starting points, inserted in the given order (:73-76)
+      for (uint32_t s = lane; s < a.n_start; s += 32) {
+        uint32_t id = a.starts[s];
+        float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
+        frB[s] = make_key(dd, id);
+      }
+      for (uint32_t s0 = 0; s0 < a.n_start && ok; s0 += 32)
+        ok = emu_batch(h, s0 + lane < a.n_start ? a.starts[s0 + lane] : PANN_PAD, s0 + lane < a.n_start, lane, &sdummy);
+      __syncwarp();
+      warp_rank_sort(frB, fr, (int)a.n_start, lane);
+      fn = (int)a.n_start;
+      cn = 0;
+      cmps = a.n_start;
+      nvis = 0;
+    }
     __syncwarp();
-    int fn = (int)a.n_start;
-    int cn = 0;
-    uint32_t cmps = a.n_start;
-    uint64_t nvis = 0;
     uint32_t status = QS_REF_WOULD_GROW;
     if (!ok) status |= QS_TABLE_FULL;
 
@@ -338,7 +382,8 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
         if (i0 < nnew) {
           v0 = nbuf[i0];
           v1 = i1 < nnew ? nbuf[i1] : 0u;
-          point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
+          // one warp per SM here: registers are plentiful, load whole rows at once
+          point_dist2<DT, MT, 24>(a.points + (uint64_t)v0 * a.stride,
                               i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
                               a.opaque_zero);
         }
@@ -380,7 +425,11 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     if (status & QS_TABLE_FULL) {
       // the emulated table outgrew this tier: the next tier (larger, global) re-runs it
       if (lane == 0) {
-        if (e.overflow_list) e.overflow_list[atomicAdd(e.overflow_count, 1u)] = qi;
+        if (e.overflow_list) {
+          uint32_t pos = atomicAdd(e.overflow_count, 1u);
+          e.overflow_list[pos] = qi;
+          e.overflow_rec[pos] = rec_id;
+        }
         if (a.out_status) a.out_status[qi] = status;
       }
       __syncwarp();
