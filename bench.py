@@ -58,47 +58,58 @@ def make_data():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clock and throttle reasons sampled every 5 ms by a thread (NVML)
+    while the timed region runs; falls back to nvidia-smi at 200 ms."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    HW_SLOWDOWN, SW_POWER_CAP, HW_THERMAL, SW_THERMAL = 0x8, 0x4, 0x40, 0x20
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+        self.samples = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
 
     def __enter__(self):
+        import threading
+
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(mhz), int(reasons)))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.005)
+
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
         except Exception:
-            self.p = None
+            self._thread = None
         return self
 
     def __exit__(self, *a):
-        if self.p:
-            self.p.terminate()
-            try:
-                self.p.wait(timeout=5)
-            except Exception:
-                self.p.kill()
+        if self._thread:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
-            os.unlink(self.f.name)
-        except Exception:
+        if not self.samples:
             return None
-        if not rows:
-            return None
-        sm = [float(r[1]) for r in rows]
-        mx = float(rows[0][2])
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        names = {self.HW_SLOWDOWN: "hw_slowdown", self.HW_THERMAL: "hw_thermal_slowdown",
+                 self.SW_THERMAL: "sw_thermal_slowdown", self.SW_POWER_CAP: "sw_power_cap"}
+        reasons = sorted({n for _, r in self.samples for bit, n in names.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml, 5 ms"}
 
 
 def measured_peak():
@@ -385,7 +396,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--beam", type=int, default=0, help="fix the beam instead of sweeping for recall 0.95")

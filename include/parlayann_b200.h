@@ -136,6 +136,37 @@ int pann_search_lists(pann_index* idx, const void* queries, uint32_t nq, const p
                       uint32_t* frontier_n, uint32_t visited_cap, uint32_t* visited_ids, float* visited_d,
                       uint32_t* visited_n, uint32_t* out_cmps);
 
+/* ---------------------------------------------------------------- precision form */
+
+/* Precision of the traversal for float32 indexes. PANN_PREC_F32 is the exact
+ * reference search. PANN_PREC_BF16 / PANN_PREC_FP8 score candidates from a
+ * low-precision copy of the points (bfloat16; or FP8 E4M3 with one scale per
+ * dimension, scale = max |x| / 448) with float32 accumulation, then re-rank the
+ * best `rerank` frontier entries (default 4k) with the exact float32 distance,
+ * like beam_search_rerank's full-precision pass (beamSearch.h:569-587). The
+ * seen-set, visited list and traversal rules are unchanged. */
+#define PANN_PREC_F32 0
+#define PANN_PREC_BF16 1
+#define PANN_PREC_FP8 2
+
+typedef struct {
+  int32_t precision; /* PANN_PREC_* */
+  uint32_t rerank;   /* candidates re-ranked in float32 (0 = 4k) */
+} pann_search_options;
+
+/* Build the low-precision copy of the points used by `precision` (kept until
+ * the next call; PANN_PREC_F32 frees it). No reference counterpart: the
+ * reference's closest feature is its scalar quantization (euclidian_point.h:98-109). */
+int pann_index_set_precision(pann_index* idx, int precision);
+
+/* pann_search with options. on_device != 0: every buffer is device memory and
+ * the call is asynchronous on `stream` (as pann_search_device); else host
+ * buffers and a synchronous call (as pann_search). */
+int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                   const pann_search_options* opt, const uint32_t* starts, uint32_t n_start, uint32_t* out_ids,
+                   float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags, int on_device,
+                   void* stream);
+
 /* ---------------------------------------------------------------- build */
 
 /* Vamana batch-insertion build into the index's graph (knn_index::build_index,

@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(_HERE, "libparlayann_b200.so")
 PANN_OK, PANN_EINVAL, PANN_ENOMEM, PANN_ETIMEOUT, PANN_EDEVICE, PANN_EOVERFLOW, PANN_ESHORT = range(7)
 U8, I8, F32 = 0, 1, 2
 L2, MIPS = 0, 1
+PREC_F32, PREC_BF16, PREC_FP8 = 0, 1, 2
 _DTYPES = {np.dtype(np.uint8): U8, np.dtype(np.int8): I8, np.dtype(np.float32): F32}
 _NP_OF = {U8: np.uint8, I8: np.int8, F32: np.float32}
 
@@ -45,6 +46,12 @@ class QueryParams(ctypes.Structure):
         ("degree_limit", ctypes.c_uint32),
         ("batch_factor", ctypes.c_double),
     ]
+
+
+class SearchOptions(ctypes.Structure):
+    """pann_search_options: precision form and re-rank count."""
+
+    _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32)]
 
 
 class BuildParams(ctypes.Structure):
@@ -89,6 +96,9 @@ SIGNATURES = {
     "pann_search_device": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P, _P]),
     "pann_search_lists": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _U32, _P, _P, _P,
                                _P]),
+    "pann_index_set_precision": (_I, [_P, _I]),
+    "pann_search_ex": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.POINTER(SearchOptions), _P, _U32, _P,
+                            _P, _P, _P, _P, _I, _P]),
     "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
     "pann_groundtruth": (_I, [_P, _P, _U32, _U32, _P, _P]),
     "pann_last_error": (ctypes.c_char_p, []),
@@ -229,8 +239,13 @@ class Index:
         _check(lib().pann_build(self._h, ctypes.byref(bp), _ptr(p), ctypes.byref(st)))
         return st
 
+    def set_precision(self, precision: int):
+        """Build the low-precision copy used by the precision form (float32 indexes)."""
+        _check(lib().pann_index_set_precision(self._h, precision))
+
     def search(self, queries: np.ndarray, k: int, L: int, limit: int | None = None, degree_limit: int | None = None,
-               batch_factor: float = 0.125, starts=(0,), allow_short: bool = False) -> SearchResult:
+               batch_factor: float = 0.125, starts=(0,), allow_short: bool = False, precision: int = PREC_F32,
+               rerank: int = 0) -> SearchResult:
         queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
         nq = queries.shape[0]
         qp = QueryParams(k, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
@@ -241,8 +256,13 @@ class Index:
         vis = np.empty(nq, np.uint32)
         cmps = np.empty(nq, np.uint32)
         flags = np.empty(nq, np.uint32)
-        rc = lib().pann_search(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(ids),
-                               _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags))
+        if precision == PREC_F32 and rerank == 0:
+            rc = lib().pann_search(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(ids),
+                                   _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags))
+        else:
+            opt = SearchOptions(precision, rerank)
+            rc = lib().pann_search_ex(self._h, _ptr(queries), nq, ctypes.byref(qp), ctypes.byref(opt), _ptr(st),
+                                      len(st), _ptr(ids), _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags), 0, None)
         if not (allow_short and rc == PANN_ESHORT):
             _check(rc)
         return SearchResult(ids, dists, vis, cmps, flags)

@@ -13,6 +13,7 @@
 #include "index.cuh"
 #include "search.cuh"
 #include "search_emu.cuh"
+#include "lowprec.cuh"
 
 namespace pann {
 
@@ -103,9 +104,9 @@ static uint32_t pow2_at_least(uint64_t x) {
   return p;
 }
 
-template <int DT, int MT, bool G>
+template <int DT, int MT, bool G, int PREC = PREC_F32>
 static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
-  auto k = search_kernel<DT, MT, G>;
+  auto k = search_kernel<DT, MT, G, PREC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k<<<blocks, threads, smem, st>>>(a);
@@ -113,7 +114,20 @@ static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads,
 }
 
 static cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
-                                 int threads, size_t smem, cudaStream_t st) {
+                                 int threads, size_t smem, cudaStream_t st, int prec = PREC_F32) {
+  if (prec != PREC_F32) {
+    if (dtype != DT_F32) return cudaErrorInvalidValue;
+#define PANN_LP_CASE(MT, PR)                                                               \
+    if (metric == MT && prec == PR)                                                        \
+      return global_table ? launch_search_t<DT_F32, MT, true, PR>(a, blocks, threads, smem, st) \
+                          : launch_search_t<DT_F32, MT, false, PR>(a, blocks, threads, smem, st);
+    PANN_LP_CASE(MT_L2, PREC_BF16)
+    PANN_LP_CASE(MT_IP, PREC_BF16)
+    PANN_LP_CASE(MT_L2, PREC_FP8)
+    PANN_LP_CASE(MT_IP, PREC_FP8)
+#undef PANN_LP_CASE
+    return cudaErrorInvalidValue;
+  }
 #define PANN_SEARCH_CASE(DT, MT)                                                        \
   if (dtype == DT && metric == MT)                                                      \
     return global_table ? launch_search_t<DT, MT, true>(a, blocks, threads, smem, st)   \
@@ -152,10 +166,10 @@ static cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const
   return cudaErrorInvalidValue;
 }
 
-template <int DT, int MT, bool G>
+template <int DT, int MT, bool G, int PREC = PREC_F32>
 static int occupancy_t(int threads, size_t smem) {
   int nb = 0;
-  auto k = search_kernel<DT, MT, G>;
+  auto k = search_kernel<DT, MT, G, PREC>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
   return nb;
@@ -173,10 +187,20 @@ static int search_occupancy(int dtype, int metric, bool g, int threads, size_t s
   return 0;
 }
 
+static int lp_occupancy(int metric, int prec, int threads, size_t smem) {
+  if (metric == MT_L2 && prec == PREC_BF16) return occupancy_t<DT_F32, MT_L2, false, PREC_BF16>(threads, smem);
+  if (metric == MT_IP && prec == PREC_BF16) return occupancy_t<DT_F32, MT_IP, false, PREC_BF16>(threads, smem);
+  if (metric == MT_L2 && prec == PREC_FP8) return occupancy_t<DT_F32, MT_L2, false, PREC_FP8>(threads, smem);
+  if (metric == MT_IP && prec == PREC_FP8) return occupancy_t<DT_F32, MT_IP, false, PREC_FP8>(threads, smem);
+  return 0;
+}
+
 // Shared-memory seen-table slots of tier 0: the PANN_SEEN_SLOTS environment
-// variable, else room (at 3/4 load) for about (L + 16) * min(dl, R) * 3/4
-// distinct ids, between 4 (R + 1) and 8192 slots; queries that need more
-// continue in the per-warp global spill table.
+// variable, else the power of two at or above (L + 16) * min(dl, R) * 2/3
+// (about 3/4-load room for the ids a search typically sees), between 4 (R + 1)
+// and 8192 slots; queries that need more continue in the per-warp global
+// spill table. Doubling the table halves the warps that fit on an SM, so the
+// estimate errs small.
 static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
   uint32_t floor_s = pow2_at_least(4ull * (R + 1));
   if (const char* e = std::getenv("PANN_SEEN_SLOTS")) {
@@ -184,7 +208,7 @@ static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
     if (v > 0) return std::max<uint32_t>(pow2_at_least((uint64_t)v), floor_s);
   }
   uint32_t nel = std::min(p.dl, R);
-  uint64_t est = (uint64_t)(p.L + 16) * nel;  // (3/4 of the ids) / (3/4 load)
+  uint64_t est = (uint64_t)(p.L + 16) * nel * 2 / 3;
   uint32_t s = pow2_at_least(est);
   s = std::min<uint32_t>(s, 8192);
   return std::max<uint32_t>(s, floor_s);
@@ -196,7 +220,8 @@ static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
 // re-run with that hashset emulated exactly.
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
-               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st) {
+               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
+               int precision, uint32_t rerank) {
   if (nq == 0) return PANN_OK;
   // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
   // [5] shared-memory emulation job counter, [6] emulation list length,
@@ -242,6 +267,15 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.emu_list = emu;
   a.emu_rec = emu_rec;
   a.emu_count = cnt + 6;
+  if (precision != PREC_F32) {
+    if (idx->lp_prec != precision) return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
+    a.emu_list = nullptr;  // the precision form is not a reference path: no hashset emulation
+    a.lp_rows = idx->lp_rows.as<uint8_t>();
+    a.lp_stride = idx->lp_stride;
+    a.lp_chunks = idx->lp_chunks;
+    a.lp_scales = idx->lp_scales.as<float>();
+    a.rerank = rerank ? rerank : 4 * plan.k;
+  }
 
   const size_t smem_cap = idx->smem_optin;
   // ---- tier 0: many warps per SM, a modest shared-memory seen table that
@@ -256,7 +290,8 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
       wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
     }
     if ((size_t)wb * wpb > smem_cap) return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
-    int occ = search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb);
+    int occ = precision == PREC_F32 ? search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb)
+                                    : lp_occupancy(idx->metric, precision, 32 * wpb, (size_t)wb * wpb);
     if (occ <= 0) occ = 1;
     uint64_t want = (nq + wpb - 1) / wpb;
     int blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
@@ -301,7 +336,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
       t.gspill = nullptr;
       t.Sg = 0;
     }
-    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st));
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st, precision));
   }
   // ---- tier 2: queries whose tables still filled up, with one global-memory
   // seen table per warp sized above the reference's own capacity
@@ -321,8 +356,9 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     t.job_counter = cnt + 2;
     t.redo_list = nullptr;
     t.redo_count = nullptr;
-    PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, slots, 32, wb, st));
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, slots, 32, wb, st, precision));
   }
+  if (precision != PREC_F32) return PANN_OK;
   // ---- tier E: exact emulation of the reference's hashset for flagged queries,
   // first with the emulated table in shared memory (capacities 4 S0 / 2 S0),
   // then, for queries that outgrow it, in global memory (16 S0 / 8 S0)
@@ -478,7 +514,7 @@ int pann_index_destroy(pann_index* idx) {
   if (idx->d_graph) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
                     &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->handoff, &idx->starts,
-                    &idx->tmp})
+                    &idx->tmp, &idx->lp_rows, &idx->lp_scales})
     b->release();
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;
@@ -651,6 +687,120 @@ int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_qu
   if (out_cmps) PANN_CUDA(cudaMemcpyAsync(out_cmps, idx->cmps.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
   std::vector<uint32_t> status(nq);
   PANN_CUDA(cudaMemcpyAsync(status.data(), idx->status.p, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  return summarize_status(status.data(), nq, out_flags);
+}
+
+int pann_index_set_precision(pann_index* idx, int precision) {
+  if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points");
+  if (precision == PANN_PREC_F32) {
+    idx->lp_rows.release();
+    idx->lp_scales.release();
+    idx->lp_prec = 0;
+    return PANN_OK;
+  }
+  if (idx->dtype != PANN_F32) return fail(PANN_EINVAL, "the precision form needs float32 points");
+  if (precision != PANN_PREC_BF16 && precision != PANN_PREC_FP8) return fail(PANN_EINVAL, "unknown precision");
+  cudaStream_t st = idx->stream;
+  const uint64_t n = idx->n;
+  const uint32_t d = idx->d;
+  const uint64_t vals = precision == PANN_PREC_BF16 ? 2 : 1;
+  idx->lp_stride = ((uint64_t)d * vals + 15) & ~15ull;
+  idx->lp_chunks = (uint32_t)(idx->lp_stride / 16);
+  PANN_CUDA(idx->lp_rows.ensure(idx->lp_stride * n));
+  PANN_CUDA(cudaMemsetAsync(idx->lp_rows.p, 0, idx->lp_stride * n, st));
+  const uint32_t dpad = (d + 15) & ~15u;
+  PANN_CUDA(idx->lp_scales.ensure(4ull * dpad * 2));
+  PANN_CUDA(cudaMemsetAsync(idx->lp_scales.p, 0, 4ull * dpad * 2, st));
+  int blocks = (int)std::min<uint64_t>((n * d + 255) / 256, 65535ull * 4);
+  if (precision == PANN_PREC_BF16) {
+    to_bf16_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const float*>(idx->d_points), idx->stride / 4,
+                                           idx->lp_rows.as<uint16_t>(), idx->lp_stride / 2, n, d);
+    PANN_CUDA(cudaGetLastError());
+  } else {
+    uint32_t* bits = idx->lp_scales.as<uint32_t>() + dpad;  // scratch: per-dimension max |x|
+    absmax_kernel<<<1024, 128, 0, st>>>(reinterpret_cast<const float*>(idx->d_points), idx->stride / 4, n, d, bits);
+    PANN_CUDA(cudaGetLastError());
+    std::vector<uint32_t> hb(d);
+    PANN_CUDA(cudaMemcpyAsync(hb.data(), bits, 4ull * d, cudaMemcpyDeviceToHost, st));
+    PANN_CUDA(cudaStreamSynchronize(st));
+    std::vector<float> scale(dpad, 0.0f), inv(d);
+    for (uint32_t j = 0; j < d; j++) {
+      float m;
+      std::memcpy(&m, &hb[j], 4);
+      scale[j] = m > 0.0f ? m / 448.0f : 1.0f;
+      inv[j] = 1.0f / scale[j];
+    }
+    DevBuf dinv;
+    PANN_CUDA(dinv.ensure(4ull * d));
+    PANN_CUDA(cudaMemcpyAsync(dinv.p, inv.data(), 4ull * d, cudaMemcpyHostToDevice, st));
+    PANN_CUDA(cudaMemcpyAsync(idx->lp_scales.p, scale.data(), 4ull * dpad, cudaMemcpyHostToDevice, st));
+    to_fp8_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<const float*>(idx->d_points), idx->stride / 4,
+                                          idx->lp_rows.as<uint8_t>(), idx->lp_stride, n, d, dinv.as<float>());
+    PANN_CUDA(cudaGetLastError());
+    PANN_CUDA(cudaStreamSynchronize(st));
+    dinv.release();
+  }
+  PANN_CUDA(cudaStreamSynchronize(st));
+  idx->lp_prec = precision;
+  return PANN_OK;
+}
+
+int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                   const pann_search_options* opt, const uint32_t* starts, uint32_t n_start, uint32_t* out_ids,
+                   float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags, int on_device,
+                   void* stream) {
+  int rc = check_index(idx, true);
+  if (rc) return rc;
+  if (nq && (!queries || !out_ids)) return fail(PANN_EINVAL, "queries or out_ids is NULL");
+  const int prec = opt ? opt->precision : PANN_PREC_F32;
+  const uint32_t rerank = opt ? opt->rerank : 0;
+  SearchPlan plan;
+  rc = make_plan(idx, qp, n_start, &plan);
+  if (rc) return rc;
+  if (prec != PANN_PREC_F32 && idx->lp_prec != prec)
+    return fail(PANN_EINVAL, "call pann_index_set_precision for this precision first");
+  if (nq == 0) return PANN_OK;
+  cudaStream_t st = on_device ? static_cast<cudaStream_t>(stream) : idx->stream;
+  rc = stage_starts(idx, starts, n_start, st);
+  if (rc) return rc;
+  const size_t k = plan.k;
+  size_t rb = (size_t)idx->d * idx->esize;
+  const uint8_t* q = static_cast<const uint8_t*>(queries);
+  if (!on_device || rb != idx->stride) {
+    PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
+    if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(idx->q.p, 0, idx->stride * (size_t)nq, st));
+    PANN_CUDA(cudaMemcpy2DAsync(idx->q.p, idx->stride, queries, rb, rb, nq,
+                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    q = idx->q.as<uint8_t>();
+  }
+  uint32_t *d_ids = out_ids, *d_vis = out_visited, *d_cmps = out_cmps, *d_status = out_flags;
+  float* d_dists = out_dists;
+  if (!on_device) {
+    PANN_CUDA(idx->ids.ensure(4 * std::max<size_t>(1, k * nq)));
+    PANN_CUDA(idx->dists.ensure(4 * std::max<size_t>(1, k * nq)));
+    PANN_CUDA(idx->vis.ensure(4 * (size_t)nq));
+    PANN_CUDA(idx->cmps.ensure(4 * (size_t)nq));
+    d_ids = idx->ids.as<uint32_t>();
+    d_dists = idx->dists.as<float>();
+    d_vis = idx->vis.as<uint32_t>();
+    d_cmps = idx->cmps.as<uint32_t>();
+  }
+  if (!on_device || !d_status) {
+    PANN_CUDA(idx->status.ensure(4 * (size_t)nq));
+    d_status = idx->status.as<uint32_t>();
+  }
+  rc = run_search(idx, plan, q, nullptr, nq, idx->starts.as<uint32_t>(), d_ids, d_dists, d_vis, d_cmps, d_status,
+                  nullptr, 0, st, prec, rerank);
+  if (rc || on_device) return rc;
+  if (k) {
+    PANN_CUDA(cudaMemcpyAsync(out_ids, d_ids, 4 * k * nq, cudaMemcpyDeviceToHost, st));
+    if (out_dists) PANN_CUDA(cudaMemcpyAsync(out_dists, d_dists, 4 * k * nq, cudaMemcpyDeviceToHost, st));
+  }
+  if (out_visited) PANN_CUDA(cudaMemcpyAsync(out_visited, d_vis, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  if (out_cmps) PANN_CUDA(cudaMemcpyAsync(out_cmps, d_cmps, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
+  std::vector<uint32_t> status(nq);
+  PANN_CUDA(cudaMemcpyAsync(status.data(), d_status, 4 * (size_t)nq, cudaMemcpyDeviceToHost, st));
   PANN_CUDA(cudaStreamSynchronize(st));
   return summarize_status(status.data(), nq, out_flags);
 }

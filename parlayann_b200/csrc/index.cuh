@@ -56,6 +56,11 @@ struct pann_index {
   cudaStream_t stream = nullptr;
   // search scratch
   pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, gtables2, emu, handoff, starts, tmp;
+  // precision form: low-precision copy of float32 points (lowprec.cuh)
+  pann::DevBuf lp_rows, lp_scales;
+  int lp_prec = 0;
+  uint64_t lp_stride = 0;
+  uint32_t lp_chunks = 0;
   uint32_t starts_cached_n = 0;
   uint32_t starts_cached[64] = {};
 };
@@ -75,8 +80,11 @@ int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_sta
 
 // Run the tiered search on device buffers (queries already in index row layout).
 // self_ids (device, nullable) selects build mode: query j is point self_ids[j].
+// precision != 0 runs the precision form (low-precision traversal, exact
+// re-rank of the best `rerank` entries).
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
-               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st);
+               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
+               int precision = 0, uint32_t rerank = 0);
 
 }  // namespace pann

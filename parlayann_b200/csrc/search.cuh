@@ -24,6 +24,7 @@
 // (so float sums keep the reference's sequential order).
 #pragma once
 #include "common.cuh"
+#include "lowprec.cuh"
 
 namespace pann {
 
@@ -82,6 +83,13 @@ struct SearchArgs {
   uint32_t rec_cap;
   uint32_t rec_words;
   uint32_t* rec_count;
+  // precision form (float32 indexes): low-precision rows steer the search,
+  // the best `rerank` frontier entries are re-scored exactly at the end
+  const uint8_t* lp_rows;
+  uint64_t lp_stride;
+  uint32_t lp_chunks;
+  const float* lp_scales;
+  uint32_t rerank;
 };
 
 // Resume record: 8-word header (query, fn, cn, visits, cmps, entries), the
@@ -172,7 +180,7 @@ __device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint
   return 0;
 }
 
-template <int DT, int MT, bool TABLE_GLOBAL>
+template <int DT, int MT, bool TABLE_GLOBAL, int PREC = PREC_F32>
 __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int lane = threadIdx.x & 31;
@@ -200,7 +208,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
   const uint32_t spill_limit = (a.Sg >> 2) * 3;
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
   const uint32_t L = a.L;
-  const bool handoff = a.inslog != nullptr && a.emu_list != nullptr;
+  const bool handoff = PREC == PREC_F32 && a.inslog != nullptr && a.emu_list != nullptr;
   uint32_t* const wlog = handoff ? a.inslog + ((size_t)blockIdx.x * wpb + warp) * a.logcap : nullptr;
   uint32_t* const wvis = handoff ? a.vislog + ((size_t)blockIdx.x * wpb + warp) * a.viscap : nullptr;
 
@@ -227,7 +235,10 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
     // starting points (:73-77); n_start <= L, staged in frB then sorted into frA
     for (uint32_t s = lane; s < a.n_start; s += 32) {
       uint32_t id = a.starts[s];
-      float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
+      float dd, dummy;
+      if (PREC == PREC_F32) dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq);
+      else lp_dist2<MT, PREC>(a.lp_rows + (uint64_t)id * a.lp_stride, nullptr, reinterpret_cast<const float*>(qs),
+                              a.lp_scales, (int)a.d, (int)a.lp_chunks, dd, dummy);
       frB[s] = make_key(dd, id);
       table_insert(table, mask, id);
       if (handoff) wlog[s] = id;
@@ -334,9 +345,14 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
         if (i0 < nnew) {
           v0 = nbuf[i0];
           v1 = i1 < nnew ? nbuf[i1] : 0u;
-          point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
-                              i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
-                              a.opaque_zero);
+          if (PREC == PREC_F32)
+            point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
+                                i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
+                                a.opaque_zero);
+          else
+            lp_dist2<MT, PREC>(a.lp_rows + (uint64_t)v0 * a.lp_stride,
+                               i1 < nnew ? a.lp_rows + (uint64_t)v1 * a.lp_stride : nullptr,
+                               reinterpret_cast<const float*>(qs), a.lp_scales, (int)a.d, (int)a.lp_chunks, d0, d1);
         }
         bool keep0 = i0 < nnew && !(d0 >= cutoff);
         unsigned m0 = __ballot_sync(FULL, keep0);
@@ -403,10 +419,44 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       continue;
     }
     if ((uint32_t)fn < a.k) status |= QS_SHORT;
-    for (uint32_t j = lane; j < a.k; j += 32) {
-      bool ok = j < (uint32_t)fn;
-      a.out_ids[(uint64_t)qi * a.k + j] = ok ? key_id(fr[j]) : PANN_PAD;
-      if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = ok ? key_dist(fr[j]) : 0.0f;
+    if (PREC != PREC_F32) {
+      // re-rank the best min(rerank, fn) entries by exact float32 distance
+      // (beam_search_rerank's full-precision pass, beamSearch.h:569-587)
+      const int nr = (int)min((uint32_t)fn, a.rerank > a.k ? a.rerank : a.k);
+      for (int b = 0; b < nr; b += 64) {
+        const int i0 = b + lane, i1 = b + 32 + lane;
+        float d0 = 0.f, d1 = 0.f;
+        uint32_t v0 = 0, v1 = 0;
+        if (i0 < nr) {
+          v0 = key_id(fr[i0]);
+          v1 = i1 < nr ? key_id(fr[i1]) : 0u;
+          point_dist2<DT, MT>(a.points + (uint64_t)v0 * a.stride,
+                              i1 < nr ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
+                              a.opaque_zero);
+          fr2[i0] = make_key(d0, v0);
+          if (i1 < nr) fr2[i1] = make_key(d1, v1);
+        }
+      }
+      __syncwarp();
+      for (int i = lane; i < nr; i += 32) {
+        const uint64_t ki = fr2[i];
+        int r = 0;
+        for (int j = 0; j < nr; j++) r += fr2[j] < ki;
+        if ((uint32_t)r < a.k) {
+          a.out_ids[(uint64_t)qi * a.k + r] = key_id(ki);
+          if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + r] = key_dist(ki);
+        }
+      }
+      for (uint32_t j = (uint32_t)nr + lane; j < a.k; j += 32) {
+        a.out_ids[(uint64_t)qi * a.k + j] = PANN_PAD;
+        if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = 0.0f;
+      }
+    } else {
+      for (uint32_t j = lane; j < a.k; j += 32) {
+        bool ok = j < (uint32_t)fn;
+        a.out_ids[(uint64_t)qi * a.k + j] = ok ? key_id(fr[j]) : PANN_PAD;
+        if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = ok ? key_dist(fr[j]) : 0.0f;
+      }
     }
     if (lane == 0) {
       if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;

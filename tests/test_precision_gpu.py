@@ -1,0 +1,59 @@
+"""The precision form (float32 indexes): traversal scored from a bfloat16 or
+FP8-E4M3 (per-dimension scales) copy of the points, best 4k re-ranked with the
+exact float32 distance. Results are not bit-exact with the reference (the
+traversal differs by design); the tests bound the recall loss against FP64
+brute force and check that every reported distance is the exact float32
+distance of its id (the re-rank), and that results are reproducible."""
+import numpy as np
+import pytest
+
+import parlayann_b200 as P
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+RECALL_LOSS = {P.PREC_BF16: 0.01, P.PREC_FP8: 0.03}  # allowed recall@10 loss vs the exact search
+
+
+@pytest.fixture(scope="module")
+def mix_index(lib_built):
+    base = P.synth_mixture(P.F32, 30000, 96, 64, 1, 0, sigma=0.3, normalize=True)
+    q = P.synth_mixture(P.F32, 500, 96, 64, 1, 1, sigma=0.3, normalize=True)
+    out = {}
+    for metric in (P.L2, P.MIPS):
+        idx = P.Index(base, 32, metric)
+        idx.build(64, 1.2, num_passes=1)
+        gt, _ = idx.groundtruth(q, 10)
+        out[metric] = (idx, gt)
+    yield base, q, out
+    for idx, _ in out.values():
+        idx.close()
+
+
+@pytest.mark.parametrize("metric", [P.L2, P.MIPS], ids=["l2", "mips"])
+@pytest.mark.parametrize("prec", [P.PREC_BF16, P.PREC_FP8], ids=["bf16", "fp8"])
+def test_precision_recall_and_exact_rerank(mix_index, metric, prec):
+    base, q, out = mix_index
+    idx, gt = out[metric]
+    exact = idx.search(q, 10, 40)
+    idx.set_precision(prec)
+    r = idx.search(q, 10, 40, precision=prec)
+    r2 = idx.search(q, 10, 40, precision=prec)
+    np.testing.assert_array_equal(r.ids, r2.ids)          # deterministic
+    rec_exact = P.recall_at_k(exact.ids, gt, 10)
+    rec = P.recall_at_k(r.ids, gt, 10)
+    assert rec >= rec_exact - RECALL_LOSS[prec], (rec, rec_exact)
+    # every reported distance is the exact float32 distance (sequential sum)
+    for i in range(0, q.shape[0], 25):
+        for j in range(10):
+            v = int(r.ids[i, j])
+            dd = O.olib().oracle_distance(2, metric, 96, base[v].ctypes.data, q[i].ctypes.data)
+            assert r.dists[i, j] == np.float32(dd)
+        assert np.all(np.diff(r.dists[i]) >= 0)
+    idx.set_precision(P.PREC_F32)
+
+
+def test_precision_requires_float_points(lib_built):
+    idx = P.Index(np.zeros((100, 8), np.uint8), 4)
+    with pytest.raises(P.PannError):
+        idx.set_precision(P.PREC_BF16)
+    idx.close()
