@@ -117,8 +117,8 @@ int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_qu
 /* Same, with every buffer in device memory, on `stream` (a cudaStream_t;
  * 0 is the legacy default stream).
  * Does not synchronise. d_out_flags (may be NULL) receives per-query status
- * bits: 1 = the reference's hashset grows on this query (result reproduced
- * exactly), 2 or 16 = the query's state outgrew every buffer (result invalid),
+ * bits: 2 = the reference's hashset grows on this query (result reproduced
+ * exactly), 1 or 16 = the query's state outgrew every buffer (result invalid),
  * 4 = fewer than k results. starts is a HOST array. */
 int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,

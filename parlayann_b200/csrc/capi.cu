@@ -68,6 +68,39 @@ __global__ void graph_to_ref_kernel(const uint32_t* __restrict__ in, uint32_t* _
   }
 }
 
+// ------------------------------------------------------------ precision-form conversions
+__global__ void to_bf16_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint16_t* dst,
+                               uint64_t dst_stride_h, uint64_t n, uint32_t d) {
+  uint64_t total = n * (uint64_t)d;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = t / d;
+    uint32_t j = (uint32_t)(t - i * d);
+    __nv_bfloat16 b = __float2bfloat16_rn(src[i * src_stride_f + j]);
+    dst[i * dst_stride_h + j] = *reinterpret_cast<uint16_t*>(&b);
+  }
+}
+
+// per-dimension max |x| (as float bits: non-negative floats order like unsigned ints)
+__global__ void absmax_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint64_t n, uint32_t d,
+                              uint32_t* out_bits) {
+  for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
+    float m = 0.0f;
+    for (uint64_t i = blockIdx.x; i < n; i += gridDim.x) m = fmaxf(m, fabsf(src[i * src_stride_f + j]));
+    atomicMax(out_bits + j, __float_as_uint(m));
+  }
+}
+
+__global__ void to_fp8_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint8_t* dst, uint64_t dst_stride,
+                              uint64_t n, uint32_t d, const float* __restrict__ inv_scale) {
+  uint64_t total = n * (uint64_t)d;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = t / d;
+    uint32_t j = (uint32_t)(t - i * d);
+    __nv_fp8_e4m3 v(src[i * src_stride_f + j] * inv_scale[j]);
+    dst[i * dst_stride + j] = *reinterpret_cast<uint8_t*>(&v);
+  }
+}
+
 int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan) {
   if (!qp) return fail(PANN_EINVAL, "query params are NULL");
   if (qp->beam == 0) return fail(PANN_EINVAL, "beam (L) must be positive");
@@ -113,7 +146,7 @@ static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads,
   return cudaGetLastError();
 }
 
-static cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
+cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
                                  int threads, size_t smem, cudaStream_t st, int prec = PREC_F32) {
   if (prec != PREC_F32) {
     if (dtype != DT_F32) return cudaErrorInvalidValue;
@@ -150,7 +183,7 @@ static cudaError_t launch_emulate_t(const SearchArgs& a, const EmuArgs& e, int b
   k<<<blocks, 32, smem, st>>>(a, e);
   return cudaGetLastError();
 }
-static cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
+cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
                                   int blocks, size_t smem, cudaStream_t st) {
 #define PANN_EMU_CASE(DT, MT)                                                              \
   if (dtype == DT && metric == MT)                                                         \
@@ -174,7 +207,7 @@ static int occupancy_t(int threads, size_t smem) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
   return nb;
 }
-static int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem) {
+int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem) {
 #define PANN_OCC_CASE(DT, MT) \
   if (dtype == DT && metric == MT) return g ? occupancy_t<DT, MT, true>(threads, smem) : occupancy_t<DT, MT, false>(threads, smem);
   PANN_OCC_CASE(DT_U8, MT_L2)
@@ -201,7 +234,7 @@ static int lp_occupancy(int metric, int prec, int threads, size_t smem) {
 // and 8192 slots; queries that need more continue in the per-warp global
 // spill table. Doubling the table halves the warps that fit on an SM, so the
 // estimate errs small.
-static uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
+uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
   uint32_t floor_s = pow2_at_least(4ull * (R + 1));
   if (const char* e = std::getenv("PANN_SEEN_SLOTS")) {
     long v = std::atol(e);
@@ -250,6 +283,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.nq = nq;
   a.k = plan.k;
   a.L = plan.L;
+  a.kstride = plan.k;
   a.dl = plan.dl;
   a.limit = plan.limit;
   a.batch_factor = plan.bf;

@@ -18,38 +18,6 @@ namespace pann {
 
 enum Precision { PREC_F32 = 0, PREC_BF16 = 1, PREC_FP8 = 2 };
 
-__global__ void to_bf16_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint16_t* dst,
-                               uint64_t dst_stride_h, uint64_t n, uint32_t d) {
-  uint64_t total = n * (uint64_t)d;
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t i = t / d;
-    uint32_t j = (uint32_t)(t - i * d);
-    __nv_bfloat16 b = __float2bfloat16_rn(src[i * src_stride_f + j]);
-    dst[i * dst_stride_h + j] = *reinterpret_cast<uint16_t*>(&b);
-  }
-}
-
-// per-dimension max |x| (as float bits: non-negative floats order like unsigned ints)
-__global__ void absmax_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint64_t n, uint32_t d,
-                              uint32_t* out_bits) {
-  for (uint32_t j = threadIdx.x; j < d; j += blockDim.x) {
-    float m = 0.0f;
-    for (uint64_t i = blockIdx.x; i < n; i += gridDim.x) m = fmaxf(m, fabsf(src[i * src_stride_f + j]));
-    atomicMax(out_bits + j, __float_as_uint(m));
-  }
-}
-
-__global__ void to_fp8_kernel(const float* __restrict__ src, uint64_t src_stride_f, uint8_t* dst, uint64_t dst_stride,
-                              uint64_t n, uint32_t d, const float* __restrict__ inv_scale) {
-  uint64_t total = n * (uint64_t)d;
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t i = t / d;
-    uint32_t j = (uint32_t)(t - i * d);
-    __nv_fp8_e4m3 v(src[i * src_stride_f + j] * inv_scale[j]);
-    dst[i * dst_stride + j] = *reinterpret_cast<uint8_t*>(&v);
-  }
-}
-
 // bf16 pair (packed in a uint32) -> two floats, exactly
 __device__ __forceinline__ float2 bf16x2_to_f2(uint32_t v) {
   return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xFFFF0000u));

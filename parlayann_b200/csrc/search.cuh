@@ -43,8 +43,12 @@ struct SearchArgs {
   const uint32_t* job_list;   // optional: job j is query job_list[j]
   const uint32_t* njobs_dev;  // optional: number of jobs read from device memory
   uint32_t* job_counter;      // dynamic work distribution (zeroed before launch)
-  // query parameters (QueryParams, types.h:233-252)
+  // query parameters (QueryParams, types.h:233-252); k and L are the maxima
+  // when qk / qL give per-query values (the batched form)
   uint32_t k, L, dl;
+  const uint32_t* qk;  // optional per-query k
+  const uint32_t* qL;  // optional per-query beam
+  uint32_t kstride;    // output row stride (>= every k)
   uint64_t limit;
   double batch_factor;
   uint32_t ref_half;  // the reference hashset's growth threshold: capacity/2
@@ -91,6 +95,16 @@ struct SearchArgs {
   const float* lp_scales;
   uint32_t rerank;
 };
+
+// The reference's seen-set capacity for beam L and degree limit dl is
+// 2^ceil(log2(2 (10 + L) dl)) (beamSearch.h:66, hashset.h:50-54); it grows
+// above half of that.
+__host__ __device__ inline uint32_t ref_bits(uint32_t L, uint32_t dl) {
+  const uint64_t n = 2ull * (10ull + L) * dl;
+  uint32_t b = 0;
+  while ((1ull << b) < n) b++;
+  return b;
+}
 
 // Resume record: 8-word header (query, fn, cn, visits, cmps, entries), the
 // frontier (2L words), the candidates (2 Ccap words), the insertion log
@@ -207,7 +221,6 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
   const uint32_t smask = a.Sg - 1;
   const uint32_t spill_limit = (a.Sg >> 2) * 3;
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
-  const uint32_t L = a.L;
   const bool handoff = PREC == PREC_F32 && a.inslog != nullptr && a.emu_list != nullptr;
   uint32_t* const wlog = handoff ? a.inslog + ((size_t)blockIdx.x * wpb + warp) * a.logcap : nullptr;
   uint32_t* const wvis = handoff ? a.vislog + ((size_t)blockIdx.x * wpb + warp) * a.viscap : nullptr;
@@ -220,6 +233,9 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
     const uint32_t qi = a.job_list ? a.job_list[job] : job;
     const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
     const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
+    const uint32_t L = a.qL ? a.qL[qi] : a.L;  // this query's beam (<= a.L, the buffer size)
+    const uint32_t kq = a.qk ? a.qk[qi] : a.k;
+    const uint32_t ref_half = a.qL ? (1u << ref_bits(L, a.dl)) / 2 : a.ref_half;
 
     // stage the query, clear the seen table
     stage_query<DT, MT>(qs, qsrc, (int)a.nchunks, lane);
@@ -276,7 +292,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       }
       if (first >= 0) cnt += 1;
       if (first < 0 || nvis >= a.limit) break;  // :116
-      if (handoff && entries + nel > a.ref_half) {
+      if (handoff && entries + nel > ref_half) {
         // this visit could cross the reference's growth threshold
         status |= QS_REF_WOULD_GROW;
         hand_over = true;
@@ -331,7 +347,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       }
       entries += ins;
       if (!spilled) entries_sh += ins;
-      if (entries > a.ref_half) status |= QS_REF_WOULD_GROW;
+      if (entries > ref_half) status |= QS_REF_WOULD_GROW;
       __syncwarp();
 
       // distances; keep those below the cutoff (:176-182)
@@ -392,7 +408,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
         if (lane == 0) r = atomicAdd(a.rec_count, 1u);
         r = __shfl_sync(FULL, r, 0);
         if (r < a.rec_cap && nvis <= a.viscap) {
-          const ResumeLayout ly = resume_layout(L, a.Ccap, a.logcap, a.viscap);
+          const ResumeLayout ly = resume_layout(a.L, a.Ccap, a.logcap, a.viscap);
           uint32_t* rec = a.rec_pool + (size_t)r * a.rec_words;
           if (lane == 0) {
             rec[0] = qi; rec[1] = (uint32_t)fn; rec[2] = (uint32_t)cn; rec[3] = (uint32_t)nvis;
@@ -418,11 +434,14 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       __syncwarp();
       continue;
     }
-    if ((uint32_t)fn < a.k) status |= QS_SHORT;
+    if ((uint32_t)fn < kq) status |= QS_SHORT;
+    uint32_t* const oid = a.out_ids + (uint64_t)qi * a.kstride;
+    float* const odist = a.out_dists ? a.out_dists + (uint64_t)qi * a.kstride : nullptr;
     if (PREC != PREC_F32) {
       // re-rank the best min(rerank, fn) entries by exact float32 distance
       // (beam_search_rerank's full-precision pass, beamSearch.h:569-587)
-      const int nr = (int)min((uint32_t)fn, a.rerank > a.k ? a.rerank : a.k);
+      const uint32_t rr = a.qk ? 4 * kq : a.rerank;
+      const int nr = (int)min((uint32_t)fn, rr > kq ? rr : kq);
       for (int b = 0; b < nr; b += 64) {
         const int i0 = b + lane, i1 = b + 32 + lane;
         float d0 = 0.f, d1 = 0.f;
@@ -442,20 +461,20 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
         const uint64_t ki = fr2[i];
         int r = 0;
         for (int j = 0; j < nr; j++) r += fr2[j] < ki;
-        if ((uint32_t)r < a.k) {
-          a.out_ids[(uint64_t)qi * a.k + r] = key_id(ki);
-          if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + r] = key_dist(ki);
+        if ((uint32_t)r < kq) {
+          oid[r] = key_id(ki);
+          if (odist) odist[r] = key_dist(ki);
         }
       }
-      for (uint32_t j = (uint32_t)nr + lane; j < a.k; j += 32) {
-        a.out_ids[(uint64_t)qi * a.k + j] = PANN_PAD;
-        if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = 0.0f;
+      for (uint32_t j = min((uint32_t)nr, kq) + lane; j < a.kstride; j += 32) {
+        oid[j] = PANN_PAD;
+        if (odist) odist[j] = 0.0f;
       }
     } else {
-      for (uint32_t j = lane; j < a.k; j += 32) {
-        bool ok = j < (uint32_t)fn;
-        a.out_ids[(uint64_t)qi * a.k + j] = ok ? key_id(fr[j]) : PANN_PAD;
-        if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = ok ? key_dist(fr[j]) : 0.0f;
+      for (uint32_t j = lane; j < a.kstride; j += 32) {
+        bool ok = j < (uint32_t)fn && j < kq;
+        oid[j] = ok ? key_id(fr[j]) : PANN_PAD;
+        if (odist) odist[j] = ok ? key_dist(fr[j]) : 0.0f;
       }
     }
     if (lane == 0) {

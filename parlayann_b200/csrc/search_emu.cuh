@@ -257,7 +257,6 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
   }
   const uint32_t vmask = e.vs_slots - 1;
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
-  const uint32_t L = a.L;
 
   for (;;) {
     uint32_t job = 0;
@@ -266,16 +265,19 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     if (job >= njobs) break;
     const uint32_t qi = a.job_list ? a.job_list[job] : job;
     const uint32_t rec_id = e.job_rec ? e.job_rec[job] : PANN_PAD;
+    const uint32_t L = a.qL ? a.qL[qi] : a.L;  // this query's beam
+    const uint32_t kq = a.qk ? a.qk[qi] : a.k;
+    const uint32_t bits0 = a.qL ? ref_bits(L, a.dl) : e.bits0;
     const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
     const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
     stage_query<DT, MT>(qs, qsrc, (int)a.nchunks, lane);
-    for (uint32_t i = lane; i < (1u << e.bits0); i += 32) tabA[i] = PANN_PAD;
+    for (uint32_t i = lane; i < (1u << bits0); i += 32) tabA[i] = PANN_PAD;
     for (uint32_t i = lane; i < e.vs_slots; i += 32) vset[i] = PANN_PAD;
     __syncwarp();
     __threadfence_block();
     EmuHash h;
     h.cur = tabA; h.other = tabB; h.cur_cap = e.capA; h.other_cap = e.capB;
-    h.bits = e.bits0; h.num_entries = 0;
+    h.bits = bits0; h.num_entries = 0;
     bool ok = true;
     bool sdummy;
     int32_t qq = 0;
@@ -440,11 +442,14 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       __syncwarp();
       continue;
     }
-    if ((uint32_t)fn < a.k) status |= QS_SHORT;
-    for (uint32_t j = lane; j < a.k; j += 32) {
-      bool okk = j < (uint32_t)fn;
-      a.out_ids[(uint64_t)qi * a.k + j] = okk ? key_id(fr[j]) : PANN_PAD;
-      if (a.out_dists) a.out_dists[(uint64_t)qi * a.k + j] = okk ? key_dist(fr[j]) : 0.0f;
+    // a query handed over before its table could cross the growth threshold
+    // may finish without the reference's hashset ever growing
+    if (h.bits == bits0) status &= ~(uint32_t)QS_REF_WOULD_GROW;
+    if ((uint32_t)fn < kq) status |= QS_SHORT;
+    for (uint32_t j = lane; j < a.kstride; j += 32) {
+      bool okk = j < (uint32_t)fn && j < kq;
+      a.out_ids[(uint64_t)qi * a.kstride + j] = okk ? key_id(fr[j]) : PANN_PAD;
+      if (a.out_dists) a.out_dists[(uint64_t)qi * a.kstride + j] = okk ? key_dist(fr[j]) : 0.0f;
     }
     if (lane == 0) {
       if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;
