@@ -124,6 +124,37 @@ int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, cons
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
                        uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
 
+/* pann_search_device that allocates no device memory. This entry point has
+ * no counterpart in the reference. It is for callers that must not call
+ * cudaMalloc / cudaFree while they serve queries: cudaFree waits for the whole
+ * device to go idle (stalling every other stream on it), a framework's
+ * caching allocator may already hold the device's memory, and a latency-bound
+ * request path cannot afford an allocation that only its first large batch
+ * would trigger.
+ *
+ * Same arguments, results and status bits as pann_search_device (the same
+ * ids, distances, visited and comparison counts). All working memory comes
+ * from one statically declared device array of PANN_NOALLOC_SCRATCH_BYTES,
+ * which every device that loads this library holds until the process exits;
+ * the call makes no cudaMalloc / cudaFree and calls no allocating library
+ * routine. A call whose working set does not fit (too many queries, or a
+ * beam and degree limit whose seen tables are too large) returns PANN_EINVAL
+ * with a message giving the bytes needed; split the batch.
+ *  - The first call on each device looks up the array's device address
+ *    (which may load the module that holds it) with that device current;
+ *    make that first call before any stream capture. The index's device must
+ *    be the current device.
+ *  - Every call shares the array and finds the previous call's contents in
+ *    it; each call clears what must start at zero. Calls that overlap on the
+ *    GPU (on different streams, or for different indexes on one device) race
+ *    on the array: serialise them (one stream, or an event between).
+ *  - The index's own buffers are not used, so it mixes freely with the other
+ *    entry points on one index. */
+#define PANN_NOALLOC_SCRATCH_BYTES (32u << 20)
+int pann_search_device_noalloc(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
+                               const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
+                               uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
+
 /* Beam search returning the reference's full per-query output: the final
  * frontier (<= beam entries, sorted by (distance, id)) and the visited list
  * (sorted by (distance, id)), as filtered_beam_search returns them

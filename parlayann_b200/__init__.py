@@ -26,6 +26,7 @@ PANN_OK, PANN_EINVAL, PANN_ENOMEM, PANN_ETIMEOUT, PANN_EDEVICE, PANN_EOVERFLOW, 
 U8, I8, F32 = 0, 1, 2
 L2, MIPS = 0, 1
 PREC_F32, PREC_BF16, PREC_FP8 = 0, 1, 2
+PANN_NOALLOC_SCRATCH_BYTES = 32 << 20  # static scratch of pann_search_device_noalloc, per device
 _DTYPES = {np.dtype(np.uint8): U8, np.dtype(np.int8): I8, np.dtype(np.float32): F32}
 _NP_OF = {U8: np.uint8, I8: np.int8, F32: np.float32}
 
@@ -94,6 +95,7 @@ SIGNATURES = {
     "pann_graph_save": (_I, [_P, ctypes.c_char_p]),
     "pann_search": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P]),
     "pann_search_device": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P, _P]),
+    "pann_search_device_noalloc": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _P, _P, _P]),
     "pann_search_lists": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), _P, _U32, _P, _P, _P, _U32, _P, _P, _P,
                                _P]),
     "pann_index_set_precision": (_I, [_P, _I]),
