@@ -198,6 +198,54 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
                    float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags, int on_device,
                    void* stream);
 
+/* ---------------------------------------------------------------- batched form */
+
+/* A batch object: a reusable launch sequence for many queries whose k and beam
+ * differ per query, with its device buffers allocated once. The reference runs
+ * such mixes as one parlay::parallel_for over beam_search calls with
+ * different QueryParams (beamSearch.h:492-526); here every run is one
+ * persistent, work-stealing launch per tier in which queries are taken
+ * longest-beam first, optionally replayed from a CUDA graph captured on the
+ * first run. Per query the results equal pann_search's with QueryParams
+ * (k[i], beam[i], limit, degree_limit, batch_factor) — exact, bit for bit, on
+ * the PANN_PREC_F32 path.
+ *
+ * bounds->k / bounds->beam are the largest k and beam any run may use (output
+ * rows have bounds->k entries; entries past a query's own k are PAD /
+ * 0.0f); bounds->limit, degree_limit and batch_factor apply to every query.
+ * opt may be NULL (exact float32). */
+typedef struct pann_batch pann_batch;
+
+typedef struct {
+  int32_t use_graph; /* capture the device launch sequence as a CUDA graph on the first run, replay it after */
+  int32_t autotune;  /* time tier-0 seen-table sizes and warps per block on the first run, keep the fastest */
+  uint32_t seen_slots;      /* tier-0 seen-table slots (power of two; 0 = automatic) */
+  uint32_t warps_per_block; /* tier-0 warps per block (1, 2 or 4; 0 = automatic) */
+} pann_batch_options;
+
+int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, const pann_query_params* bounds,
+                      const uint32_t* starts, uint32_t n_start, const pann_search_options* opt,
+                      const pann_batch_options* bopt);
+
+/* Run nq <= max_queries queries. k and beam are HOST arrays of nq entries
+ * (checked: 1 <= k[i] <= beam[i] <= bounds->beam, k[i] <= bounds->k,
+ * beam[i] >= n_start). on_device != 0: queries and outputs are device memory
+ * and the call is asynchronous on `stream`; else host memory and the call
+ * returns when the results are in place. out_ids / out_dists rows have
+ * bounds->k entries. out_flags as in pann_search_device (device) or
+ * pann_search (host). */
+int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32_t* k, const uint32_t* beam,
+                   uint32_t* out_ids, float* out_dists, uint32_t* out_visited, uint32_t* out_cmps,
+                   uint32_t* out_flags, int on_device, void* stream);
+
+/* The launch configuration in use (after autotuning, if any): tier-0 seen
+ * slots, warps per block, blocks, and whether a CUDA graph is replayed.
+ * Any pointer may be NULL. */
+int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps_per_block, uint32_t* blocks,
+                      int32_t* graph_captured);
+
+int pann_batch_destroy(pann_batch* b);
+
 /* ---------------------------------------------------------------- build */
 
 /* Vamana batch-insertion build into the index's graph (knn_index::build_index,

@@ -55,6 +55,13 @@ class SearchOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32)]
 
 
+class BatchOptions(ctypes.Structure):
+    """pann_batch_options: CUDA-graph replay, autotuning, fixed tier-0 shape."""
+
+    _fields_ = [("use_graph", ctypes.c_int32), ("autotune", ctypes.c_int32), ("seen_slots", ctypes.c_uint32),
+                ("warps_per_block", ctypes.c_uint32)]
+
+
 class BuildParams(ctypes.Structure):
     """BuildParams fields of the Vamana build (types.h:155-230)."""
 
@@ -101,6 +108,11 @@ SIGNATURES = {
     "pann_index_set_precision": (_I, [_P, _I]),
     "pann_search_ex": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.POINTER(SearchOptions), _P, _U32, _P,
                             _P, _P, _P, _P, _I, _P]),
+    "pann_batch_create": (_I, [ctypes.POINTER(_P), _P, _U32, ctypes.POINTER(QueryParams), _P, _U32,
+                               ctypes.POINTER(SearchOptions), ctypes.POINTER(BatchOptions)]),
+    "pann_batch_run": (_I, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pann_batch_config": (_I, [_P, _P, _P, _P, _P]),
+    "pann_batch_destroy": (_I, [_P]),
     "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
     "pann_groundtruth": (_I, [_P, _P, _U32, _U32, _P, _P]),
     "pann_last_error": (ctypes.c_char_p, []),
@@ -269,6 +281,14 @@ class Index:
             _check(rc)
         return SearchResult(ids, dists, vis, cmps, flags)
 
+    def batch(self, max_queries: int, max_k: int, max_beam: int, limit: int | None = None,
+              degree_limit: int | None = None, batch_factor: float = 0.125, starts=(0,), precision: int = PREC_F32,
+              rerank: int = 0, use_graph: bool = True, autotune: bool = False, seen_slots: int = 0,
+              warps_per_block: int = 0) -> "Batch":
+        """A reusable batch for queries with per-query k and beam (pann_batch_create)."""
+        return Batch(self, max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts, precision, rerank,
+                     use_graph, autotune, seen_slots, warps_per_block)
+
     def search_lists(self, queries: np.ndarray, L: int, limit: int | None = None, degree_limit: int | None = None,
                      batch_factor: float = 0.125, starts=(0,), visited_cap: int | None = None):
         """Full beam_search output: frontier (<= L) and sorted visited list per query."""
@@ -295,6 +315,62 @@ class Index:
         dd = np.empty((queries.shape[0], k), np.float64)
         _check(lib().pann_groundtruth(self._h, _ptr(queries), queries.shape[0], k, _ptr(ids), _ptr(dd)))
         return ids, dd
+
+
+class Batch:
+    """Batched form: runs of up to max_queries queries, each with its own k and
+    beam, through one persistent launch sequence (optionally a replayed CUDA
+    graph). Per query the results equal Index.search with that k and beam."""
+
+    def __init__(self, index: "Index", max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts,
+                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block):
+        self.index = index
+        self.max_k = max_k
+        qp = QueryParams(max_k, max_beam, index.n if limit is None else limit,
+                         index.R if degree_limit is None else degree_limit, batch_factor)
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+        opt = SearchOptions(precision, rerank)
+        bo = BatchOptions(int(use_graph), int(autotune), seen_slots, warps_per_block)
+        h = ctypes.c_void_p()
+        _check(lib().pann_batch_create(ctypes.byref(h), index.handle, max_queries, ctypes.byref(qp), _ptr(st), len(st),
+                                       ctypes.byref(opt), ctypes.byref(bo)))
+        self._h = h
+
+    def run(self, queries: np.ndarray, k, beam, allow_short: bool = False) -> SearchResult:
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.index.dtype])
+        nq = queries.shape[0]
+        k = np.ascontiguousarray(np.broadcast_to(np.asarray(k, np.uint32), (nq,)))
+        beam = np.ascontiguousarray(np.broadcast_to(np.asarray(beam, np.uint32), (nq,)))
+        ids = np.empty((nq, self.max_k), np.uint32)
+        dists = np.empty((nq, self.max_k), np.float32)
+        vis = np.empty(nq, np.uint32)
+        cmps = np.empty(nq, np.uint32)
+        flags = np.empty(nq, np.uint32)
+        rc = lib().pann_batch_run(self._h, _ptr(queries), nq, _ptr(k), _ptr(beam), _ptr(ids), _ptr(dists), _ptr(vis),
+                                  _ptr(cmps), _ptr(flags), 0, None)
+        if not (allow_short and rc == PANN_ESHORT):
+            _check(rc)
+        return SearchResult(ids, dists, vis, cmps, flags)
+
+    def config(self) -> dict:
+        s, w, b, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int32()
+        _check(lib().pann_batch_config(self._h, ctypes.byref(s), ctypes.byref(w), ctypes.byref(b), ctypes.byref(g)))
+        return dict(seen_slots=s.value, warps_per_block=w.value, blocks=b.value, graph=bool(g.value))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().pann_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def recall_at_k(ids: np.ndarray, gt_ids: np.ndarray, k: int) -> float:

@@ -1,0 +1,336 @@
+// Batched form: many queries with their own k and beam in one launch sequence
+// (include/parlayann_b200.h, pann_batch_*).
+//
+// The reference serves such a mix as a parlay::parallel_for over beam_search
+// calls, each with its own QueryParams (beamSearch.h:492-526). Here the tiers
+// of the exact search run once per batch: every query carries its k and beam
+// (SearchArgs::qk / qL), the shared-memory state is sized for the largest, and
+// the persistent first tier takes queries longest-beam first so that the long
+// searches do not trail at the end. The buffers are allocated when the batch
+// is created, so the device launch sequence has fixed arguments and can be
+// captured once as a CUDA graph and replayed. The tier-0 seen-table size and
+// warps per block, the two knobs that trade occupancy against table
+// overflow, can be picked by timing them on the first batch.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "index.cuh"
+#include "tiers.cuh"
+
+struct pann_batch {
+  pann_index* idx = nullptr;
+  pann::SearchPlan plan{};
+  uint32_t max_q = 0;
+  int prec = 0;
+  uint32_t rerank = 0;
+  pann_batch_options bopt{};
+  pann::TierSizes z{};
+  // device buffers, allocated at creation
+  pann::DevBuf q, qk, qL, order, ids, dists, vis, cmps, status, counters, redo, spill, handoff, gt2, ge2, starts;
+  // pinned host staging for the per-query arrays (k, beam, order, nq)
+  uint32_t* h_stage = nullptr;
+  cudaEvent_t staged = nullptr;  // the last upload from h_stage has completed
+  cudaStream_t cap = nullptr;    // capture stream
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int runs = 0;
+};
+
+namespace pann {
+
+int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan);
+
+static int ensure_tier_buffers(pann_batch* b, const TierSizes& z) {
+  PANN_CUDA(b->spill.ensure(std::max<size_t>(z.spill_bytes, 16)));
+  if (b->prec == PREC_F32) PANN_CUDA(b->handoff.ensure(std::max<size_t>(z.handoff_bytes, 16)));
+  PANN_CUDA(b->gt2.ensure(z.t2_bytes));
+  if (b->prec == PREC_F32) PANN_CUDA(b->ge2.ensure(z.e2_bytes));
+  return PANN_OK;
+}
+
+static TierBufs tier_bufs(pann_batch* b) {
+  const uint32_t m = b->max_q;
+  TierBufs t{};
+  t.cnt = b->counters.as<uint32_t>();
+  t.redo0 = b->redo.as<uint32_t>();
+  t.redo1 = t.redo0 + m;
+  t.emu = t.redo1 + m;
+  t.ovf = t.emu + m;
+  t.emu_rec = t.ovf + m;
+  t.ovf_rec = t.emu_rec + m;
+  t.gspill = b->spill.as<uint32_t>();
+  t.handoff = b->prec == PREC_F32 ? b->handoff.as<uint32_t>() : nullptr;
+  t.gt2 = b->gt2.as<uint32_t>();
+  t.ge2 = b->prec == PREC_F32 ? b->ge2.as<uint32_t>() : nullptr;
+  t.job_list0 = b->order.as<uint32_t>();
+  t.njobs0 = b->counters.as<uint32_t>() + 32;  // outside the words every enqueue clears
+  return t;
+}
+
+// The device launch sequence of one run over the batch's own buffers; the
+// number of queries is read from device memory, so one capture serves every nq.
+static int enqueue(pann_batch* b, const TierSizes& z, cudaStream_t st) {
+  pann_index* idx = b->idx;
+  SearchArgs a = base_args(idx, b->plan, b->q.as<uint8_t>(), nullptr, b->max_q, b->starts.as<uint32_t>(),
+                           b->ids.as<uint32_t>(), b->dists.as<float>(), b->vis.as<uint32_t>(), b->cmps.as<uint32_t>(),
+                           b->status.as<uint32_t>(), nullptr, 0);
+  a.qk = b->qk.as<uint32_t>();
+  a.qL = b->qL.as<uint32_t>();
+  a.kstride = b->plan.k;
+  return enqueue_tiers(idx, b->plan, a, z, tier_bufs(b), st, b->prec, b->rerank);
+}
+
+// Picks the tier-0 seen-table slots and warps per block by timing each
+// candidate on the staged batch (two timed runs each, the faster counts).
+static int autotune(pann_batch* b, cudaStream_t st) {
+  const uint32_t base_S = b->z.S;
+  const uint32_t floor_S = 4 * (b->idx->R + 1);
+  std::vector<std::pair<uint32_t, int>> cands;
+  for (uint32_t S : {base_S / 2, base_S, base_S * 2})
+    for (int w : {2, 4})
+      if (S >= floor_S && S <= 16384) cands.push_back({S, w});
+  cudaEvent_t e0, e1;
+  PANN_CUDA(cudaEventCreate(&e0));
+  PANN_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  TierSizes best_z = b->z;
+  int rc = PANN_OK;
+  for (auto& c : cands) {
+    TierSizes z;
+    if (size_tiers(b->idx, b->plan, b->max_q, b->prec, c.first, c.second, &z) != PANN_OK) continue;
+    if (z.S != c.first || z.wpb != c.second) continue;  // did not fit as asked
+    if ((rc = ensure_tier_buffers(b, z)) != PANN_OK) break;
+    float t_min = 1e30f;
+    for (int rep = 0; rep < 3 && rc == PANN_OK; rep++) {
+      cudaEventRecord(e0, st);
+      rc = enqueue(b, z, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "autotune run");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) t_min = std::min(t_min, ms);  // the first run warms the caches
+    }
+    if (rc) break;
+    if (t_min < best) {
+      best = t_min;
+      best_z = z;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->z = best_z;
+  return PANN_OK;
+}
+
+}  // namespace pann
+
+using namespace pann;
+
+extern "C" {
+
+int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, const pann_query_params* bounds,
+                      const uint32_t* starts, uint32_t n_start, const pann_search_options* opt,
+                      const pann_batch_options* bopt) {
+  if (!out) return fail(PANN_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points (pann_index_set_points)");
+  if (max_queries == 0) return fail(PANN_EINVAL, "max_queries must be positive");
+  if (!starts) return fail(PANN_EINVAL, "start points are NULL");
+  for (uint32_t i = 0; i < n_start; i++) {
+    if ((uint64_t)starts[i] >= idx->n) return fail(PANN_EINVAL, "start point id out of range");
+    for (uint32_t j = 0; j < i; j++)
+      if (starts[j] == starts[i]) return fail(PANN_EINVAL, "duplicate start point");
+  }
+  SearchPlan plan;
+  int rc = make_plan(idx, bounds, n_start, &plan);
+  if (rc) return rc;
+  if (plan.k == 0) return fail(PANN_EINVAL, "bounds->k must be positive");
+  // any query may defer candidates (its own beam is at most the bound)
+  plan.Ccap = (uint32_t)std::floor(plan.bf * (double)plan.L) + std::min(plan.dl, idx->R) + 1;
+  const int prec = opt ? opt->precision : PANN_PREC_F32;
+  if (prec != PANN_PREC_F32 && idx->lp_prec != prec)
+    return fail(PANN_EINVAL, "call pann_index_set_precision for this precision first");
+
+  pann_batch* b = new pann_batch();
+  b->idx = idx;
+  b->plan = plan;
+  b->max_q = max_queries;
+  b->prec = prec;
+  b->rerank = opt ? opt->rerank : 0;
+  if (bopt) b->bopt = *bopt;
+  auto bail = [&](int code) {
+    pann_batch_destroy(b);
+    return code;
+  };
+  rc = size_tiers(idx, plan, max_queries, prec, b->bopt.seen_slots, (int)b->bopt.warps_per_block, &b->z);
+  if (rc) return bail(rc);
+  const size_t m = max_queries;
+  cudaError_t e = cudaSuccess;
+  auto need = [&](DevBuf& d, size_t bytes) {
+    if (e == cudaSuccess) e = d.ensure(std::max<size_t>(bytes, 16));
+  };
+  need(b->q, idx->stride * m);
+  need(b->qk, 4 * m);
+  need(b->qL, 4 * m);
+  need(b->order, 4 * m);
+  need(b->ids, 4 * m * plan.k);
+  need(b->dists, 4 * m * plan.k);
+  need(b->vis, 4 * m);
+  need(b->cmps, 4 * m);
+  need(b->status, 4 * m);
+  need(b->counters, 4 * 64);
+  need(b->redo, 4 * 6 * m);
+  need(b->starts, 4ull * std::max<uint32_t>(n_start, 1));
+  if (e != cudaSuccess) return bail(cuda_fail(e, "batch buffers"));
+  if ((rc = ensure_tier_buffers(b, b->z)) != PANN_OK) return bail(rc);
+  e = cudaMallocHost(&b->h_stage, 4 * (3 * m + 1));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMemcpy(b->starts.p, starts, 4ull * n_start, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(b->q.p, 0, idx->stride * m);  // zero row padding once
+  if (e != cudaSuccess) return bail(cuda_fail(e, "batch setup"));
+  *out = b;
+  return PANN_OK;
+}
+
+int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32_t* k, const uint32_t* beam,
+                   uint32_t* out_ids, float* out_dists, uint32_t* out_visited, uint32_t* out_cmps,
+                   uint32_t* out_flags, int on_device, void* stream) {
+  if (!b) return fail(PANN_EINVAL, "batch is NULL");
+  if (nq > b->max_q) return fail(PANN_EINVAL, "nq = " + std::to_string(nq) + " exceeds the batch's max_queries = " +
+                                                  std::to_string(b->max_q));
+  if (nq == 0) return PANN_OK;
+  if (!queries || !out_ids || !k || !beam) return fail(PANN_EINVAL, "queries, out_ids, k or beam is NULL");
+  const SearchPlan& p = b->plan;
+  for (uint32_t i = 0; i < nq; i++) {
+    if (k[i] == 0 || k[i] > p.k) return fail(PANN_EINVAL, "query " + std::to_string(i) + ": k must be in [1, bounds->k]");
+    if (beam[i] < k[i])
+      return fail(PANN_EINVAL, "query " + std::to_string(i) + ": beam search parameter Q = " + std::to_string(beam[i]) +
+                                   " same size or smaller than k = " + std::to_string(k[i]));
+    if (beam[i] > p.L) return fail(PANN_EINVAL, "query " + std::to_string(i) + ": beam exceeds bounds->beam");
+    if (beam[i] < p.n_start)
+      return fail(PANN_EINVAL, "query " + std::to_string(i) + ": beam search has more starting points than beam size");
+  }
+  pann_index* idx = b->idx;
+  cudaStream_t st = on_device ? static_cast<cudaStream_t>(stream) : idx->stream;
+  // stage k, beam, the longest-beam-first order and nq (counting sort on beam)
+  PANN_CUDA(cudaEventSynchronize(b->staged));  // the previous run's upload is done with h_stage
+  uint32_t* hk = b->h_stage;
+  uint32_t* hL = hk + b->max_q;
+  uint32_t* ho = hL + b->max_q;
+  uint32_t* hn = ho + b->max_q;
+  std::memcpy(hk, k, 4ull * nq);
+  std::memcpy(hL, beam, 4ull * nq);
+  {
+    std::vector<uint32_t> count(p.L + 2, 0);
+    for (uint32_t i = 0; i < nq; i++) count[p.L - beam[i]]++;
+    uint32_t acc = 0;
+    for (auto& c : count) {
+      uint32_t t = c;
+      c = acc;
+      acc += t;
+    }
+    for (uint32_t i = 0; i < nq; i++) ho[count[p.L - beam[i]]++] = i;
+  }
+  *hn = nq;
+  const size_t rb = (size_t)idx->d * idx->esize;
+  PANN_CUDA(cudaMemcpy2DAsync(b->q.p, idx->stride, queries, rb, rb, nq,
+                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(b->qk.p, hk, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(b->qL.p, hL, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(b->order.p, ho, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(b->counters.as<uint32_t>() + 32, hn, 4, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaEventRecord(b->staged, st));
+
+  int rc = PANN_OK;
+  if (b->runs == 0 && b->bopt.autotune && !b->bopt.seen_slots && !b->bopt.warps_per_block) {
+    rc = autotune(b, st);
+    if (rc) return rc;
+  }
+  if (b->exec) {
+    PANN_CUDA(cudaGraphLaunch(b->exec, st));
+  } else {
+    rc = enqueue(b, b->z, st);
+    if (rc) return rc;
+    if (b->bopt.use_graph) {
+      // capture after an eager run, so every kernel is already loaded
+      PANN_CUDA(cudaStreamSynchronize(st));
+      PANN_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+      rc = enqueue(b, b->z, b->cap);
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+      ce = cudaGraphInstantiate(&b->exec, g, 0);
+      if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        b->exec = nullptr;
+        return cuda_fail(ce, "cudaGraphInstantiate");
+      }
+      b->graph = g;
+    }
+  }
+  b->runs++;
+  // results out of the batch's buffers
+  const size_t kb = 4ull * p.k * nq;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  PANN_CUDA(cudaMemcpyAsync(out_ids, b->ids.p, kb, kind, st));
+  if (out_dists) PANN_CUDA(cudaMemcpyAsync(out_dists, b->dists.p, kb, kind, st));
+  if (out_visited) PANN_CUDA(cudaMemcpyAsync(out_visited, b->vis.p, 4ull * nq, kind, st));
+  if (out_cmps) PANN_CUDA(cudaMemcpyAsync(out_cmps, b->cmps.p, 4ull * nq, kind, st));
+  if (on_device) {
+    if (out_flags) PANN_CUDA(cudaMemcpyAsync(out_flags, b->status.p, 4ull * nq, kind, st));
+    return PANN_OK;
+  }
+  std::vector<uint32_t> status(nq);
+  PANN_CUDA(cudaMemcpyAsync(status.data(), b->status.p, 4ull * nq, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  int rc2 = PANN_OK;
+  for (uint32_t i = 0; i < nq; i++) {
+    uint32_t s = status[i];
+    if (out_flags) out_flags[i] = (s & QS_REF_WOULD_GROW) ? 1u : 0u;
+    if (s & (QS_TABLE_FULL | QS_INTERNAL)) rc2 = PANN_EOVERFLOW;
+    else if ((s & QS_SHORT) && rc2 == PANN_OK) rc2 = PANN_ESHORT;
+  }
+  if (rc2 == PANN_EOVERFLOW) return fail(rc2, "a query's seen-set outgrew the largest table");
+  if (rc2 == PANN_ESHORT) return fail(rc2, "beam search returned fewer than k results");
+  return PANN_OK;
+}
+
+int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps_per_block, uint32_t* blocks,
+                      int32_t* graph_captured) {
+  if (!b) return fail(PANN_EINVAL, "batch is NULL");
+  if (seen_slots) *seen_slots = b->z.S;
+  if (warps_per_block) *warps_per_block = (uint32_t)b->z.wpb;
+  if (blocks) *blocks = (uint32_t)b->z.blocks;
+  if (graph_captured) *graph_captured = b->exec != nullptr;
+  return PANN_OK;
+}
+
+int pann_batch_destroy(pann_batch* b) {
+  if (!b) return PANN_OK;
+  if (b->idx && b->idx->stream) cudaStreamSynchronize(b->idx->stream);
+  if (b->cap) cudaStreamSynchronize(b->cap);
+  if (b->staged) cudaEventSynchronize(b->staged);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (DevBuf* d : {&b->q, &b->qk, &b->qL, &b->order, &b->ids, &b->dists, &b->vis, &b->cmps, &b->status, &b->counters,
+                    &b->redo, &b->spill, &b->handoff, &b->gt2, &b->ge2, &b->starts})
+    d->release();
+  if (b->h_stage) cudaFreeHost(b->h_stage);
+  if (b->staged) cudaEventDestroy(b->staged);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+  return PANN_OK;
+}
+
+}  // extern "C"

@@ -14,6 +14,7 @@
 #include "search.cuh"
 #include "search_emu.cuh"
 #include "lowprec.cuh"
+#include "tiers.cuh"
 
 namespace pann {
 
@@ -147,7 +148,7 @@ static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads,
 }
 
 cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
-                                 int threads, size_t smem, cudaStream_t st, int prec = PREC_F32) {
+                                 int threads, size_t smem, cudaStream_t st, int prec) {
   if (prec != PREC_F32) {
     if (dtype != DT_F32) return cudaErrorInvalidValue;
 #define PANN_LP_CASE(MT, PR)                                                               \
@@ -251,26 +252,179 @@ uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
 // global spill table; (2) queries whose tables still filled up, with one large
 // global table per warp; (E) queries on which the reference's hashset grows,
 // re-run with that hashset emulated exactly.
-int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
-               uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
-               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
-               int precision, uint32_t rerank) {
-  if (nq == 0) return PANN_OK;
-  // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
-  // [5] shared-memory emulation job counter, [6] emulation list length,
-  // [7] global emulation job counter, [8] emulation overflow count,
-  // [9] resume records taken
-  PANN_CUDA(idx->counters.ensure(64));
-  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)nq));
-  uint32_t* cnt = idx->counters.as<uint32_t>();
-  uint32_t* redo0 = idx->redo.as<uint32_t>();
-  uint32_t* redo1 = redo0 + nq;
-  uint32_t* emu = redo1 + nq;
-  uint32_t* ovf = emu + nq;
-  uint32_t* emu_rec = ovf + nq;
-  uint32_t* ovf_rec = emu_rec + nq;
-  PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
+int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int precision, uint32_t S_force,
+               int wpb_force, TierSizes* z) {
+  const size_t smem_cap = idx->smem_optin;
+  TierSizes& t = *z;
+  t = TierSizes{};
+  // ---- tier 0
+  uint32_t S = S_force ? std::max<uint32_t>(pow2_at_least(S_force), pow2_at_least(4ull * (idx->R + 1)))
+                       : tier0_slots(plan, idx->R);
+  uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
+  int wpb = wpb_force > 0 ? std::min(wpb_force, 4) : 4;
+  while (wpb > 1 && (size_t)wb * wpb > smem_cap) wpb >>= 1;
+  while ((size_t)wb * wpb > smem_cap && S > pow2_at_least(4ull * (idx->R + 1))) {
+    S >>= 1;
+    wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
+  }
+  if ((size_t)wb * wpb > smem_cap) return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
+  int occ = precision == PREC_F32 ? search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb)
+                                  : lp_occupancy(idx->metric, precision, 32 * wpb, (size_t)wb * wpb);
+  if (occ <= 0) occ = 1;
+  uint64_t want = (std::max<uint64_t>(nq, 1) + wpb - 1) / wpb;
+  t.S = S;
+  t.wb = wb;
+  t.wpb = wpb;
+  t.blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
+  t.slots = (size_t)t.blocks * wpb;
+  uint32_t Sg = std::max<uint32_t>(4 * S, pow2_at_least(2ull * plan.ref_half));
+  while (Sg > 4 * S && t.slots * Sg * 4 > (1ull << 30)) Sg >>= 1;
+  t.Sg = Sg;
+  t.spill_bytes = t.slots * Sg * 4;
+  // ---- hand-off buffers: per-warp insertion/visit logs and the resume records
+  t.logcap = plan.ref_half;
+  t.viscap = pow2_at_least(8ull * plan.L + 64);
+  t.ly = resume_layout(plan.L, plan.Ccap, t.logcap, t.viscap);
+  t.rec_cap = std::min<uint64_t>(std::max<uint64_t>(nq, 1), std::max<uint64_t>(64, (256ull << 20) / (4ull * t.ly.words)));
+  t.handoff_bytes = 4ull * (t.slots * (size_t)(t.logcap + t.viscap) + t.rec_cap * t.ly.words);
+  // ---- tier 2
+  t.S2 = std::min<uint32_t>(std::max<uint32_t>(1u << 16, pow2_at_least(4ull * plan.ref_half)), 1u << 24);
+  t.t2_slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * idx->sm_count, (256ull << 20) / (4ull * t.S2)));
+  t.wb2 = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, t.S2, true);
+  t.t2_bytes = (size_t)t.t2_slots * t.S2 * 4;
+  // ---- emulation tiers
+  double cap_n = 2.0 * (10.0 + (double)plan.L) * (double)plan.dl;
+  t.bits0 = (uint32_t)std::ceil(std::log2(cap_n));
+  t.S0 = 1ull << t.bits0;
+  t.vs = pow2_at_least(8ull * plan.L + 64);
+  t.base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, true);
+  t.emu_smem_need = emu_smem_bytes(t.base, t.vs, (uint32_t)(4 * t.S0), (uint32_t)(2 * t.S0), true);
+  t.emu_smem = t.emu_smem_need <= smem_cap && 4 * t.S0 < (1ull << 31);
+  t.capA = 16 * t.S0;
+  t.capB = 8 * t.S0;
+  size_t per_slot = 4ull * (t.capA + t.capB);
+  t.e2_slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(idx->sm_count, (1ull << 30) / per_slot));
+  t.e2_bytes = per_slot * t.e2_slots;
+  return PANN_OK;
+}
 
+int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a0, const TierSizes& z,
+                  const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank) {
+  uint32_t* cnt = b.cnt;
+  PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
+  SearchArgs a = a0;
+  a.emu_list = b.emu;
+  a.emu_rec = b.emu_rec;
+  a.emu_count = cnt + 6;
+  if (precision != PREC_F32) {
+    if (idx->lp_prec != precision) return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
+    a.emu_list = nullptr;  // the precision form is not a reference path: no hashset emulation
+    a.lp_rows = idx->lp_rows.as<uint8_t>();
+    a.lp_stride = idx->lp_stride;
+    a.lp_chunks = idx->lp_chunks;
+    a.lp_scales = idx->lp_scales.as<float>();
+    a.rerank = rerank;  // 0: 4k per query
+  }
+  // ---- tier 0: many warps per SM, a modest shared-memory seen table that
+  // spills into a per-warp global table for the queries that outgrow it
+  {
+    SearchArgs t = a;
+    t.S = z.S;
+    t.warp_bytes = z.wb;
+    t.job_counter = cnt + 0;
+    t.job_list = b.job_list0;
+    t.njobs_dev = b.njobs0;
+    t.redo_list = b.redo0;
+    t.redo_count = cnt + 3;
+    if (b.handoff) {
+      t.inslog = b.handoff;
+      t.logcap = z.logcap;
+      t.vislog = t.inslog + z.slots * (size_t)z.logcap;
+      t.viscap = z.viscap;
+      t.rec_pool = t.vislog + z.slots * (size_t)z.viscap;
+      t.rec_cap = (uint32_t)z.rec_cap;
+      t.rec_words = z.ly.words;
+      t.rec_count = cnt + 9;
+      a.logcap = z.logcap;  // the emulation tiers read the record layout
+      a.viscap = z.viscap;
+      a.rec_pool = t.rec_pool;
+      a.rec_words = z.ly.words;
+    } else {
+      t.inslog = nullptr;
+    }
+    t.gspill = b.gspill;
+    t.Sg = b.gspill ? z.Sg : 0;
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, z.blocks, 32 * z.wpb, (size_t)z.wb * z.wpb, st, precision));
+  }
+  // ---- tier 2: queries whose tables still filled up, with one global-memory
+  // seen table per warp sized above the reference's own capacity
+  {
+    SearchArgs t = a;
+    t.S = z.S2;
+    t.warp_bytes = z.wb2;
+    t.gtables = b.gt2;
+    t.inslog = nullptr;
+    t.job_list = b.redo0;
+    t.njobs_dev = cnt + 3;
+    t.job_counter = cnt + 2;
+    t.redo_list = nullptr;
+    t.redo_count = nullptr;
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, z.t2_slots, 32, z.wb2, st, precision));
+  }
+  if (precision != PREC_F32) return PANN_OK;
+  // ---- tier E: exact emulation of the reference's hashset for flagged queries,
+  // first with the emulated table in shared memory (capacities 4 S0 / 2 S0),
+  // then, for queries that outgrow it, in global memory (16 S0 / 8 S0)
+  {
+    SearchArgs t = a;
+    t.redo_list = nullptr;
+    t.redo_count = nullptr;
+    t.emu_list = nullptr;
+    t.emu_count = nullptr;
+    EmuArgs e{};
+    e.bits0 = z.bits0;
+    e.vs_slots = z.vs;
+    e.base_bytes = z.base;
+    const uint32_t* glist = b.emu;
+    uint32_t* gcount = cnt + 6;
+    const uint32_t* grec = b.emu_rec;
+    if (z.emu_smem) {
+      e.capA = (uint32_t)(4 * z.S0);
+      e.capB = (uint32_t)(2 * z.S0);
+      e.overflow_list = b.ovf;
+      e.overflow_rec = b.ovf_rec;
+      e.overflow_count = cnt + 8;
+      e.job_rec = b.emu_rec;
+      t.job_list = b.emu;
+      t.njobs_dev = cnt + 6;
+      t.job_counter = cnt + 5;
+      PANN_CUDA(launch_emulate(idx->dtype, idx->metric, true, t, e, 2 * idx->sm_count, z.emu_smem_need, st));
+      glist = b.ovf;
+      grec = b.ovf_rec;
+      gcount = cnt + 8;
+    }
+    e.gA = b.ge2;
+    e.gB = e.gA + (size_t)z.e2_slots * z.capA;
+    e.capA = (uint32_t)z.capA;
+    e.capB = (uint32_t)z.capB;
+    e.overflow_list = nullptr;
+    e.overflow_rec = nullptr;
+    e.overflow_count = nullptr;
+    e.job_rec = grec;
+    t.job_list = glist;
+    t.njobs_dev = gcount;
+    t.job_counter = cnt + 7;
+    PANN_CUDA(launch_emulate(idx->dtype, idx->metric, false, t, e, z.e2_slots, emu_smem_bytes(z.base, z.vs, 0, 0, false),
+                             st));
+  }
+  return PANN_OK;
+}
+
+// Fills the search arguments every tier shares.
+SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries,
+                     const uint32_t* d_self_ids, uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids,
+                     float* d_dists, uint32_t* d_vis, uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys,
+                     uint32_t vis_cap) {
   SearchArgs a{};
   a.points = idx->d_points;
   a.stride = idx->stride;
@@ -298,157 +452,51 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   a.out_status = d_status;
   a.vis_keys = d_vis_keys;
   a.vis_cap = vis_cap;
-  a.emu_list = emu;
-  a.emu_rec = emu_rec;
-  a.emu_count = cnt + 6;
-  if (precision != PREC_F32) {
-    if (idx->lp_prec != precision) return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
-    a.emu_list = nullptr;  // the precision form is not a reference path: no hashset emulation
-    a.lp_rows = idx->lp_rows.as<uint8_t>();
-    a.lp_stride = idx->lp_stride;
-    a.lp_chunks = idx->lp_chunks;
-    a.lp_scales = idx->lp_scales.as<float>();
-    a.rerank = rerank ? rerank : 4 * plan.k;
-  }
+  a.opaque_zero = 0;
+  return a;
+}
 
-  const size_t smem_cap = idx->smem_optin;
-  // ---- tier 0: many warps per SM, a modest shared-memory seen table that
-  // spills into a per-warp global table for the queries that outgrow it
-  {
-    uint32_t S = tier0_slots(plan, idx->R);
-    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
-    int wpb = 4;
-    while (wpb > 1 && (size_t)wb * wpb > smem_cap) wpb >>= 1;
-    while ((size_t)wb * wpb > smem_cap && S > pow2_at_least(4ull * (idx->R + 1))) {
-      S >>= 1;
-      wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
-    }
-    if ((size_t)wb * wpb > smem_cap) return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
-    int occ = precision == PREC_F32 ? search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb)
-                                    : lp_occupancy(idx->metric, precision, 32 * wpb, (size_t)wb * wpb);
-    if (occ <= 0) occ = 1;
-    uint64_t want = (nq + wpb - 1) / wpb;
-    int blocks = (int)std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count);
-    uint32_t Sg = std::max<uint32_t>(4 * S, pow2_at_least(2ull * plan.ref_half));
-    size_t slots = (size_t)blocks * wpb;
-    while (Sg > 4 * S && slots * Sg * 4 > (1ull << 30)) Sg >>= 1;
-    SearchArgs t = a;
-    t.S = S;
-    t.warp_bytes = wb;
-    t.job_counter = cnt + 0;
-    t.redo_list = redo0;
-    t.redo_count = cnt + 3;
-    // hand-off buffers: per-warp insertion/visit logs and the resume records
-    {
-      const uint32_t logcap = plan.ref_half;
-      const uint32_t viscap = pow2_at_least(8ull * plan.L + 64);
-      const ResumeLayout ly = resume_layout(plan.L, plan.Ccap, logcap, viscap);
-      uint64_t rec_cap = std::min<uint64_t>(nq, std::max<uint64_t>(64, (256ull << 20) / (4ull * ly.words)));
-      size_t need = 4ull * (slots * (size_t)(logcap + viscap) + rec_cap * ly.words);
-      if (idx->handoff.ensure(need) == cudaSuccess) {
-        t.inslog = idx->handoff.as<uint32_t>();
-        t.logcap = logcap;
-        t.vislog = t.inslog + slots * (size_t)logcap;
-        t.viscap = viscap;
-        t.rec_pool = t.vislog + slots * (size_t)viscap;
-        t.rec_cap = (uint32_t)rec_cap;
-        t.rec_words = ly.words;
-        t.rec_count = cnt + 9;
-        a.logcap = logcap;  // the emulation tiers read the record layout
-        a.viscap = viscap;
-        a.rec_pool = t.rec_pool;
-        a.rec_words = ly.words;
-      } else {
-        cudaGetLastError();
-      }
-    }
-    if (idx->gtables.ensure(slots * Sg * 4) == cudaSuccess) {
-      t.gspill = idx->gtables.as<uint32_t>();
-      t.Sg = Sg;
-    } else {
-      cudaGetLastError();
-      t.gspill = nullptr;
-      t.Sg = 0;
-    }
-    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, blocks, 32 * wpb, (size_t)wb * wpb, st, precision));
+int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
+               uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
+               uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
+               int precision, uint32_t rerank) {
+  if (nq == 0) return PANN_OK;
+  if (precision != PREC_F32 && idx->lp_prec != precision)
+    return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
+  TierSizes z;
+  int rc = size_tiers(idx, plan, nq, precision, 0, 0, &z);
+  if (rc) return rc;
+  // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
+  // [5] shared-memory emulation job counter, [6] emulation list length,
+  // [7] global emulation job counter, [8] emulation overflow count,
+  // [9] resume records taken
+  PANN_CUDA(idx->counters.ensure(64));
+  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)nq));
+  TierBufs b{};
+  b.cnt = idx->counters.as<uint32_t>();
+  b.redo0 = idx->redo.as<uint32_t>();
+  b.redo1 = b.redo0 + nq;
+  b.emu = b.redo1 + nq;
+  b.ovf = b.emu + nq;
+  b.emu_rec = b.ovf + nq;
+  b.ovf_rec = b.emu_rec + nq;
+  // the spill table and the hand-off buffers are optional: without them
+  // queries re-run in the later tiers
+  if (precision == PREC_F32) {
+    if (idx->handoff.ensure(z.handoff_bytes) == cudaSuccess) b.handoff = idx->handoff.as<uint32_t>();
+    else cudaGetLastError();
   }
-  // ---- tier 2: queries whose tables still filled up, with one global-memory
-  // seen table per warp sized above the reference's own capacity
-  {
-    uint32_t S = std::max<uint32_t>(1u << 16, pow2_at_least(4ull * plan.ref_half));
-    S = std::min<uint32_t>(S, 1u << 24);
-    int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(2ull * idx->sm_count, (256ull << 20) / (4ull * S)));
-    PANN_CUDA(idx->gtables2.ensure((size_t)slots * S * 4));
-    uint32_t wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, true);
-    SearchArgs t = a;
-    t.S = S;
-    t.warp_bytes = wb;
-    t.gtables = idx->gtables2.as<uint32_t>();
-    t.inslog = nullptr;
-    t.job_list = redo0;
-    t.njobs_dev = cnt + 3;
-    t.job_counter = cnt + 2;
-    t.redo_list = nullptr;
-    t.redo_count = nullptr;
-    PANN_CUDA(launch_search(idx->dtype, idx->metric, true, t, slots, 32, wb, st, precision));
+  if (idx->gtables.ensure(z.spill_bytes) == cudaSuccess) b.gspill = idx->gtables.as<uint32_t>();
+  else cudaGetLastError();
+  PANN_CUDA(idx->gtables2.ensure(z.t2_bytes));
+  b.gt2 = idx->gtables2.as<uint32_t>();
+  if (precision == PREC_F32) {
+    PANN_CUDA(idx->emu.ensure(z.e2_bytes));
+    b.ge2 = idx->emu.as<uint32_t>();
   }
-  if (precision != PREC_F32) return PANN_OK;
-  // ---- tier E: exact emulation of the reference's hashset for flagged queries,
-  // first with the emulated table in shared memory (capacities 4 S0 / 2 S0),
-  // then, for queries that outgrow it, in global memory (16 S0 / 8 S0)
-  {
-    double cap_n = 2.0 * (10.0 + (double)plan.L) * (double)plan.dl;
-    uint32_t bits0 = (uint32_t)std::ceil(std::log2(cap_n));
-    uint64_t S0 = 1ull << bits0;
-    uint32_t vs = pow2_at_least(8ull * plan.L + 64);
-    uint32_t base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, true);
-    SearchArgs t = a;
-    t.redo_list = nullptr;
-    t.redo_count = nullptr;
-    t.emu_list = nullptr;
-    t.emu_count = nullptr;
-    EmuArgs e{};
-    e.bits0 = bits0;
-    e.vs_slots = vs;
-    e.base_bytes = base;
-    size_t smem_need = emu_smem_bytes(base, vs, (uint32_t)(4 * S0), (uint32_t)(2 * S0), true);
-    const uint32_t* glist = emu;
-    uint32_t* gcount = cnt + 6;
-    const uint32_t* grec = emu_rec;
-    if (smem_need <= smem_cap && 4 * S0 < (1ull << 31)) {
-      e.capA = (uint32_t)(4 * S0);
-      e.capB = (uint32_t)(2 * S0);
-      e.overflow_list = ovf;
-      e.overflow_rec = ovf_rec;
-      e.overflow_count = cnt + 8;
-      e.job_rec = emu_rec;
-      t.job_list = emu;
-      t.njobs_dev = cnt + 6;
-      t.job_counter = cnt + 5;
-      PANN_CUDA(launch_emulate(idx->dtype, idx->metric, true, t, e, 2 * idx->sm_count, smem_need, st));
-      glist = ovf;
-      grec = ovf_rec;
-      gcount = cnt + 8;
-    }
-    uint64_t capA = 16 * S0, capB = 8 * S0;
-    size_t per_slot = 4ull * (capA + capB);
-    int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>(idx->sm_count, (1ull << 30) / per_slot));
-    PANN_CUDA(idx->emu.ensure(per_slot * slots));
-    e.gA = idx->emu.as<uint32_t>();
-    e.gB = e.gA + (size_t)slots * capA;
-    e.capA = (uint32_t)capA;
-    e.capB = (uint32_t)capB;
-    e.overflow_list = nullptr;
-    e.overflow_rec = nullptr;
-    e.overflow_count = nullptr;
-    e.job_rec = grec;
-    t.job_list = glist;
-    t.njobs_dev = gcount;
-    t.job_counter = cnt + 7;
-    PANN_CUDA(launch_emulate(idx->dtype, idx->metric, false, t, e, slots,
-                             emu_smem_bytes(base, vs, 0, 0, false), st));
-  }
-  return PANN_OK;
+  SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
+                           d_vis_keys, vis_cap);
+  return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank);
 }
 
 static int check_index(const pann_index* idx, bool need_graph) {

@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
     if (PREC != PREC_F32) {
       // re-rank the best min(rerank, fn) entries by exact float32 distance
       // (beam_search_rerank's full-precision pass, beamSearch.h:569-587)
-      const uint32_t rr = a.qk ? 4 * kq : a.rerank;
+      const uint32_t rr = a.rerank ? a.rerank : 4 * kq;  // 0: 4k of this query
       const int nr = (int)min((uint32_t)fn, rr > kq ? rr : kq);
       for (int b = 0; b < nr; b += 64) {
         const int i0 = b + lane, i1 = b + 32 + lane;
