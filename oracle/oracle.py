@@ -58,6 +58,9 @@ def olib():
         L.oracle_permutation.argtypes = [_U32, _U64, _P]
         L.oracle_batch_schedule.restype = _U32
         L.oracle_batch_schedule.argtypes = [_U64, _U64, _D, _D, _P, _P, _U32]
+        L.oracle_range_search.restype = _I
+        L.oracle_range_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _I, _D, _D, _U32,
+                                          _P, _P, _U64, _P, _P, _P]
         L.oracle_distance.restype = ctypes.c_float
         L.oracle_distance.argtypes = [_I, _I, ctypes.c_uint, _P, _P]
         _olib = L
@@ -81,6 +84,9 @@ def rlib():
         L.ref_robust_prune.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _U32, _P, _P, _D, _I, _P, _P, _P]
         L.ref_build.restype = _I
         L.ref_build.argtypes = [_I, _I, _U32, _U32, _P, _U32, _U32, _D, _I, _D, _P, _P, _P, _P]
+        L.ref_range_search.restype = _I
+        L.ref_range_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _I, _D, _D, _U32, _P,
+                                       _P, _U64, _P, _P]
         L.ref_num_workers.restype = _I
         L.ref_num_workers.argtypes = []
         _rlib = L
@@ -127,6 +133,41 @@ def search(impl: str, base, queries, graph, k, L, limit=None, degree_limit=None,
                                batch_factor, len(st), _p(st), _p(ids), _p(dists), _p(vis), _p(cmps), _p(fn), _p(fi),
                                _p(fd), vcap, _p(vi), _p(vd))
     out["rc"] = rc
+    return out
+
+
+RANGE_GREEDY, RANGE_DOUBLING, RANGE_BEAM = 1, 2, 3  # rangeQueryType (types.h:153)
+
+
+def range_search(impl, base, queries, graph, beam, radius, rtype=RANGE_GREEDY, start=0, esr=0.0, esc=0, metric=0,
+                 cap=None):
+    """Range search per query ('oracle': pann_oracle.c; 'ref': RangeSearch / DoubleBeamRangeSearch compiled in
+    place). Returns dict(ids=[uint32 arrays], visited, cmps[, hash_grew])."""
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    nq = queries.shape[0]
+    cap = cap or n
+    cnt = np.zeros(nq, np.uint64)
+    ids = np.zeros((nq, cap), np.uint32)
+    vis = np.zeros(nq, np.uint32)
+    cmps = np.zeros(nq, np.uint64)
+    dt = _DT[base.dtype]
+    out = {}
+    if impl == "oracle":
+        grew = np.zeros(nq, np.int32)
+        rc = olib().oracle_range_search(dt, metric, n, d, _p(base), nq, _p(queries), R, _p(graph), beam, start, rtype,
+                                        radius, esr, esc, _p(cnt), _p(ids), cap, _p(vis), _p(cmps), _p(grew))
+        out["hash_grew"] = grew
+    else:
+        rc = rlib().ref_range_search(dt, metric, n, d, _p(base), nq, _p(queries), R, _p(graph), beam, start, rtype,
+                                     radius, esr, esc, _p(cnt), _p(ids), cap, _p(vis), _p(cmps))
+    assert rc == 0, rc
+    assert (cnt <= cap).all(), "raise cap"
+    out.update(ids=[ids[i, : int(cnt[i])].copy() for i in range(nq)], visited=vis,
+               cmps=(cmps & 0xFFFFFFFF).astype(np.uint32))
     return out
 
 

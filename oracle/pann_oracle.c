@@ -164,6 +164,10 @@ typedef struct {
   uint32_t k, L, degree_limit;
   uint64_t limit;
   double batch_factor;
+  /* early stopping (earlyStopping.h:19-29); es_count == 0 disables it */
+  double es_count;  /* QP.early_stopping_count */
+  double es_radius; /* QP.radius as the early-stopping rule sees it */
+  double es_esr;    /* QP.early_stopping_radius */
 } qparams_t;
 
 typedef struct {
@@ -173,8 +177,9 @@ typedef struct {
   int hash_grew;                         /* seen-set growth events */
 } bs_out_t;
 
-/* filtered_beam_search with use_filtering = false and no early stopping
- * (beamSearch.h:33-228). self != EMPTY32 marks the build-time query point:
+/* filtered_beam_search with use_filtering = false (beamSearch.h:33-228), with
+ * the early_stopping functor of range search when QP->es_count > 0
+ * (earlyStopping.h:19-29, called at beamSearch.h:120-121). self != EMPTY32 marks the build-time query point:
  * Points[a].same_as(p) is pointer equality, i.e. a == self (euclidian_point.h:184-186).
  * Returns 0, or -1 on invalid start points (beamSearch.h:51-57). */
 static int beam_search_one(const pts_t* P, const uint32_t* G, uint32_t R, const void* q,
@@ -212,6 +217,11 @@ static int beam_search_one(const pts_t* P, const uint32_t* G, uint32_t R, const 
 
   while (remain > offset && (uint64_t)num_visited < QP->limit) { /* :116 */
     pair_t current = unvisited[offset];
+    /* early_stopping(frontier, unvisited_frontier, visited, QP): it reads
+     * unvisited_frontier[0], which is only refreshed at a merge */
+    if (QP->es_count > 0 && (double)vn >= QP->es_count && !((double)frontier[0].d <= QP->es_radius) &&
+        !((double)unvisited[0].d <= QP->es_esr))
+      break;
     /* insert into the sorted visited list (:125-127) */
     if (vn == vcap) { vcap *= 2; visited = (pair_t*)realloc(visited, sizeof(pair_t) * vcap); }
     size_t pos = vn;
@@ -344,6 +354,106 @@ int oracle_search(int dtype, int metric, uint32_t n, uint32_t d, const void* bas
     free(o.visited);
   }
   return rc;
+}
+
+/* ------------------------------------------------------------ range search */
+/* greedy_search (rangeSearch.h:21-55): a breadth-first expansion over points
+ * within `radius`, seeded with the beam's in-range frontier, with the
+ * reference's growing hashset of initial capacity 2 * |seeds| * 64. Appends
+ * to *res (grown with realloc); returns the distance comparisons. */
+static uint64_t greedy_one(const pts_t* P, const uint32_t* G, uint32_t R, const void* q, const pair_t* seeds,
+                           uint32_t m, double radius, uint32_t** res, size_t* rn, size_t* rcap, int* grew) {
+  hset_t seen;
+  hs_init(&seen, 2 * (long)m * 64);
+#define PUSH(v) do { if (*rn == *rcap) { *rcap = *rcap * 2 + 16; *res = (uint32_t*)realloc(*res, 4 * *rcap); } \
+                     (*res)[(*rn)++] = (v); } while (0)
+  for (uint32_t i = 0; i < m; i++) { /* :30-33 */
+    if (hs_test_insert(&seen, seeds[i].id) || (double)seeds[i].d > radius) continue;
+    PUSH(seeds[i].id);
+  }
+  uint64_t cmps = 0;
+  uint32_t* unseen = (uint32_t*)malloc(4 * (R + 1));
+  size_t position = 0;
+  while (position < *rn) { /* :38-52 */
+    uint32_t next = (*res)[position++];
+    const uint32_t* gr = G + (size_t)next * (R + 1);
+    uint32_t deg = gr[0], un = 0;
+    for (uint32_t i = 0; i < deg; i++) {
+      uint32_t v = gr[1 + i];
+      if (hs_test_insert(&seen, v)) continue;
+      unseen[un++] = v;
+    }
+    for (uint32_t i = 0; i < un; i++) {
+      cmps++;
+      if ((double)dist(P, row(P, unseen[i]), q) <= radius) PUSH(unseen[i]);
+    }
+  }
+#undef PUSH
+  free(unseen);
+  *grew += seen.grew;
+  hs_free(&seen);
+  return cmps;
+}
+
+/* Range search per query from one start point:
+ *   type 1 (Greedy) / 3 (Beam): RangeSearch (rangeSearch.h:183-276) without
+ *     quantization: a beam search of width `beam` (k = beam, limit = n,
+ *     degree_limit = R, batch_factor .125) with early stopping, where the
+ *     early-stopping radii pass through Point::translate_distance (a float
+ *     rounding for unquantized points, euclidian_point.h:119-123,
+ *     mips_point.h:90-92); the frontier entries with distance <= radius are
+ *     the answer unless all `beam` of them are in range and the type is Greedy,
+ *     in which case greedy_search from them (radius rounded the same way)
+ *     gives the answer, in its discovery order.
+ *   type 2 (Doubling): DoubleBeamRangeSearch (doublingSearch.h:50-148). Its
+ *     first round is the same beam search with the radius not rounded. When
+ *     every frontier entry is in range it runs beam_search again from them
+ *     with QueryParams(2 beam, 2 beam, 0.0, G.size(), G.max_degree()), whose
+ *     third argument is the visit limit: with limit 0 that search visits
+ *     nothing and returns the start points sorted, so the answer stays the
+ *     in-range frontier, visited gains 0 and comparisons gain `beam`.
+ * visited / cmps accumulate as QueryStats does (rangeSearch.h:258-267,
+ * doublingSearch.h:88-89,138-139). Per query, out_count gets the answer's
+ * size and out_ids (rows of `cap`) its first cap ids. */
+int oracle_range_search(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+                        const void* queries, uint32_t R, const uint32_t* graph, uint32_t beam, uint32_t start,
+                        int type, double radius, double esr, uint32_t esc, uint64_t* out_count, uint32_t* out_ids,
+                        uint64_t cap, uint32_t* out_visited, uint64_t* out_cmps, int32_t* out_grew) {
+  if (beam == 0 || type < 1 || type > 3) return -1;
+  pts_t P = {dtype, metric, d, d * elem_size(dtype), (const uint8_t*)base};
+  pts_t Q = {dtype, metric, d, d * elem_size(dtype), (const uint8_t*)queries};
+  const double r_f = (double)(float)radius, esr_f = (double)(float)esr;
+  qparams_t QP = {beam, beam, R, (uint64_t)n, 0.125, (double)esc, type == 2 ? radius : r_f, esr_f};
+  size_t rcap = 0;
+  uint32_t* res = NULL;
+  for (uint32_t i = 0; i < nq; i++) {
+    const void* q = row(&Q, i);
+    bs_out_t o;
+    if (beam_search_one(&P, graph, R, q, EMPTY32, &start, 1, &QP, &o) != 0) { free(res); return -1; }
+    uint64_t visited = o.visited_n, cmps = o.cmps;
+    int grew = o.hash_grew;
+    uint32_t c = 0;
+    while (c < o.frontier_n && (double)o.frontier[c].d <= radius) c++; /* the sorted frontier's in-range prefix */
+    size_t rn = 0;
+    if (c < beam || type == 3) {
+      for (uint32_t j = 0; j < c; j++) { if (rn == rcap) { rcap = rcap * 2 + 16; res = (uint32_t*)realloc(res, 4 * rcap); } res[rn++] = o.frontier[j].id; }
+    } else if (type == 2) {
+      for (uint32_t j = 0; j < c; j++) { if (rn == rcap) { rcap = rcap * 2 + 16; res = (uint32_t*)realloc(res, 4 * rcap); } res[rn++] = o.frontier[j].id; }
+      cmps += c; /* the limit-0 second round: start points only */
+    } else {
+      cmps += greedy_one(&P, graph, R, q, o.frontier, c, r_f, &res, &rn, &rcap, &grew);
+      visited += rn;
+    }
+    out_count[i] = rn;
+    for (size_t j = 0; j < rn && j < cap; j++) out_ids[(size_t)i * cap + j] = res[j];
+    if (out_visited) out_visited[i] = (uint32_t)visited;
+    if (out_cmps) out_cmps[i] = cmps;
+    if (out_grew) out_grew[i] = grew;
+    free(o.frontier);
+    free(o.visited);
+  }
+  free(res);
+  return 0;
 }
 
 /* ------------------------------------------------------------ robustPrune */

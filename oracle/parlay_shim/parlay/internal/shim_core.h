@@ -498,6 +498,7 @@ struct timer {
   double next_time() { auto t = clk::now(); double d = secs(t - last); last = t; total_ += d; return d; }
   void next(const std::string& s) { double d = next_time(); std::cout << name << ": " << s << ": " << d << std::endl; }
   void total() { std::cout << name << ": " << get_total() << std::endl; }
+  double total_time() { return get_total(); }
 };
 }  // namespace internal
 

@@ -13,6 +13,8 @@
 //   ref_qsearch_time qsearchAll() timed as checkRecall (check_nn_recall.h:46-59)
 //   ref_robust_prune knn_index::robustPrune()          (index.h:63-120)
 //   ref_build        knn_index::build_index()          (index.h:150-186)
+//   ref_range_search RangeSearch() / DoubleBeamRangeSearch()
+//                                        (rangeSearch.h:183-276, doublingSearch.h:50-157)
 //   ref_num_workers  threads used by parallel_for
 #include <cstdint>
 #include <cstring>
@@ -25,6 +27,8 @@
 #include "utils/beamSearch.h"
 #include "utils/stats.h"
 #include "vamana/index.h"
+#include "utils/rangeSearch.h"
+#include "utils/doublingSearch.h"
 
 using namespace parlayANN;
 
@@ -182,6 +186,40 @@ int build_t(uint32_t n, uint32_t d, const void* base, uint32_t R, uint32_t L, do
   return 0;
 }
 
+template <typename Point>
+int range_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries, uint32_t R,
+            const uint32_t* graph, uint32_t beam, uint32_t start, int type, double radius, double esr,
+            uint32_t esc, uint64_t* out_count, uint32_t* out_ids, uint64_t cap, uint32_t* out_visited,
+            uint64_t* out_cmps) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto G = make_graph(graph, n, R);
+  // as range_search_wrapper builds it (check_range_recall.h:132-133)
+  QueryParams QP((long)beam, (long)beam, (long)G.size(), (long)G.max_degree(), (long)(esc > 0), esr, (long)esc,
+                 (rangeQueryType)type, radius);
+  stats<unsigned int> QS(nq);
+  QS.clear();
+  auto emit = [&](size_t i, const auto& v) {
+    out_count[i] = v.size();
+    for (size_t j = 0; j < v.size() && j < cap; j++) out_ids[i * cap + j] = v[j];
+  };
+  if (type == Doubling) {
+    parlay::sequence<unsigned int> sp = {start};
+    auto active = parlay::tabulate(nq, [](size_t i) { return (unsigned int)i; });
+    auto res = DoubleBeamRangeSearch(G, Q, B, Q, B, QS, sp, QP, active);
+    for (size_t i = 0; i < nq; i++) emit(i, res.first[i]);
+  } else {
+    auto res = RangeSearch<Point, PR, PR, unsigned int>(G, Q, B, Q, B, QS, start, QP);
+    for (size_t i = 0; i < nq; i++) emit(i, res.first[i]);
+  }
+  for (size_t i = 0; i < nq; i++) {
+    if (out_visited) out_visited[i] = QS.visited[i];
+    if (out_cmps) out_cmps[i] = QS.distances[i];
+  }
+  return 0;
+}
+
 }  // namespace
 
 #define DISPATCH(dtype, metric, FN, ...)                                                  \
@@ -238,6 +276,15 @@ int ref_build(int dtype, int metric, uint32_t n, uint32_t d, const void* base, u
               double* seconds, uint64_t* out_dist_total, uint32_t* out_visited) {
   DISPATCH(dtype, metric, build_t, n, d, base, R, L, alpha, passes, batch_factor, out_graph,
            seconds, out_dist_total, out_visited);
+  return -1;
+}
+
+int ref_range_search(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+                     const void* queries, uint32_t R, const uint32_t* graph, uint32_t beam, uint32_t start,
+                     int type, double radius, double esr, uint32_t esc, uint64_t* out_count, uint32_t* out_ids,
+                     uint64_t cap, uint32_t* out_visited, uint64_t* out_cmps) {
+  DISPATCH(dtype, metric, range_t, n, d, base, nq, queries, R, graph, beam, start, type, radius, esr, esc,
+           out_count, out_ids, cap, out_visited, out_cmps);
   return -1;
 }
 

@@ -69,6 +69,31 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"build_{nm}.npz"), base=base, R=10, L=20, alpha=1.2, passes=2,
                             metric=metric, graph=gr, dist_total=tot, perm=O.permutation(800))
         cases.append(f"build_{nm}")
+    # range search (RangeSearch / DoubleBeamRangeSearch): greedy expansions
+    # large enough for the seen-set to grow, early stopping, all three types
+    for ci, (dtype, metric, quant) in enumerate([(np.uint8, 0, 0.2), (np.float32, 0, 0.3), (np.float32, 1, 0.1)]):
+        base = pts(dtype, 3000, 8, 500 + ci)
+        q = pts(dtype, 16, 8, 600 + ci)
+        g = O.random_graph(3000, 24, 700 + ci)
+        rng = np.random.default_rng(800 + ci)
+        for i in range(0, 3000, 5):                     # repeated ids inside some rows
+            deg = g[i, 0]
+            g[i, 1 + rng.integers(0, deg, 3)] = g[i, 1 + rng.integers(0, deg, 3)]
+        samp = [O.olib().oracle_distance(O._DT[base.dtype], metric, 8, q[i].ctypes.data, base[j].ctypes.data)
+                for i in range(4) for j in range(0, 3000, 7)]
+        radius = float(np.quantile(samp, quant))
+        runs = [(1, 10, 0, 0.0), (1, 24, 10, 2 * radius), (2, 12, 0, 0.0), (3, 16, 6, radius)]
+        out = dict(base=base, queries=q, graph=g, radius=radius, metric=metric,
+                   runs=np.array([(t, b, c, e) for t, b, c, e in runs], np.float64))
+        for j, (rtype, beam, esc, esr) in enumerate(runs):
+            r = O.range_search("ref", base, q, g, beam, radius, rtype, esr=esr, esc=esc, metric=metric)
+            out[f"counts{j}"] = np.array([len(x) for x in r["ids"]], np.int64)
+            out[f"ids{j}"] = np.concatenate(r["ids"]).astype(np.uint32)
+            out[f"visited{j}"] = r["visited"]
+            out[f"cmps{j}"] = r["cmps"]
+        name = f"range_{np.dtype(dtype).name}_{'l2' if metric == 0 else 'mips'}"
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        cases.append(name)
     print("\n".join(cases))
 
 

@@ -132,3 +132,49 @@ def test_oracle_prune_matches_reference(lib_built):
                 b = O.robust_prune("ref", base, g, p, cand, cd, alpha, add)
                 np.testing.assert_array_equal(a[0], b[0])
                 assert a[1] == b[1]
+
+
+def sample_radius(base, q, metric, quant):
+    d = q.shape[1]
+    dt = O._DT[base.dtype]
+    samp = [O.olib().oracle_distance(dt, metric, d, np.ascontiguousarray(q[i]).ctypes.data,
+                                     np.ascontiguousarray(base[j]).ctypes.data)
+            for i in range(min(4, len(q))) for j in range(0, len(base), 7)]
+    return float(np.quantile(samp, quant))
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "range_*.npz"))), ids=os.path.basename)
+def test_oracle_range_search_matches_golden(path, lib_built):
+    """RangeSearch / DoubleBeamRangeSearch (rangeSearch.h:183-276,
+    doublingSearch.h:50-157): answers in the reference's order (duplicates the
+    reference's growing hashset lets through included), visited and
+    comparison counts."""
+    z = np.load(path)
+    for j, (rtype, beam, esc, esr) in enumerate(z["runs"]):
+        r = O.range_search("oracle", z["base"], z["queries"], z["graph"], int(beam), float(z["radius"]), int(rtype),
+                           esr=float(esr), esc=int(esc), metric=int(z["metric"]))
+        np.testing.assert_array_equal([len(x) for x in r["ids"]], z[f"counts{j}"], err_msg=f"counts run {j}")
+        np.testing.assert_array_equal(np.concatenate(r["ids"]), z[f"ids{j}"], err_msg=f"ids run {j}")
+        np.testing.assert_array_equal(r["visited"], z[f"visited{j}"], err_msg=f"visited run {j}")
+        np.testing.assert_array_equal(r["cmps"], z[f"cmps{j}"], err_msg=f"cmps run {j}")
+
+
+@needs_ref
+@pytest.mark.parametrize("dtype,metric", [(np.uint8, 0), (np.int8, 1), (np.float32, 0), (np.float32, 1)])
+def test_oracle_range_search_matches_reference(dtype, metric, lib_built):
+    base = random_points(dtype, 5000, 8, 61)
+    q = random_points(dtype, 24, 8, 62)
+    g = O.random_graph(5000, 20, 63)
+    grew = 0
+    for quant in (0.01, 0.15):
+        radius = sample_radius(base, q, metric, quant)
+        for rtype in (O.RANGE_GREEDY, O.RANGE_DOUBLING, O.RANGE_BEAM):
+            for beam, esc, esr in [(10, 0, 0.0), (20, 10, 1.5 * radius)]:
+                a = O.range_search("oracle", base, q, g, beam, radius, rtype, esr=esr, esc=esc, metric=metric)
+                b = O.range_search("ref", base, q, g, beam, radius, rtype, esr=esr, esc=esc, metric=metric)
+                for x, y in zip(a["ids"], b["ids"]):
+                    np.testing.assert_array_equal(x, y)
+                np.testing.assert_array_equal(a["visited"], b["visited"])
+                np.testing.assert_array_equal(a["cmps"], b["cmps"])
+                grew += int(a["hash_grew"].sum())
+    assert grew > 0   # the greedy expansion's seen-set grew somewhere
