@@ -198,6 +198,39 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
                    float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags, int on_device,
                    void* stream);
 
+/* ---------------------------------------------------------------- range search */
+
+/* rangeQueryType (types.h:153) */
+#define PANN_RANGE_GREEDY 1
+#define PANN_RANGE_DOUBLING 2
+#define PANN_RANGE_BEAM 3
+
+typedef struct {
+  uint32_t beam;                  /* QP.beamSize: the beam search's width (and k) */
+  int32_t type;                   /* PANN_RANGE_* */
+  double radius;                  /* in Point::distance units: squared L2, or the negated inner product */
+  double early_stopping_radius;   /* QP.early_stopping_radius */
+  uint32_t early_stopping_count;  /* QP.early_stopping_count; 0 disables early stopping (earlyStopping.h:24-25) */
+} pann_range_params;
+
+/* Range search from one start point, as RangeSearch (type GREEDY or BEAM,
+ * rangeSearch.h:183-276) and DoubleBeamRangeSearch (type DOUBLING,
+ * doublingSearch.h:50-157) compute it on unquantized points: a beam search of
+ * width `beam` with early stopping (earlyStopping.h:19-29); its frontier
+ * entries within `radius` are the answer, unless all `beam` are within it and
+ * the type is GREEDY, in which case greedy_search (rangeSearch.h:21-55)
+ * expands from them and its discovery order is the answer (duplicates that
+ * the reference's hashset lets through included). Host buffers: answer i is
+ * out_ids[out_offsets[i] .. out_offsets[i+1]) (out_offsets has nq + 1
+ * entries). If the answers need more than ids_cap ids, out_offsets is filled,
+ * out_ids is not, and PANN_EOVERFLOW is returned: call again with room for
+ * out_offsets[nq]. out_visited / out_cmps (may be NULL) get the QueryStats
+ * counts; out_flags (may be NULL): bit 0 = the beam's hashset grew, bit 1 =
+ * the expansion's hashset grew (both reproduced exactly). */
+int pann_range_search(pann_index* idx, const void* queries, uint32_t nq, const pann_range_params* rp,
+                      uint32_t start_point, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
+                      uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags);
+
 /* ---------------------------------------------------------------- batched form */
 
 /* A batch object: a reusable launch sequence for many queries whose k and beam

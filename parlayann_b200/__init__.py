@@ -62,6 +62,16 @@ class BatchOptions(ctypes.Structure):
                 ("warps_per_block", ctypes.c_uint32)]
 
 
+class RangeParams(ctypes.Structure):
+    """pann_range_params: RangeSearch / DoubleBeamRangeSearch parameters (types.h:254-259)."""
+
+    _fields_ = [("beam", ctypes.c_uint32), ("type", ctypes.c_int32), ("radius", ctypes.c_double),
+                ("early_stopping_radius", ctypes.c_double), ("early_stopping_count", ctypes.c_uint32)]
+
+
+RANGE_GREEDY, RANGE_DOUBLING, RANGE_BEAM = 1, 2, 3
+
+
 class BuildParams(ctypes.Structure):
     """BuildParams fields of the Vamana build (types.h:155-230)."""
 
@@ -108,6 +118,7 @@ SIGNATURES = {
     "pann_index_set_precision": (_I, [_P, _I]),
     "pann_search_ex": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.POINTER(SearchOptions), _P, _U32, _P,
                             _P, _P, _P, _P, _I, _P]),
+    "pann_range_search": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, _P, _P, _U64, _P, _P, _P]),
     "pann_batch_create": (_I, [ctypes.POINTER(_P), _P, _U32, ctypes.POINTER(QueryParams), _P, _U32,
                                ctypes.POINTER(SearchOptions), ctypes.POINTER(BatchOptions)]),
     "pann_batch_run": (_I, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
@@ -288,6 +299,30 @@ class Index:
         """A reusable batch for queries with per-query k and beam (pann_batch_create)."""
         return Batch(self, max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts, precision, rerank,
                      use_graph, autotune, seen_slots, warps_per_block)
+
+    def range_search(self, queries: np.ndarray, beam: int, radius: float, rtype: int = RANGE_GREEDY, start: int = 0,
+                     early_stopping_radius: float = 0.0, early_stopping_count: int = 0):
+        """Range search (pann_range_search). Returns dict(ids=[uint32 array per query], offsets, visited, cmps,
+        flags); ids are in the reference's answer order."""
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        nq = queries.shape[0]
+        rp = RangeParams(beam, rtype, radius, early_stopping_radius, early_stopping_count)
+        offs = np.zeros(nq + 1, np.uint64)
+        vis = np.zeros(nq, np.uint32)
+        cmps = np.zeros(nq, np.uint32)
+        flags = np.zeros(nq, np.uint32)
+        cap = max(1, nq * beam * 4)
+        for _ in range(2):
+            ids = np.zeros(cap, np.uint32)
+            rc = lib().pann_range_search(self._h, _ptr(queries), nq, ctypes.byref(rp), start, _ptr(offs), _ptr(ids),
+                                         cap, _ptr(vis), _ptr(cmps), _ptr(flags))
+            if rc == PANN_EOVERFLOW and int(offs[nq]) > cap:
+                cap = int(offs[nq])
+                continue
+            _check(rc)
+            break
+        lists = [ids[int(offs[i]):int(offs[i + 1])].copy() for i in range(nq)]
+        return dict(ids=lists, offsets=offs, visited=vis, cmps=cmps, flags=flags)
 
     def search_lists(self, queries: np.ndarray, L: int, limit: int | None = None, degree_limit: int | None = None,
                      batch_factor: float = 0.125, starts=(0,), visited_cap: int | None = None):

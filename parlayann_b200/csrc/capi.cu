@@ -466,13 +466,23 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   TierSizes z;
   int rc = size_tiers(idx, plan, nq, precision, 0, 0, &z);
   if (rc) return rc;
+  TierBufs b{};
+  rc = index_tier_buffers(idx, z, nq, precision, &b);
+  if (rc) return rc;
+  SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
+                           d_vis_keys, vis_cap);
+  return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank);
+}
+
+int index_tier_buffers(pann_index* idx, const TierSizes& z, uint32_t nq, int precision, TierBufs* out) {
   // counters: [0..2] job counters per tier, [3] redo count 0, [4] redo count 1,
   // [5] shared-memory emulation job counter, [6] emulation list length,
   // [7] global emulation job counter, [8] emulation overflow count,
   // [9] resume records taken
   PANN_CUDA(idx->counters.ensure(64));
-  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)nq));
-  TierBufs b{};
+  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)std::max<uint32_t>(nq, 1)));
+  TierBufs& b = *out;
+  b = TierBufs{};
   b.cnt = idx->counters.as<uint32_t>();
   b.redo0 = idx->redo.as<uint32_t>();
   b.redo1 = b.redo0 + nq;
@@ -494,9 +504,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     PANN_CUDA(idx->emu.ensure(z.e2_bytes));
     b.ge2 = idx->emu.as<uint32_t>();
   }
-  SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
-                           d_vis_keys, vis_cap);
-  return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank);
+  return PANN_OK;
 }
 
 static int check_index(const pann_index* idx, bool need_graph) {
@@ -506,7 +514,7 @@ static int check_index(const pann_index* idx, bool need_graph) {
   return PANN_OK;
 }
 
-static int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st) {
+int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st) {
   if (!starts) return fail(PANN_EINVAL, "start points are NULL");
   for (uint32_t i = 0; i < n_start; i++) {
     if ((uint64_t)starts[i] >= idx->n) return fail(PANN_EINVAL, "start point id out of range");
@@ -596,7 +604,8 @@ int pann_index_destroy(pann_index* idx) {
   if (idx->d_graph) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
                     &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->handoff, &idx->starts,
-                    &idx->tmp, &idx->lp_rows, &idx->lp_scales})
+                    &idx->tmp, &idx->lp_rows, &idx->lp_scales, &idx->range_meta, &idx->range_tabs,
+                    &idx->range_pool, &idx->range_out})
     b->release();
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;

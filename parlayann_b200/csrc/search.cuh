@@ -94,6 +94,10 @@ struct SearchArgs {
   uint32_t lp_chunks;
   const float* lp_scales;
   uint32_t rerank;
+  // early stopping of range search (earlyStopping.h:19-29); es_count == 0 disables it
+  double es_count;   // QP.early_stopping_count
+  double es_radius;  // QP.radius as the rule sees it
+  double es_esr;     // QP.early_stopping_radius
 };
 
 // The reference's seen-set capacity for beam L and degree limit dl is
@@ -274,6 +278,10 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
     uint32_t status = 0;
     bool hand_over = false;
     const uint32_t nel = a.dl < a.R ? a.dl : a.R;
+    // the reference's early-stopping rule reads unvisited_frontier[0], which is
+    // refreshed only at a merge: its distance, taken at the first scan after one
+    float u0 = 0.0f;
+    bool u0_fresh = true;
 
     for (;;) {
       __syncwarp();
@@ -292,6 +300,13 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       }
       if (first >= 0) cnt += 1;
       if (first < 0 || nvis >= a.limit) break;  // :116
+      if (u0_fresh) {
+        u0 = key_dist(fr[first]);
+        u0_fresh = false;
+      }
+      if (a.es_count > 0.0 && (double)nvis >= a.es_count && !((double)key_dist(fr[0]) <= a.es_radius) &&
+          !((double)u0 <= a.es_esr))
+        break;  // early_stopping (earlyStopping.h:19-29), checked at beamSearch.h:120-121
       if (handoff && entries + nel > ref_half) {
         // this visit could cross the reference's growth threshold
         status |= QS_REF_WOULD_GROW;
@@ -385,6 +400,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       warp_rank_sort(cand, cand2, cn, lane);
       __syncwarp();
       fn = warp_merge(fr, fn, cand2, cn, fr2, (int)L, lane);
+      u0_fresh = true;
       uint64_t* t = fr; fr = fr2; fr2 = t;
       cn = 0;
       __syncwarp();
@@ -412,7 +428,7 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
           uint32_t* rec = a.rec_pool + (size_t)r * a.rec_words;
           if (lane == 0) {
             rec[0] = qi; rec[1] = (uint32_t)fn; rec[2] = (uint32_t)cn; rec[3] = (uint32_t)nvis;
-            rec[4] = cmps; rec[5] = entries;
+            rec[4] = cmps; rec[5] = entries; rec[6] = __float_as_uint(u0);
           }
           uint64_t* rfr = reinterpret_cast<uint64_t*>(rec + ly.fr);
           uint64_t* rcand = reinterpret_cast<uint64_t*>(rec + ly.cand);

@@ -54,14 +54,16 @@ struct EmuHash {
 };
 
 // Order-preserving parallel linear probing. Lanes in `act` each hold a key;
-// processing them in lane order one at a time ("find the key or the first
-// empty slot from pos, insert there") gives the same table and results as
-// running rounds in which every unfinished lane probes the current table, and
-// among lanes that reach the same empty slot the lowest lane inserts while the
-// others continue past it. (A later key never changes an earlier key's
-// outcome: an empty slot on an earlier key's path before its own stop would
-// have been that key's stop.) Returns, per lane, whether it inserted (*ins)
-// and the slot where it stopped (*pos).
+// the result equals processing them in lane order one at a time ("find the
+// key or the first empty slot from pos, insert there"). Rounds: every
+// unfinished lane scans the current table to its key or its first empty slot.
+// Lanes that stop at different empty slots do not interact, except through a
+// lane that lost a shared slot to a lower lane: in lane order it continues
+// past that slot and may take a slot that a higher lane found empty. So in a
+// round the lowest lane of each shared slot inserts only if it is below the
+// lowest losing lane; every other unfinished lane scans again in the next
+// round (the lowest unfinished lane always inserts, so rounds end). Returns,
+// per lane, whether it inserted (*ins) and the slot where it stopped (*pos).
 __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, uint32_t key, bool act, uint32_t start,
                                                  int lane, bool* ins, uint32_t* pos) {
   const unsigned FULL = 0xFFFFFFFFu;
@@ -77,7 +79,10 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
     unsigned want = __ballot_sync(FULL, !done);
     if (!want) break;
     unsigned grp = __match_any_sync(FULL, done ? (0x80000000u | (uint32_t)lane) : p);
-    const bool win = !done && (__ffs(grp & want) - 1) == lane;
+    const bool lowest = !done && (__ffs(grp & want) - 1) == lane;
+    const unsigned losers = want & ~__ballot_sync(FULL, lowest);
+    const unsigned below = losers ? ((1u << (__ffs(losers) - 1)) - 1u) : FULL;
+    const bool win = lowest && ((below >> lane) & 1u);
     if (win) {
       tab[p] = key;
       inserted = true;
@@ -288,6 +293,8 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
     int fn, cn;
     uint32_t cmps;
     uint64_t nvis;
+    float u0 = 0.0f;  // distance of unvisited_frontier[0] at the last merge (early stopping)
+    bool u0_fresh = true;
     if (rec_id != PANN_PAD) {
       // resume tier 0's query: its state before the visit that could cross the
       // growth threshold, and the reference's table rebuilt from the insertion
@@ -299,6 +306,8 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       nvis = rec[3];
       cmps = rec[4];
       const uint32_t entries = rec[5];
+      u0 = __uint_as_float(rec[6]);  // taken by tier 0 before it handed over
+      u0_fresh = false;
       const uint64_t* rfr = reinterpret_cast<const uint64_t*>(rec + ly.fr);
       const uint64_t* rcand = reinterpret_cast<const uint64_t*>(rec + ly.cand);
       for (int i = lane; i < fn; i += 32) fr[i] = rfr[i];
@@ -344,6 +353,13 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
         cnt += __popc(m);
       }
       if (first < 0 || nvis >= a.limit) break;
+      if (u0_fresh) {
+        u0 = key_dist(fr[first]);
+        u0_fresh = false;
+      }
+      if (a.es_count > 0.0 && (double)nvis >= a.es_count && !((double)key_dist(fr[0]) <= a.es_radius) &&
+          !((double)u0 <= a.es_esr))
+        break;  // early_stopping (earlyStopping.h:19-29)
       const uint64_t cur_key = fr[first];
       __syncwarp();
       if (lane == 0) fr[first] = cur_key | PANN_VFLAG;
@@ -419,6 +435,7 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       }
       __syncwarp();
       fn = warp_merge(fr, fn, cand, un, fr2, (int)L, lane);
+      u0_fresh = true;
       uint64_t* t = fr; fr = fr2; fr2 = t;
       cn = 0;
       __syncwarp();

@@ -57,6 +57,10 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
                int wpb_force, TierSizes* z);
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a, const TierSizes& z,
                   const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank);
+// Validates the start points and copies them to idx->starts (cached).
+int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st);
+// The index's own tier buffers for nq queries (grown as needed).
+int index_tier_buffers(pann_index* idx, const TierSizes& z, uint32_t nq, int precision, TierBufs* b);
 SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries,
                      const uint32_t* d_self_ids, uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids,
                      float* d_dists, uint32_t* d_vis, uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys,
