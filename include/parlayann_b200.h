@@ -279,6 +279,59 @@ int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps
 
 int pann_batch_destroy(pann_batch* b);
 
+/* ---------------------------------------------------------------- serving form */
+
+/* A request loop over one resident index (no counterpart in the reference,
+ * which searches closed batches: qsearchAll, beamSearch.h:599-646). Requests
+ * are submitted from any thread and answered asynchronously: a dispatcher
+ * thread keeps up to `inflight` batches on the GPU, each a pann_batch whose
+ * device scratch holds max_batch_queries queries (the admission unit), and
+ * fills every slot that frees up with the waiting k-NN requests in arrival
+ * order (continuous batching: requests that arrive while others run join the
+ * next slot, and batches overlap on the device). Range requests run on a
+ * second worker through pann_range_search. Each request's answer equals the
+ * same request run alone (pann_search / pann_range_search). While a server
+ * runs it is the only user of its index. */
+typedef struct pann_server pann_server;
+
+typedef struct {
+  uint32_t max_batch_queries; /* queries per in-flight batch (also the largest k-NN request) */
+  uint32_t inflight;          /* batches on the GPU at once, 1..16 */
+  uint32_t max_k, max_beam;   /* bounds of k-NN requests */
+  uint64_t limit;             /* QueryParams.limit of every k-NN request */
+  uint32_t degree_limit;
+  double batch_factor;
+  int32_t precision;          /* PANN_PREC_*; low precision needs pann_index_set_precision first */
+} pann_server_options;
+
+int pann_server_create(pann_server** out, pann_index* idx, const pann_server_options* opt, const uint32_t* starts,
+                       uint32_t n_start);
+/* Queries are copied at submission (host memory, nq rows). *ticket names the request. */
+int pann_server_submit_knn(pann_server* s, const void* queries, uint32_t nq, uint32_t k, uint32_t beam,
+                           uint64_t* ticket);
+int pann_server_submit_range(pann_server* s, const void* queries, uint32_t nq, const pann_range_params* rp,
+                             uint32_t start_point, uint64_t* ticket);
+/* Block until the request is answered, copy its results (k-NN: nq x k ids and
+ * distances; range: nq + 1 offsets and the ids, as pann_range_search) and
+ * release the ticket. Any output may be NULL. latency_s = submission to
+ * answer in host memory. */
+int pann_server_wait_knn(pann_server* s, uint64_t ticket, uint32_t* out_ids, float* out_dists, double* latency_s);
+int pann_server_wait_range(pann_server* s, uint64_t ticket, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
+                           double* latency_s);
+/* Requests and queries answered, seconds elapsed, median and 99th-percentile
+ * latency since the last reset (reset != 0 starts a new window). */
+int pann_server_stats(pann_server* s, int reset, uint64_t* requests, uint64_t* queries, double* seconds, double* p50_s,
+                      double* p99_s);
+/* Open-loop load generator: request i (k-NN if kind[i] == 0, else range with
+ * *rp from range_start) is submitted arrival_s[i] seconds after the call
+ * starts, with nq[i] queries from row q_row[i] of query_pool; waits for all.
+ * out_latency_s[i] gets each latency, *out_wall_s the time to the last answer. */
+int pann_server_replay(pann_server* s, uint32_t nreq, const double* arrival_s, const uint32_t* kind,
+                       const uint32_t* nq, const uint32_t* k, const uint32_t* beam, const uint64_t* q_row,
+                       const void* query_pool, const pann_range_params* rp, uint32_t range_start, double* out_latency_s,
+                       double* out_wall_s);
+int pann_server_destroy(pann_server* s);
+
 /* ---------------------------------------------------------------- build */
 
 /* Vamana batch-insertion build into the index's graph (knn_index::build_index,

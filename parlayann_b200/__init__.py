@@ -72,6 +72,14 @@ class RangeParams(ctypes.Structure):
 RANGE_GREEDY, RANGE_DOUBLING, RANGE_BEAM = 1, 2, 3
 
 
+class ServerOptions(ctypes.Structure):
+    """pann_server_options: slots, admission unit and the bounds of k-NN requests."""
+
+    _fields_ = [("max_batch_queries", ctypes.c_uint32), ("inflight", ctypes.c_uint32), ("max_k", ctypes.c_uint32),
+                ("max_beam", ctypes.c_uint32), ("limit", ctypes.c_uint64), ("degree_limit", ctypes.c_uint32),
+                ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32)]
+
+
 class BuildParams(ctypes.Structure):
     """BuildParams fields of the Vamana build (types.h:155-230)."""
 
@@ -119,6 +127,16 @@ SIGNATURES = {
     "pann_search_ex": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.POINTER(SearchOptions), _P, _U32, _P,
                             _P, _P, _P, _P, _I, _P]),
     "pann_range_search": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, _P, _P, _U64, _P, _P, _P]),
+    "pann_server_create": (_I, [ctypes.POINTER(_P), _P, ctypes.POINTER(ServerOptions), _P, _U32]),
+    "pann_server_submit_knn": (_I, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U64)]),
+    "pann_server_submit_range": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, ctypes.POINTER(_U64)]),
+    "pann_server_wait_knn": (_I, [_P, _U64, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "pann_server_wait_range": (_I, [_P, _U64, _P, _P, _U64, ctypes.POINTER(ctypes.c_double)]),
+    "pann_server_stats": (_I, [_P, _I, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "pann_server_replay": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(RangeParams), _U32, _P,
+                                ctypes.POINTER(ctypes.c_double)]),
+    "pann_server_destroy": (_I, [_P]),
     "pann_batch_create": (_I, [ctypes.POINTER(_P), _P, _U32, ctypes.POINTER(QueryParams), _P, _U32,
                                ctypes.POINTER(SearchOptions), ctypes.POINTER(BatchOptions)]),
     "pann_batch_run": (_I, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
@@ -399,6 +417,94 @@ class Batch:
     def close(self):
         if self._h:
             lib().pann_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving form (pann_server_*): continuous batching of k-NN requests over
+    `inflight` batch slots, range requests on a second worker. While it runs it
+    is the only user of its index."""
+
+    def __init__(self, index: "Index", max_batch_queries: int = 1024, inflight: int = 3, max_k: int = 100,
+                 max_beam: int = 400, limit: int | None = None, degree_limit: int | None = None,
+                 batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,)):
+        self.index = index
+        o = ServerOptions(max_batch_queries, inflight, max_k, max_beam, index.n if limit is None else limit,
+                          index.R if degree_limit is None else degree_limit, batch_factor, precision)
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+        h = ctypes.c_void_p()
+        _check(lib().pann_server_create(ctypes.byref(h), index.handle, ctypes.byref(o), _ptr(st), len(st)))
+        self._h = h
+        self._kinds = {}
+
+    def _q(self, queries):
+        return np.ascontiguousarray(queries, dtype=_NP_OF[self.index.dtype])
+
+    def submit_knn(self, queries, k: int, beam: int) -> int:
+        q = self._q(queries)
+        t = ctypes.c_uint64()
+        _check(lib().pann_server_submit_knn(self._h, _ptr(q), q.shape[0], k, beam, ctypes.byref(t)))
+        self._kinds[t.value] = ("knn", q.shape[0], k)
+        return t.value
+
+    def submit_range(self, queries, beam: int, radius: float, rtype: int = RANGE_GREEDY, start: int = 0,
+                     early_stopping_radius: float = 0.0, early_stopping_count: int = 0) -> int:
+        q = self._q(queries)
+        rp = RangeParams(beam, rtype, radius, early_stopping_radius, early_stopping_count)
+        t = ctypes.c_uint64()
+        _check(lib().pann_server_submit_range(self._h, _ptr(q), q.shape[0], ctypes.byref(rp), start, ctypes.byref(t)))
+        self._kinds[t.value] = ("range", q.shape[0], 0)
+        return t.value
+
+    def wait(self, ticket: int):
+        """k-NN: (ids, dists, latency_s); range: (list of id arrays, latency_s)."""
+        kind, nq, k = self._kinds.pop(ticket)
+        lat = ctypes.c_double()
+        if kind == "knn":
+            ids = np.empty((nq, k), np.uint32)
+            dists = np.empty((nq, k), np.float32)
+            _check(lib().pann_server_wait_knn(self._h, ticket, _ptr(ids), _ptr(dists), ctypes.byref(lat)))
+            return ids, dists, lat.value
+        offs = np.zeros(nq + 1, np.uint64)
+        cap = 1 << 22
+        ids = np.empty(cap, np.uint32)
+        _check(lib().pann_server_wait_range(self._h, ticket, _ptr(offs), _ptr(ids), cap, ctypes.byref(lat)))
+        return [ids[int(offs[i]):int(offs[i + 1])].copy() for i in range(nq)], lat.value
+
+    def stats(self, reset: bool = False) -> dict:
+        r, q = ctypes.c_uint64(), ctypes.c_uint64()
+        sec, p50, p99 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(lib().pann_server_stats(self._h, int(reset), ctypes.byref(r), ctypes.byref(q), ctypes.byref(sec),
+                                       ctypes.byref(p50), ctypes.byref(p99)))
+        return dict(requests=r.value, queries=q.value, seconds=sec.value, p50_s=p50.value, p99_s=p99.value)
+
+    def replay(self, arrival_s, kind, nq, k, beam, q_row, query_pool, range_params: RangeParams | None = None,
+               range_start: int = 0):
+        """Open-loop load generation in native code; returns (latencies_s, wall_s)."""
+        a = np.ascontiguousarray(arrival_s, np.float64)
+        n = len(a)
+        kd = np.ascontiguousarray(kind, np.uint32)
+        nqa = np.ascontiguousarray(nq, np.uint32)
+        ka = np.ascontiguousarray(k, np.uint32)
+        ba = np.ascontiguousarray(beam, np.uint32)
+        rows = np.ascontiguousarray(q_row, np.uint64)
+        pool = self._q(query_pool)
+        lat = np.zeros(n, np.float64)
+        wall = ctypes.c_double()
+        rp = range_params if range_params is not None else RangeParams(10, RANGE_BEAM, 0.0, 0.0, 0)
+        _check(lib().pann_server_replay(self._h, n, _ptr(a), _ptr(kd), _ptr(nqa), _ptr(ka), _ptr(ba), _ptr(rows),
+                                        _ptr(pool), ctypes.byref(rp), range_start, _ptr(lat), ctypes.byref(wall)))
+        return lat, wall.value
+
+    def close(self):
+        if self._h:
+            lib().pann_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

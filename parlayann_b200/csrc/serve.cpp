@@ -1,0 +1,478 @@
+// Serving form (include/parlayann_b200.h, pann_server_*): a request loop over
+// one resident index with continuous batching.
+//
+// The reference answers queries in closed batches (qsearchAll,
+// beamSearch.h:599-646; RangeSearch, rangeSearch.h:183-276); it has no request
+// loop. Here requests arrive one by one from any thread. A dispatcher thread
+// owns `inflight` batch slots, each a pann_batch (its device scratch sized for
+// max_batch_queries queries, which is the admission unit) with its own stream,
+// device and pinned host buffers. Whenever a slot is free it takes the waiting
+// k-NN requests in arrival order while their queries fit, launches the batch
+// (CUDA-graph replay of the tiered search) and moves on: requests that arrive
+// while other batches are on the GPU go into the next free slot, so batches
+// overlap on the device. Finished slots are retired by polling their events;
+// each request's latency runs from its submission to the moment its results
+// are in host memory. Range requests run on a second worker through
+// pann_range_search, concurrently with the k-NN batches. Results of a request
+// are the same as that request run alone (same kernels, per-query
+// parameters).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "index.cuh"
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct Request {
+  uint64_t ticket = 0;
+  int kind = 0;  // 0 = k-NN, 1 = range
+  uint32_t nq = 0, k = 0, beam = 0;
+  std::vector<uint8_t> queries;
+  pann_range_params rp{};
+  uint32_t start = 0;
+  // results
+  std::vector<uint32_t> ids;
+  std::vector<float> dists;
+  std::vector<uint64_t> offsets;
+  int rc = PANN_OK;
+  std::string err;
+  bool done = false;
+  clk::time_point t_submit, t_done;
+};
+
+struct Slot {
+  pann_batch* b = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  uint8_t* d_q = nullptr;
+  uint32_t* d_ids = nullptr;
+  float* d_d = nullptr;
+  uint8_t* h_q = nullptr;  // pinned
+  uint32_t* h_ids = nullptr;
+  float* h_d = nullptr;
+  std::vector<uint32_t> hk, hL;
+  std::vector<Request*> reqs;
+  uint32_t nq = 0;
+  bool busy = false;
+};
+
+}  // namespace
+
+struct pann_server {
+  pann_index* idx = nullptr;
+  pann_server_options opt{};
+  size_t row_bytes = 0;
+  std::vector<uint32_t> starts;
+  std::vector<Slot> slots;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Request*> knn_q, range_q;
+  std::unordered_map<uint64_t, Request*> reqs;
+  uint64_t next_ticket = 1;
+  bool stop = false;
+  std::thread dispatcher, ranger;
+  int device = 0;
+  // statistics since the last reset
+  std::vector<double> lat;
+  uint64_t done_queries = 0;
+  clk::time_point stats_t0;
+  std::string fatal;
+};
+
+namespace {
+
+void finish(pann_server* s, Request* r, int rc, const std::string& err) {
+  r->rc = rc;
+  r->err = err;
+  r->t_done = clk::now();
+  r->done = true;
+  s->lat.push_back(std::chrono::duration<double>(r->t_done - r->t_submit).count());
+  s->done_queries += r->nq;
+}
+
+// Copies a finished slot's results into its requests (called with s->mu held).
+void retire(pann_server* s, Slot& sl) {
+  uint32_t off = 0;
+  const uint32_t K = s->opt.max_k;
+  for (Request* r : sl.reqs) {
+    r->ids.resize((size_t)r->nq * r->k);
+    r->dists.resize((size_t)r->nq * r->k);
+    for (uint32_t i = 0; i < r->nq; i++) {
+      std::memcpy(&r->ids[(size_t)i * r->k], sl.h_ids + (size_t)(off + i) * K, 4ull * r->k);
+      std::memcpy(&r->dists[(size_t)i * r->k], sl.h_d + (size_t)(off + i) * K, 4ull * r->k);
+    }
+    off += r->nq;
+    finish(s, r, PANN_OK, "");
+  }
+  sl.reqs.clear();
+  sl.busy = false;
+}
+
+// Launches the waiting k-NN requests that fit into a free slot (s->mu held on
+// entry; released during the launch). Returns true if something was launched.
+bool launch(pann_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
+  if (s->knn_q.empty()) return false;
+  uint32_t nq = 0;
+  while (!s->knn_q.empty() && nq + s->knn_q.front()->nq <= s->opt.max_batch_queries) {
+    Request* r = s->knn_q.front();
+    s->knn_q.pop_front();
+    sl.reqs.push_back(r);
+    nq += r->nq;
+  }
+  if (sl.reqs.empty()) return false;
+  sl.busy = true;
+  sl.nq = nq;
+  lk.unlock();
+  uint32_t at = 0;
+  for (Request* r : sl.reqs) {
+    std::memcpy(sl.h_q + (size_t)at * s->row_bytes, r->queries.data(), (size_t)r->nq * s->row_bytes);
+    for (uint32_t i = 0; i < r->nq; i++) {
+      sl.hk[at + i] = r->k;
+      sl.hL[at + i] = r->beam;
+    }
+    at += r->nq;
+  }
+  int rc = PANN_OK;
+  cudaError_t e = cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * s->row_bytes, cudaMemcpyHostToDevice, sl.st);
+  if (e == cudaSuccess)
+    rc = pann_batch_run(sl.b, sl.d_q, nq, sl.hk.data(), sl.hL.data(), sl.d_ids, sl.d_d, nullptr, nullptr, nullptr, 1,
+                        sl.st);
+  const size_t ob = 4ull * nq * s->opt.max_k;
+  if (e == cudaSuccess && rc == PANN_OK) e = cudaMemcpyAsync(sl.h_ids, sl.d_ids, ob, cudaMemcpyDeviceToHost, sl.st);
+  if (e == cudaSuccess && rc == PANN_OK) e = cudaMemcpyAsync(sl.h_d, sl.d_d, ob, cudaMemcpyDeviceToHost, sl.st);
+  if (e == cudaSuccess && rc == PANN_OK) e = cudaEventRecord(sl.done, sl.st);
+  lk.lock();
+  if (e != cudaSuccess || rc != PANN_OK) {
+    std::string msg = e != cudaSuccess ? std::string("CUDA error: ") + cudaGetErrorString(e) : pann_last_error();
+    cudaStreamSynchronize(sl.st);
+    for (Request* r : sl.reqs) finish(s, r, rc != PANN_OK ? rc : PANN_EDEVICE, msg);
+    sl.reqs.clear();
+    sl.busy = false;
+    s->cv_done.notify_all();
+  }
+  return true;
+}
+
+void dispatcher_main(pann_server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    bool progress = false;
+    // retire finished batches
+    for (Slot& sl : s->slots) {
+      if (sl.busy && !sl.reqs.empty() && cudaEventQuery(sl.done) == cudaSuccess) {
+        retire(s, sl);
+        progress = true;
+      }
+    }
+    if (progress) s->cv_done.notify_all();
+    // fill free slots
+    for (Slot& sl : s->slots)
+      if (!sl.busy && launch(s, sl, lk)) progress = true;
+    bool any_busy = false;
+    for (Slot& sl : s->slots) any_busy |= sl.busy;
+    if (s->stop && !any_busy && s->knn_q.empty()) break;
+    if (!progress) {
+      // batches on the device: poll their events at a short interval; idle:
+      // sleep until a request arrives
+      if (any_busy) s->cv_work.wait_for(lk, std::chrono::microseconds(20));
+      else s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+    }
+  }
+}
+
+void ranger_main(pann_server* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    if (s->range_q.empty()) {
+      if (s->stop) break;
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+      continue;
+    }
+    Request* r = s->range_q.front();
+    s->range_q.pop_front();
+    lk.unlock();
+    std::vector<uint64_t> offs((size_t)r->nq + 1, 0);
+    std::vector<uint32_t> ids((size_t)r->nq * r->rp.beam * 4 + 16);
+    int rc = pann_range_search(s->idx, r->queries.data(), r->nq, &r->rp, r->start, offs.data(), ids.data(), ids.size(),
+                               nullptr, nullptr, nullptr);
+    if (rc == PANN_EOVERFLOW && offs[r->nq] > ids.size()) {
+      ids.resize(offs[r->nq]);
+      rc = pann_range_search(s->idx, r->queries.data(), r->nq, &r->rp, r->start, offs.data(), ids.data(), ids.size(),
+                             nullptr, nullptr, nullptr);
+    }
+    std::string msg = rc ? pann_last_error() : "";
+    ids.resize(rc == PANN_OK ? offs[r->nq] : 0);
+    lk.lock();
+    r->offsets = std::move(offs);
+    r->ids = std::move(ids);
+    finish(s, r, rc, msg);
+    s->cv_done.notify_all();
+  }
+}
+
+int submit(pann_server* s, Request* r, uint64_t* ticket) {
+  r->t_submit = clk::now();
+  std::lock_guard<std::mutex> g(s->mu);
+  if (s->stop) {
+    delete r;
+    return pann::fail(PANN_EINVAL, "server is stopping");
+  }
+  r->ticket = s->next_ticket++;
+  s->reqs[r->ticket] = r;
+  (r->kind == 0 ? s->knn_q : s->range_q).push_back(r);
+  *ticket = r->ticket;
+  s->cv_work.notify_all();
+  return PANN_OK;
+}
+
+// Waits for a ticket and removes it (s->mu not held on entry).
+Request* take(pann_server* s, uint64_t ticket, int* rc) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) {
+    *rc = pann::fail(PANN_EINVAL, "unknown ticket");
+    return nullptr;
+  }
+  Request* r = it->second;
+  s->cv_done.wait(lk, [&] { return r->done; });
+  s->reqs.erase(it);
+  *rc = PANN_OK;
+  return r;
+}
+
+double quantile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  size_t i = (size_t)std::min<double>((double)v.size() - 1, std::floor(q * (double)(v.size() - 1) + 0.5));
+  return v[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+int pann_server_create(pann_server** out, pann_index* idx, const pann_server_options* opt, const uint32_t* starts,
+                       uint32_t n_start) {
+  if (!out || !idx || !opt || !starts) return pann::fail(PANN_EINVAL, "NULL argument");
+  if (!idx->points_set) return pann::fail(PANN_EINVAL, "index has no points (pann_index_set_points)");
+  *out = nullptr;
+  if (opt->max_batch_queries == 0 || opt->inflight == 0 || opt->inflight > 16)
+    return pann::fail(PANN_EINVAL, "max_batch_queries must be positive and inflight in [1, 16]");
+  pann_server* s = new pann_server();
+  s->idx = idx;
+  s->opt = *opt;
+  s->starts.assign(starts, starts + n_start);
+  cudaGetDevice(&s->device);
+  pann_query_params bounds{opt->max_k, opt->max_beam, opt->limit, opt->degree_limit, opt->batch_factor};
+  pann_search_options so{opt->precision, 0};
+  pann_batch_options bo{1, 0, 0, 0};
+  s->row_bytes = (size_t)idx->d * idx->esize;
+  s->slots.resize(opt->inflight);
+  auto bail = [&](int rc) {
+    pann_server_destroy(s);
+    return rc;
+  };
+  for (Slot& sl : s->slots) {
+    int rc = pann_batch_create(&sl.b, idx, opt->max_batch_queries, &bounds, starts, n_start, &so, &bo);
+    if (rc) return bail(rc);
+    const size_t m = opt->max_batch_queries;
+    cudaError_t e = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&sl.d_q, m * s->row_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&sl.d_ids, 4 * m * opt->max_k);
+    if (e == cudaSuccess) e = cudaMalloc(&sl.d_d, 4 * m * opt->max_k);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_q, m * s->row_bytes);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_ids, 4 * m * opt->max_k);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_d, 4 * m * opt->max_k);
+    if (e != cudaSuccess) return bail(pann::cuda_fail(e, "server slot"));
+    sl.hk.resize(m);
+    sl.hL.resize(m);
+  }
+  s->stats_t0 = clk::now();
+  s->dispatcher = std::thread(dispatcher_main, s);
+  s->ranger = std::thread(ranger_main, s);
+  *out = s;
+  return PANN_OK;
+}
+
+int pann_server_submit_knn(pann_server* s, const void* queries, uint32_t nq, uint32_t k, uint32_t beam,
+                           uint64_t* ticket) {
+  if (!s || !queries || !ticket) return pann::fail(PANN_EINVAL, "NULL argument");
+  if (nq == 0 || nq > s->opt.max_batch_queries)
+    return pann::fail(PANN_EINVAL, "a request needs 1 to max_batch_queries queries");
+  if (k == 0 || k > s->opt.max_k || beam < k || beam > s->opt.max_beam || beam < s->starts.size())
+    return pann::fail(PANN_EINVAL, "k / beam outside the server's bounds (1 <= k <= beam <= max_beam, k <= max_k)");
+  Request* r = new Request();
+  r->kind = 0;
+  r->nq = nq;
+  r->k = k;
+  r->beam = beam;
+  r->queries.assign(static_cast<const uint8_t*>(queries), static_cast<const uint8_t*>(queries) + (size_t)nq * s->row_bytes);
+  return submit(s, r, ticket);
+}
+
+int pann_server_submit_range(pann_server* s, const void* queries, uint32_t nq, const pann_range_params* rp,
+                             uint32_t start_point, uint64_t* ticket) {
+  if (!s || !queries || !rp || !ticket) return pann::fail(PANN_EINVAL, "NULL argument");
+  if (nq == 0) return pann::fail(PANN_EINVAL, "a request needs at least one query");
+  Request* r = new Request();
+  r->kind = 1;
+  r->nq = nq;
+  r->rp = *rp;
+  r->start = start_point;
+  r->queries.assign(static_cast<const uint8_t*>(queries), static_cast<const uint8_t*>(queries) + (size_t)nq * s->row_bytes);
+  return submit(s, r, ticket);
+}
+
+int pann_server_wait_knn(pann_server* s, uint64_t ticket, uint32_t* out_ids, float* out_dists, double* latency_s) {
+  if (!s) return pann::fail(PANN_EINVAL, "server is NULL");
+  int rc;
+  Request* r = take(s, ticket, &rc);
+  if (!r) return rc;
+  if (r->kind != 0) {
+    delete r;
+    return pann::fail(PANN_EINVAL, "ticket is a range request");
+  }
+  rc = r->rc;
+  if (rc == PANN_OK) {
+    if (out_ids) std::memcpy(out_ids, r->ids.data(), 4 * r->ids.size());
+    if (out_dists) std::memcpy(out_dists, r->dists.data(), 4 * r->dists.size());
+  } else {
+    pann::fail(rc, r->err);
+  }
+  if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  delete r;
+  return rc;
+}
+
+int pann_server_wait_range(pann_server* s, uint64_t ticket, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
+                           double* latency_s) {
+  if (!s) return pann::fail(PANN_EINVAL, "server is NULL");
+  int rc;
+  Request* r = take(s, ticket, &rc);
+  if (!r) return rc;
+  if (r->kind != 1) {
+    delete r;
+    return pann::fail(PANN_EINVAL, "ticket is a k-NN request");
+  }
+  rc = r->rc;
+  if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+  if (rc == PANN_OK) {
+    if (out_offsets) std::memcpy(out_offsets, r->offsets.data(), 8 * r->offsets.size());
+    if (r->ids.size() > ids_cap) {
+      rc = pann::fail(PANN_EOVERFLOW, "range answers need " + std::to_string(r->ids.size()) + " ids");
+    } else if (out_ids && !r->ids.empty()) {
+      std::memcpy(out_ids, r->ids.data(), 4 * r->ids.size());
+    }
+  } else {
+    pann::fail(rc, r->err);
+  }
+  delete r;
+  return rc;
+}
+
+int pann_server_stats(pann_server* s, int reset, uint64_t* requests, uint64_t* queries, double* seconds, double* p50_s,
+                      double* p99_s) {
+  if (!s) return pann::fail(PANN_EINVAL, "server is NULL");
+  std::lock_guard<std::mutex> g(s->mu);
+  if (requests) *requests = s->lat.size();
+  if (queries) *queries = s->done_queries;
+  if (seconds) *seconds = std::chrono::duration<double>(clk::now() - s->stats_t0).count();
+  if (p50_s) *p50_s = quantile(s->lat, 0.50);
+  if (p99_s) *p99_s = quantile(s->lat, 0.99);
+  if (reset) {
+    s->lat.clear();
+    s->done_queries = 0;
+    s->stats_t0 = clk::now();
+  }
+  return PANN_OK;
+}
+
+int pann_server_destroy(pann_server* s) {
+  if (!s) return PANN_OK;
+  {
+    std::lock_guard<std::mutex> g(s->mu);
+    s->stop = true;
+    s->cv_work.notify_all();
+  }
+  if (s->dispatcher.joinable()) s->dispatcher.join();
+  if (s->ranger.joinable()) s->ranger.join();
+  for (auto& kv : s->reqs) delete kv.second;
+  for (Slot& sl : s->slots) {
+    if (sl.st) cudaStreamSynchronize(sl.st);
+    if (sl.b) pann_batch_destroy(sl.b);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.st) cudaStreamDestroy(sl.st);
+    if (sl.d_q) cudaFree(sl.d_q);
+    if (sl.d_ids) cudaFree(sl.d_ids);
+    if (sl.d_d) cudaFree(sl.d_d);
+    if (sl.h_q) cudaFreeHost(sl.h_q);
+    if (sl.h_ids) cudaFreeHost(sl.h_ids);
+    if (sl.h_d) cudaFreeHost(sl.h_d);
+  }
+  delete s;
+  return PANN_OK;
+}
+
+// Open-loop load generator: submits request i at arrival_s[i] seconds after the
+// call starts (k-NN when kind[i] == 0, else range with *rp), from queries
+// pool rows q_row[i] .. q_row[i] + nq[i] - 1, waits for all, and reports each
+// request's latency and the wall time from the first submission to the last
+// completion.
+int pann_server_replay(pann_server* s, uint32_t nreq, const double* arrival_s, const uint32_t* kind,
+                       const uint32_t* nq, const uint32_t* k, const uint32_t* beam, const uint64_t* q_row,
+                       const void* query_pool, const pann_range_params* rp, uint32_t range_start, double* out_latency_s,
+                       double* out_wall_s) {
+  if (!s || (nreq && (!arrival_s || !kind || !nq || !q_row || !query_pool))) return pann::fail(PANN_EINVAL, "NULL argument");
+  std::vector<uint64_t> tickets(nreq, 0);
+  std::vector<int> rcs(nreq, PANN_OK);
+  std::atomic<uint32_t> submitted{0};
+  const uint8_t* pool = static_cast<const uint8_t*>(query_pool);
+  const auto t0 = clk::now();
+  std::thread waiter([&] {
+    for (uint32_t i = 0; i < nreq; i++) {
+      while (submitted.load(std::memory_order_acquire) <= i) std::this_thread::yield();
+      if (rcs[i] != PANN_OK) continue;
+      double lat = 0;
+      if (kind[i] == 0) {
+        rcs[i] = pann_server_wait_knn(s, tickets[i], nullptr, nullptr, &lat);
+      } else {
+        rcs[i] = pann_server_wait_range(s, tickets[i], nullptr, nullptr, ~0ull, &lat);
+      }
+      if (out_latency_s) out_latency_s[i] = lat;
+    }
+  });
+  for (uint32_t i = 0; i < nreq; i++) {
+    const auto when = t0 + std::chrono::duration_cast<clk::duration>(std::chrono::duration<double>(arrival_s[i]));
+    while (clk::now() < when) {
+      auto left = when - clk::now();
+      if (left > std::chrono::microseconds(200)) std::this_thread::sleep_for(left - std::chrono::microseconds(100));
+    }
+    const void* q = pool + (size_t)q_row[i] * s->row_bytes;
+    rcs[i] = kind[i] == 0 ? pann_server_submit_knn(s, q, nq[i], k[i], beam[i], &tickets[i])
+                          : pann_server_submit_range(s, q, nq[i], rp, range_start, &tickets[i]);
+    submitted.store(i + 1, std::memory_order_release);
+  }
+  waiter.join();
+  if (out_wall_s) *out_wall_s = std::chrono::duration<double>(clk::now() - t0).count();
+  for (uint32_t i = 0; i < nreq; i++)
+    if (rcs[i] != PANN_OK) return pann::fail(rcs[i], "request " + std::to_string(i) + " failed");
+  return PANN_OK;
+}
+
+}  // extern "C"
