@@ -276,6 +276,9 @@ def run_ours(args):
     achieved = bytes_per_query * nq / per_launch_s / 1e9
     traffic_pq, prof = profiled_traffic()
     line = None
+    forms = None
+    if rank == 0 and not args.no_forms:
+        forms = run_forms(idx, base, q, gt, gd, beam, qps, dev, flush, args)
     if rank == 0:
         cpu = cpu_baseline(base, q, g, beam, args) if not args.no_cpu_baseline else None
         line = {
@@ -309,6 +312,8 @@ def run_ours(args):
                          "traffic_unit": "GB per launch (ncu dram read+write, scaled from profiles/)"},
             "cpu_baseline": cpu,
         }
+        if forms is not None:
+            line["forms"] = forms
         c = clk.summary()
         if c:
             line["clocks"] = c
@@ -317,6 +322,217 @@ def run_ours(args):
         dist.destroy_process_group()
     idx.close()
     return line
+
+
+def _timed(step, flush, stream, steps, warmup):
+    """Device seconds per step: CUDA events on `stream`, L2 flushed outside each timed span."""
+    import torch
+
+    for _ in range(warmup):
+        flush.fill_(1)
+        step()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        tot += e0.elapsed_time(e1) / 1e3
+    return tot / steps
+
+
+def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
+    """The precision, batched and serving forms and range search on the same
+    index, each next to the plain form: QPS at recall@10 >= 0.95 (device
+    timed), recall loss and distance error against FP64 brute force, p50/p99
+    latency under open-loop load."""
+    import torch
+
+    import parlayann_b200 as P
+
+    lib = P.lib()
+    k = W["k"]
+    nq = q.shape[0]
+    stream = torch.cuda.current_stream(dev)
+    starts = np.zeros(1, np.uint32)
+    dq = torch.from_numpy(q).to(dev)
+    out = {}
+    steps = max(3, min(args.steps, 10))
+
+    # FP64 distances of returned ids, for the distance error per precision
+    b64 = None
+
+    def dist_err(ids, dists):
+        nonlocal b64
+        sel = ids[:1000].astype(np.int64)
+        qq = q[:1000].astype(np.float64)
+        bb = base[sel.ravel()].astype(np.float64).reshape(sel.shape[0], sel.shape[1], -1)
+        d64 = ((bb - qq[:, None, :]) ** 2).sum(-1)
+        rel = np.abs(dists[:1000].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
+        return float(rel.max()), float(rel.mean())
+
+    # ---- precision form (+ batched): smallest beam with recall >= 0.95, device QPS through a batch object
+    prec_out = {}
+    exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, gd, k)
+    for name, prec, parents in (("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
+                                ("fp8_tile2", P.PREC_FP8, 2)):
+        idx.set_precision(prec)
+        pbeam, prec_rec, pres = None, None, None
+        for L in BEAMS:
+            if L < beam - 10:
+                continue
+            r = idx.search(q, k, L, precision=prec, parents=parents)
+            rec = P.recall_with_ties(r.ids, gt, gd, k)
+            if rec >= 0.95:
+                pbeam, prec_rec, pres = L, rec, r
+                break
+        if pbeam is None:
+            continue
+        same_beam = idx.search(q, k, beam, precision=prec, parents=parents)
+        loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, gd, k)
+        b = idx.batch(nq, k, pbeam, precision=prec, parents=parents)
+        d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+        d_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
+        ks = np.full(nq, k, np.uint32)
+        Ls = np.full(nq, pbeam, np.uint32)
+
+        def step_b():
+            rc = lib.pann_batch_run(b.handle, ctypes.c_void_p(dq.data_ptr()), nq, ks.ctypes.data_as(ctypes.c_void_p),
+                                    Ls.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(d_ids.data_ptr()),
+                                    ctypes.c_void_p(d_d.data_ptr()), None, None, None, 1,
+                                    ctypes.c_void_p(stream.cuda_stream))
+            if rc != 0:
+                raise P.PannError(rc, lib.pann_last_error().decode())
+
+        t = _timed(step_b, flush, stream, steps, 3)
+        ids_b = d_ids.cpu().numpy().astype(np.uint32)
+        assert np.array_equal(ids_b, pres.ids), "batched precision form differs from the plain precision form"
+        mx, mean = dist_err(pres.ids, pres.dists)
+        prec_out[name] = {"beam": pbeam, "parents": parents, "recall_at_10": round(prec_rec, 4),
+                          "stopped_early": int(((pres.flags & 2) != 0).sum()), "qps_batched_graph": round(nq / t, 1),
+                          "speedup_vs_plain": round(nq / t / qps_plain, 3),
+                          "recall_loss_at_plain_beam": round(loss, 4),
+                          "reported_distance_rel_error_vs_fp64": {"max": mx, "mean": mean}}
+        b.close()
+    idx.set_precision(P.PREC_F32)
+    out["precision_batched"] = prec_out
+
+    # ---- batched form with uneven shapes: k in {1,10,100}, beam uniform in [k, 4k] (beam >= 10 for k = 1)
+    rng = np.random.default_rng(5)
+    ks = rng.choice(np.array([1, 10, 100], np.uint32), nq).astype(np.uint32)
+    Ls = np.array([rng.integers(max(kk, 1), 4 * kk + 1) for kk in ks], np.uint32)
+    b = idx.batch(nq, 100, int(Ls.max()))
+    d_ids = torch.empty((nq, 100), dtype=torch.int32, device=dev)
+    d_d = torch.empty((nq, 100), dtype=torch.float32, device=dev)
+
+    def step_u():
+        rc = lib.pann_batch_run(b.handle, ctypes.c_void_p(dq.data_ptr()), nq, ks.ctypes.data_as(ctypes.c_void_p),
+                                Ls.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(d_ids.data_ptr()),
+                                ctypes.c_void_p(d_d.data_ptr()), None, None, None, 1,
+                                ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise P.PannError(rc, lib.pann_last_error().decode())
+
+    t_b = _timed(step_u, flush, stream, steps, 3)
+    ids_u = d_ids.cpu().numpy().astype(np.uint32)
+    b.close()
+    # the plain form on the same mix: one pann_search_device launch sequence per (k, beam) group
+    groups = {}
+    for i, (kk, LL) in enumerate(zip(ks.tolist(), Ls.tolist())):
+        groups.setdefault((kk, LL), []).append(i)
+    gq = {key: torch.from_numpy(q[np.array(v)]).to(dev) for key, v in groups.items()}
+    gout = {key: torch.empty((len(v), key[0]), dtype=torch.int32, device=dev) for key, v in groups.items()}
+
+    def step_plain_groups():
+        for key, v in groups.items():
+            qp = P.QueryParams(key[0], key[1], W["n"], W["R"], W["bf"])
+            rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(gq[key].data_ptr()), len(v), ctypes.byref(qp),
+                                        starts.ctypes.data_as(ctypes.c_void_p), 1,
+                                        ctypes.c_void_p(gout[key].data_ptr()), None, None, None, None,
+                                        ctypes.c_void_p(stream.cuda_stream))
+            if rc != 0:
+                raise P.PannError(rc, lib.pann_last_error().decode())
+
+    t_p = _timed(step_plain_groups, flush, stream, steps, 3)
+    exact = all(np.array_equal(ids_u[np.array(v), :key[0]], gout[key].cpu().numpy().astype(np.uint32))
+                for key, v in groups.items())
+    out["batched_uneven"] = {"queries": nq, "k": "uniform in {1,10,100}", "beam": "uniform in [k, 4k]",
+                             "qps_batched_graph": round(nq / t_b, 1), "qps_plain_per_shape": round(nq / t_p, 1),
+                             "shape_groups": len(groups), "speedup": round(t_p / t_b, 3),
+                             "bit_exact_with_plain": bool(exact)}
+
+    # ---- range search: radius = the 1%-quantile of sampled base-query distances
+    samp = []
+    rs = np.random.default_rng(6)
+    for i in rs.choice(nq, 16, replace=False):
+        cols = rs.choice(W["n"], 4000, replace=False)
+        samp.append(((base[cols] - q[i]) ** 2).sum(1))
+    radius = float(np.quantile(np.concatenate(samp), 0.01))
+    nr = 200
+    t0 = time.perf_counter()
+    rr = idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)
+    t_r = time.perf_counter() - t0
+    sizes = np.array([len(x) for x in rr["ids"]])
+    out["range"] = {"queries": nr, "beam": 20, "type": "greedy", "radius_quantile": 0.01, "radius": radius,
+                    "qps_e2e": round(nr / t_r, 1), "mean_answer": float(sizes.mean()),
+                    "answer_ids_per_s": round(float(sizes.sum()) / t_r, 1)}
+
+    # ---- serving form: open-loop Poisson arrivals at 5 offered rates, for the
+    # plain form and for the fastest precision form found above
+    rng = np.random.default_rng(7)
+    rp = P.RangeParams(20, P.RANGE_GREEDY, radius, 0.0, 0)
+    forms = [("plain", P.PREC_F32, 0, beam)]
+    best = max(prec_out.items(), key=lambda kv: kv[1]["qps_batched_graph"]) if prec_out else None
+    if best is not None:
+        nm, info = best
+        forms.append((nm, P.PREC_BF16 if nm.startswith("bf16") else P.PREC_FP8, info["parents"], info["beam"]))
+    serving = {}
+    for fname, prec, parents, kbeam in forms:
+        if prec != P.PREC_F32:
+            idx.set_precision(prec)
+        srv = P.Server(idx, max_batch_queries=4096, inflight=3, max_k=100, max_beam=max(200, kbeam), precision=prec,
+                       parents=parents)
+
+        def schedule(n, rate_qps, range_frac):
+            nqs = rng.integers(1, 257, n)
+            kinds = (rng.random(n) < range_frac).astype(np.uint32)
+            nqs[kinds == 1] = 1
+            kk = rng.choice(np.array([10, 100], np.uint32), n)
+            bb = np.where(kk == 10, kbeam, 200).astype(np.uint32)
+            gaps = rng.exponential(float(nqs.mean()) / rate_qps, n) if rate_qps else np.zeros(n)
+            rows = rng.integers(0, nq - 257, n)
+            return np.cumsum(gaps), kinds, nqs, kk, bb, rows
+
+        a, kd, nqs, kk, bb, rows = schedule(400, 0, 0.0)  # capacity: everything at t = 0
+        lat, wall = srv.replay(a, kd, nqs, kk, bb, rows, q, rp)
+        cap_qps = float(nqs.sum()) / wall
+        rates = []
+        for frac in (0.2, 0.4, 0.6, 0.8, 0.95):
+            rate = frac * cap_qps
+            n = int(min(20000, max(200, rate * 2.0 / 128)))
+            a, kd, nqs, kk, bb, rows = schedule(n, rate, 0.01)
+            lat, wall = srv.replay(a, kd, nqs, kk, bb, rows, q, rp)
+            kn, rg = lat[kd == 0], lat[kd == 1]
+            rates.append({"offered_qps": round(rate, 1), "achieved_qps": round(float(nqs.sum()) / wall, 1),
+                          "requests": n, "range_requests": int(kd.sum()),
+                          "p50_ms": round(1e3 * float(np.percentile(lat, 50)), 3),
+                          "p99_ms": round(1e3 * float(np.percentile(lat, 99)), 3),
+                          "knn_p50_ms": round(1e3 * float(np.percentile(kn, 50)), 3),
+                          "knn_p99_ms": round(1e3 * float(np.percentile(kn, 99)), 3),
+                          "range_p50_ms": round(1e3 * float(np.percentile(rg, 50)), 3) if len(rg) else None,
+                          "range_p99_ms": round(1e3 * float(np.percentile(rg, 99)), 3) if len(rg) else None})
+        srv.close()
+        serving[fname] = {"precision": int(prec), "parents": parents, "beam_k10": kbeam,
+                          "capacity_qps_closed": round(cap_qps, 1), "rates": rates}
+    idx.set_precision(P.PREC_F32)
+    out["serving"] = {"requests": "1-256 queries, k in {10,100} (beam for recall@10 >= 0.95 / 200), 1% range "
+                                  "requests (1 query, beam 20, greedy, radius at the 1% distance quantile)",
+                      "slots": 3, "batch_queries": 4096, "forms": serving}
+    return out
 
 
 def cpu_baseline(base, q, graph, beam, args):
@@ -402,6 +618,7 @@ def main():
     ap.add_argument("--beam", type=int, default=0, help="fix the beam instead of sweeping for recall 0.95")
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision / batched / range / serving forms")
     ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
     ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
     args = ap.parse_args()

@@ -105,9 +105,10 @@ int pann_graph_save(pann_index* idx, const char* path);
  * QueryParams; host buffers. Writes the first k frontier entries (ids,
  * distances) per query, and per-query visited-list size and distance
  * comparisons (stats<T> counters). Any of out_dists / out_visited / out_cmps /
- * out_flags may be NULL. out_flags[i] is 1 where the reference's hashset grows
+ * out_flags may be NULL. out_flags[i] bit 0 is set where the reference's hashset grows
  * on query i (hashset.h:25-38); those queries are reproduced by an exact
- * emulation of that hashset, so results still equal the reference's.
+ * emulation of that hashset, so results still equal the reference's. Bit 1
+ * is set where a tile search (pann_search_options::parents) stopped early.
  * Replaces qsearchAll / searchAll / beam_search (beamSearch.h:420-445,
  * 492-526, 599-646). */
 int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
@@ -183,6 +184,11 @@ int pann_search_lists(pann_index* idx, const void* queries, uint32_t nq, const p
 typedef struct {
   int32_t precision; /* PANN_PREC_* */
   uint32_t rerank;   /* candidates re-ranked in float32 (0 = 4k) */
+  uint32_t parents;  /* 0: the reference's traversal (one node expanded per step). > 0 (low precision
+                        only): the tile search, one CTA per query expanding up to `parents` (<= 4)
+                        frontier nodes per step and scoring their new neighbours as one tile staged in
+                        shared memory; its own visiting order and recall curve. Status bit 32 marks a
+                        query whose seen set filled (it stopped early). */
 } pann_search_options;
 
 /* Build the low-precision copy of the points used by `precision` (kept until
@@ -302,6 +308,7 @@ typedef struct {
   uint32_t degree_limit;
   double batch_factor;
   int32_t precision;          /* PANN_PREC_*; low precision needs pann_index_set_precision first */
+  uint32_t parents;           /* pann_search_options::parents of every k-NN request */
 } pann_server_options;
 
 int pann_server_create(pann_server** out, pann_index* idx, const pann_server_options* opt, const uint32_t* starts,

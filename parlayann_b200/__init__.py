@@ -52,7 +52,7 @@ class QueryParams(ctypes.Structure):
 class SearchOptions(ctypes.Structure):
     """pann_search_options: precision form and re-rank count."""
 
-    _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32)]
+    _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32), ("parents", ctypes.c_uint32)]
 
 
 class BatchOptions(ctypes.Structure):
@@ -77,7 +77,7 @@ class ServerOptions(ctypes.Structure):
 
     _fields_ = [("max_batch_queries", ctypes.c_uint32), ("inflight", ctypes.c_uint32), ("max_k", ctypes.c_uint32),
                 ("max_beam", ctypes.c_uint32), ("limit", ctypes.c_uint64), ("degree_limit", ctypes.c_uint32),
-                ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32)]
+                ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32), ("parents", ctypes.c_uint32)]
 
 
 class BuildParams(ctypes.Structure):
@@ -288,7 +288,7 @@ class Index:
 
     def search(self, queries: np.ndarray, k: int, L: int, limit: int | None = None, degree_limit: int | None = None,
                batch_factor: float = 0.125, starts=(0,), allow_short: bool = False, precision: int = PREC_F32,
-               rerank: int = 0) -> SearchResult:
+               rerank: int = 0, parents: int = 0) -> SearchResult:
         queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
         nq = queries.shape[0]
         qp = QueryParams(k, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
@@ -299,11 +299,11 @@ class Index:
         vis = np.empty(nq, np.uint32)
         cmps = np.empty(nq, np.uint32)
         flags = np.empty(nq, np.uint32)
-        if precision == PREC_F32 and rerank == 0:
+        if precision == PREC_F32 and rerank == 0 and parents == 0:
             rc = lib().pann_search(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(ids),
                                    _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags))
         else:
-            opt = SearchOptions(precision, rerank)
+            opt = SearchOptions(precision, rerank, parents)
             rc = lib().pann_search_ex(self._h, _ptr(queries), nq, ctypes.byref(qp), ctypes.byref(opt), _ptr(st),
                                       len(st), _ptr(ids), _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags), 0, None)
         if not (allow_short and rc == PANN_ESHORT):
@@ -313,10 +313,10 @@ class Index:
     def batch(self, max_queries: int, max_k: int, max_beam: int, limit: int | None = None,
               degree_limit: int | None = None, batch_factor: float = 0.125, starts=(0,), precision: int = PREC_F32,
               rerank: int = 0, use_graph: bool = True, autotune: bool = False, seen_slots: int = 0,
-              warps_per_block: int = 0) -> "Batch":
+              warps_per_block: int = 0, parents: int = 0) -> "Batch":
         """A reusable batch for queries with per-query k and beam (pann_batch_create)."""
         return Batch(self, max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts, precision, rerank,
-                     use_graph, autotune, seen_slots, warps_per_block)
+                     use_graph, autotune, seen_slots, warps_per_block, parents)
 
     def range_search(self, queries: np.ndarray, beam: int, radius: float, rtype: int = RANGE_GREEDY, start: int = 0,
                      early_stopping_radius: float = 0.0, early_stopping_count: int = 0):
@@ -376,13 +376,13 @@ class Batch:
     graph). Per query the results equal Index.search with that k and beam."""
 
     def __init__(self, index: "Index", max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts,
-                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block):
+                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block, parents=0):
         self.index = index
         self.max_k = max_k
         qp = QueryParams(max_k, max_beam, index.n if limit is None else limit,
                          index.R if degree_limit is None else degree_limit, batch_factor)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
-        opt = SearchOptions(precision, rerank)
+        opt = SearchOptions(precision, rerank, parents)
         bo = BatchOptions(int(use_graph), int(autotune), seen_slots, warps_per_block)
         h = ctypes.c_void_p()
         _check(lib().pann_batch_create(ctypes.byref(h), index.handle, max_queries, ctypes.byref(qp), _ptr(st), len(st),
@@ -433,10 +433,10 @@ class Server:
 
     def __init__(self, index: "Index", max_batch_queries: int = 1024, inflight: int = 3, max_k: int = 100,
                  max_beam: int = 400, limit: int | None = None, degree_limit: int | None = None,
-                 batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,)):
+                 batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,), parents: int = 0):
         self.index = index
         o = ServerOptions(max_batch_queries, inflight, max_k, max_beam, index.n if limit is None else limit,
-                          index.R if degree_limit is None else degree_limit, batch_factor, precision)
+                          index.R if degree_limit is None else degree_limit, batch_factor, precision, parents)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
         h = ctypes.c_void_p()
         _check(lib().pann_server_create(ctypes.byref(h), index.handle, ctypes.byref(o), _ptr(st), len(st)))

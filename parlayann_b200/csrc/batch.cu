@@ -28,6 +28,7 @@ struct pann_batch {
   uint32_t max_q = 0;
   int prec = 0;
   uint32_t rerank = 0;
+  uint32_t parents = 0;
   pann_batch_options bopt{};
   pann::TierSizes z{};
   // device buffers, allocated at creation
@@ -82,6 +83,12 @@ static int enqueue(pann_batch* b, const TierSizes& z, cudaStream_t st) {
   a.qk = b->qk.as<uint32_t>();
   a.qL = b->qL.as<uint32_t>();
   a.kstride = b->plan.k;
+  if (b->parents > 0 && b->prec != PREC_F32) {
+    a.job_list = b->order.as<uint32_t>();
+    a.njobs_dev = b->counters.as<uint32_t>() + 32;
+    int rc = enqueue_tile(idx, b->plan, a, b->parents, b->counters.as<uint32_t>() + 10, b->prec, b->rerank, st);
+    if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; the single-parent tiers below
+  }
   return enqueue_tiers(idx, b->plan, a, z, tier_bufs(b), st, b->prec, b->rerank);
 }
 
@@ -163,6 +170,7 @@ int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, c
   b->max_q = max_queries;
   b->prec = prec;
   b->rerank = opt ? opt->rerank : 0;
+  b->parents = opt ? opt->parents : 0;
   if (bopt) b->bopt = *bopt;
   auto bail = [&](int code) {
     pann_batch_destroy(b);
@@ -297,7 +305,7 @@ int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32
   int rc2 = PANN_OK;
   for (uint32_t i = 0; i < nq; i++) {
     uint32_t s = status[i];
-    if (out_flags) out_flags[i] = (s & QS_REF_WOULD_GROW) ? 1u : 0u;
+    if (out_flags) out_flags[i] = ((s & QS_REF_WOULD_GROW) ? 1u : 0u) | ((s & 32u) ? 2u : 0u);
     if (s & (QS_TABLE_FULL | QS_INTERNAL)) rc2 = PANN_EOVERFLOW;
     else if ((s & QS_SHORT) && rc2 == PANN_OK) rc2 = PANN_ESHORT;
   }
@@ -318,7 +326,7 @@ int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps
 
 int pann_batch_destroy(pann_batch* b) {
   if (!b) return PANN_OK;
-  if (b->idx && b->idx->stream) cudaStreamSynchronize(b->idx->stream);
+  // the index may already be gone: touch only the batch's own objects
   if (b->cap) cudaStreamSynchronize(b->cap);
   if (b->staged) cudaEventSynchronize(b->staged);
   if (b->exec) cudaGraphExecDestroy(b->exec);

@@ -131,7 +131,7 @@ extern "C" int pann_groundtruth(pann_index* idx, const void* queries, uint32_t n
 #define PANN_BF_CASE(DT, MT)                                                                                   \
   if (idx->dtype == DT && idx->metric == MT) {                                                                 \
     auto kern = bruteforce_kernel<DT, MT>;                                                                     \
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);                        \
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());                        \
     kern<<<blocks, 256, smem, st>>>(idx->d_points, idx->n, idx->stride, (int)idx->d, dq, nq, k, dids, dd);     \
     e = cudaGetLastError();                                                                                    \
   }

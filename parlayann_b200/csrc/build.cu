@@ -636,7 +636,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
       constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
       size_t sm = wpb * (stride + 16ull * R);
       auto kern = sort_neighbors_kernel<DT, MT>;
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
       int blocks = (int)std::min<uint64_t>((n + wpb - 1) / wpb, 65535ull * 8);
       kern<<<blocks, 32 * wpb, sm, st>>>(idx->d_points, stride, d, nch, idx->d_graph, R, n);
       return cudaGetLastError();

@@ -102,6 +102,18 @@ __global__ void to_fp8_kernel(const float* __restrict__ src, uint64_t src_stride
   }
 }
 
+int smem_attr_max() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 48 * 1024;
+  if (cached[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0) v = 48 * 1024;
+    cached[dev] = v;  // the same value from every thread: a benign race
+  }
+  return cached[dev];
+}
+
 int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan) {
   if (!qp) return fail(PANN_EINVAL, "query params are NULL");
   if (qp->beam == 0) return fail(PANN_EINVAL, "beam (L) must be positive");
@@ -141,7 +153,7 @@ static uint32_t pow2_at_least(uint64_t x) {
 template <int DT, int MT, bool G, int PREC = PREC_F32>
 static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
   auto k = search_kernel<DT, MT, G, PREC>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return e;
   k<<<blocks, threads, smem, st>>>(a);
   return cudaGetLastError();
@@ -179,7 +191,7 @@ cudaError_t launch_search(int dtype, int metric, bool global_table, const Search
 template <int DT, int MT, bool SM>
 static cudaError_t launch_emulate_t(const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem, cudaStream_t st) {
   auto k = search_emulate_kernel<DT, MT, SM>;
-  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (err != cudaSuccess) return err;
   k<<<blocks, 32, smem, st>>>(a, e);
   return cudaGetLastError();
@@ -204,7 +216,7 @@ template <int DT, int MT, bool G, int PREC = PREC_F32>
 static int occupancy_t(int threads, size_t smem) {
   int nb = 0;
   auto k = search_kernel<DT, MT, G, PREC>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
   return nb;
 }
@@ -459,10 +471,17 @@ SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
-               int precision, uint32_t rerank) {
+               int precision, uint32_t rerank, uint32_t parents) {
   if (nq == 0) return PANN_OK;
   if (precision != PREC_F32 && idx->lp_prec != precision)
     return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
+  if (parents > 0 && precision != PREC_F32 && d_self_ids == nullptr) {
+    PANN_CUDA(idx->counters.ensure(64));
+    SearchArgs a = base_args(idx, plan, d_queries, nullptr, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
+                             nullptr, 0);
+    int rc = enqueue_tile(idx, plan, a, parents, idx->counters.as<uint32_t>() + 10, precision, rerank, st);
+    if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; take the single-parent path
+  }
   TierSizes z;
   int rc = size_tiers(idx, plan, nq, precision, 0, 0, &z);
   if (rc) return rc;
@@ -541,7 +560,7 @@ static int summarize_status(const uint32_t* status, uint32_t nq, uint32_t* out_f
   int rc = PANN_OK;
   for (uint32_t i = 0; i < nq; i++) {
     uint32_t s = status[i];
-    if (out_flags) out_flags[i] = (s & QS_REF_WOULD_GROW) ? 1u : 0u;
+    if (out_flags) out_flags[i] = ((s & QS_REF_WOULD_GROW) ? 1u : 0u) | ((s & 32u) ? 2u : 0u);
     if (s & (QS_TABLE_FULL | QS_INTERNAL)) rc = PANN_EOVERFLOW;
     else if ((s & QS_SHORT) && rc == PANN_OK) rc = PANN_ESHORT;
   }
@@ -846,6 +865,7 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
   if (nq && (!queries || !out_ids)) return fail(PANN_EINVAL, "queries or out_ids is NULL");
   const int prec = opt ? opt->precision : PANN_PREC_F32;
   const uint32_t rerank = opt ? opt->rerank : 0;
+  const uint32_t parents = opt ? opt->parents : 0;
   SearchPlan plan;
   rc = make_plan(idx, qp, n_start, &plan);
   if (rc) return rc;
@@ -882,7 +902,7 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
     d_status = idx->status.as<uint32_t>();
   }
   rc = run_search(idx, plan, q, nullptr, nq, idx->starts.as<uint32_t>(), d_ids, d_dists, d_vis, d_cmps, d_status,
-                  nullptr, 0, st, prec, rerank);
+                  nullptr, 0, st, prec, rerank, parents);
   if (rc || on_device) return rc;
   if (k) {
     PANN_CUDA(cudaMemcpyAsync(out_ids, d_ids, 4 * k * nq, cudaMemcpyDeviceToHost, st));

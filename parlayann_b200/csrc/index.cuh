@@ -17,6 +17,12 @@ int cuda_fail(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return ::pann::cuda_fail(_e, #call); \
   } while (0)
 
+// Largest dynamic shared memory a block may use on the current device. Every
+// kernel gets this as its cudaFuncAttributeMaxDynamicSharedMemorySize, whatever
+// one launch needs, so threads that launch the same kernel with different
+// shared-memory sizes never undo each other's setting.
+int smem_attr_max();
+
 // Device scratch buffer that only grows.
 struct DevBuf {
   void* p = nullptr;
@@ -87,6 +93,6 @@ int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_sta
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
-               int precision = 0, uint32_t rerank = 0);
+               int precision = 0, uint32_t rerank = 0, uint32_t parents = 0);
 
 }  // namespace pann

@@ -239,7 +239,7 @@ __global__ void range_assemble_kernel(uint32_t nq, const unsigned long long* __r
 template <int DT, int MT>
 static cudaError_t launch_expand_t(const RangeArgs& a, int slots, size_t smem, cudaStream_t st) {
   auto k = range_expand_kernel<DT, MT>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return e;
   k<<<slots, 32, smem, st>>>(a);
   return cudaGetLastError();

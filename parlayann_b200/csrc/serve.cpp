@@ -203,24 +203,51 @@ void ranger_main(pann_server* s) {
       s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    Request* r = s->range_q.front();
-    s->range_q.pop_front();
+    // every waiting range request with the same parameters, as one search
+    std::vector<Request*> group;
+    for (auto it = s->range_q.begin(); it != s->range_q.end();) {
+      Request* r = *it;
+      const Request* f = group.empty() ? r : group.front();
+      if (group.empty() || (r->start == f->start && std::memcmp(&r->rp, &f->rp, sizeof(pann_range_params)) == 0)) {
+        group.push_back(r);
+        it = s->range_q.erase(it);
+      } else {
+        ++it;
+      }
+    }
     lk.unlock();
-    std::vector<uint64_t> offs((size_t)r->nq + 1, 0);
-    std::vector<uint32_t> ids((size_t)r->nq * r->rp.beam * 4 + 16);
-    int rc = pann_range_search(s->idx, r->queries.data(), r->nq, &r->rp, r->start, offs.data(), ids.data(), ids.size(),
-                               nullptr, nullptr, nullptr);
-    if (rc == PANN_EOVERFLOW && offs[r->nq] > ids.size()) {
-      ids.resize(offs[r->nq]);
-      rc = pann_range_search(s->idx, r->queries.data(), r->nq, &r->rp, r->start, offs.data(), ids.data(), ids.size(),
-                             nullptr, nullptr, nullptr);
+    uint32_t nq = 0;
+    for (Request* r : group) nq += r->nq;
+    std::vector<uint8_t> qs((size_t)nq * s->row_bytes);
+    {
+      size_t at = 0;
+      for (Request* r : group) {
+        std::memcpy(qs.data() + at, r->queries.data(), r->queries.size());
+        at += r->queries.size();
+      }
+    }
+    const Request* f = group.front();
+    std::vector<uint64_t> offs((size_t)nq + 1, 0);
+    std::vector<uint32_t> ids((size_t)nq * f->rp.beam * 4 + 16);
+    int rc = pann_range_search(s->idx, qs.data(), nq, &f->rp, f->start, offs.data(), ids.data(), ids.size(), nullptr,
+                               nullptr, nullptr);
+    if (rc == PANN_EOVERFLOW && offs[nq] > ids.size()) {
+      ids.resize(offs[nq]);
+      rc = pann_range_search(s->idx, qs.data(), nq, &f->rp, f->start, offs.data(), ids.data(), ids.size(), nullptr,
+                             nullptr, nullptr);
     }
     std::string msg = rc ? pann_last_error() : "";
-    ids.resize(rc == PANN_OK ? offs[r->nq] : 0);
     lk.lock();
-    r->offsets = std::move(offs);
-    r->ids = std::move(ids);
-    finish(s, r, rc, msg);
+    uint32_t q0 = 0;
+    for (Request* r : group) {
+      if (rc == PANN_OK) {
+        r->offsets.resize((size_t)r->nq + 1);
+        for (uint32_t i = 0; i <= r->nq; i++) r->offsets[i] = offs[q0 + i] - offs[q0];
+        r->ids.assign(ids.begin() + (ptrdiff_t)offs[q0], ids.begin() + (ptrdiff_t)offs[q0 + r->nq]);
+      }
+      q0 += r->nq;
+      finish(s, r, rc, msg);
+    }
     s->cv_done.notify_all();
   }
 }
@@ -279,7 +306,7 @@ int pann_server_create(pann_server** out, pann_index* idx, const pann_server_opt
   s->starts.assign(starts, starts + n_start);
   cudaGetDevice(&s->device);
   pann_query_params bounds{opt->max_k, opt->max_beam, opt->limit, opt->degree_limit, opt->batch_factor};
-  pann_search_options so{opt->precision, 0};
+  pann_search_options so{opt->precision, 0, opt->parents};
   pann_batch_options bo{1, 0, 0, 0};
   s->row_bytes = (size_t)idx->d * idx->esize;
   s->slots.resize(opt->inflight);

@@ -57,6 +57,9 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
                int wpb_force, TierSizes* z);
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a, const TierSizes& z,
                   const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank);
+// The multi-parent tile search of the precision form (tile.cu).
+int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
+                 int precision, uint32_t rerank, cudaStream_t st);
 // Validates the start points and copies them to idx->starts (cached).
 int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st);
 // The index's own tier buffers for nq queries (grown as needed).

@@ -1,0 +1,374 @@
+// Multi-parent tile search: the throughput variant of the precision form
+// (pann_search_options::parents > 0).
+//
+// The exact search expands one frontier node per step, as filtered_beam_search
+// does (beamSearch.h:116-222); every step is a chain of dependent memory round
+// trips (adjacency row, then the neighbours' rows) for one warp. This kernel
+// gives each query a CTA and expands the `parents` best unvisited frontier
+// entries per step: their adjacency rows are read together, the new
+// neighbours (an exact shared-memory seen set) form one candidate tile whose
+// low-precision rows are staged into shared memory with cp.async in a single
+// round trip, all 128 threads score the tile (bfloat16, or FP8 E4M3 with
+// per-dimension scales, float32 accumulation), and the survivors are merged
+// into the sorted frontier by rank. The best `rerank` (default 4k) frontier
+// entries are re-scored with the exact float32 distance before the top k are
+// written. The visiting order differs from the reference's (several parents
+// per step), so this is a search of its own with its own recall curve,
+// measured against FP64 brute force; it is not a parity path.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <string>
+
+#include "common.cuh"
+#include "index.cuh"
+#include "lowprec.cuh"
+#include "tiers.cuh"
+
+namespace pann {
+
+enum : uint32_t { QS_TRUNCATED = 32u };  // the seen table filled: the search stopped early
+
+struct TileLayout {
+  size_t q, sc, fr, fr2, cand, cid, table, stage, misc, total;
+  uint32_t sstride;  // staged row stride (bytes)
+};
+
+__host__ __device__ inline TileLayout tile_layout(uint32_t d, uint32_t L, uint32_t CW, uint32_t S,
+                                                  uint64_t lp_stride) {
+  TileLayout t{};
+  size_t o = 0;
+  const size_t dpad = (d + 3) & ~3u;
+  // rows at an odd multiple of 16 bytes apart: conflict-free 16-byte reads
+  t.sstride = (uint32_t)(((lp_stride / 16) % 2 == 0) ? lp_stride + 16 : lp_stride);
+  // every region starts on a 16-byte boundary (cp.async destinations need it)
+#define PANN_TILE_TAKE(field, bytes) \
+  t.field = o;                        \
+  o += ((size_t)(bytes) + 15) & ~(size_t)15;
+  PANN_TILE_TAKE(q, 4 * dpad)
+  PANN_TILE_TAKE(sc, 4 * dpad)
+  PANN_TILE_TAKE(fr, 8ull * L)
+  PANN_TILE_TAKE(fr2, 8ull * L)
+  PANN_TILE_TAKE(cand, 8ull * (CW > L ? CW : L))
+  PANN_TILE_TAKE(cid, 4ull * CW)
+  PANN_TILE_TAKE(table, 4ull * S)
+  PANN_TILE_TAKE(stage, (size_t)CW * t.sstride)
+  PANN_TILE_TAKE(misc, 64)
+#undef PANN_TILE_TAKE
+  t.total = o;
+  return t;
+}
+
+// Exact float32 distance in the reference's order (euclidian_point.h:83-90,
+// mips_point.h:60-66): sequential sum, every product and sum rounded on its own.
+template <int MT>
+__device__ __forceinline__ float exact_f32_dist(const float* __restrict__ row, const float* q, uint32_t d) {
+  float r = 0.0f;
+  for (uint32_t i = 0; i < d; i++) {
+    if (MT == MT_L2) {
+      const float t = __fsub_rn(__ldg(row + i), q[i]);
+      r = __fadd_rn(r, __fmul_rn(t, t));
+    } else {
+      r = __fadd_rn(r, __fmul_rn(__ldg(row + i), q[i]));
+    }
+  }
+  return MT == MT_L2 ? r : -r;
+}
+
+// Approximate distance of one staged low-precision row (16-byte reads).
+template <int MT, int PREC>
+__device__ __forceinline__ float tile_row_dist(const uint8_t* row, const float* q, const float* sc, uint32_t d,
+                                               uint32_t chunks) {
+  float a0 = 0.f, a1 = 0.f;
+  constexpr uint32_t VPC = PREC == PREC_BF16 ? 8 : 16;
+  for (uint32_t c = 0; c < chunks; c++) {
+    const uint4 v = reinterpret_cast<const uint4*>(row)[c];
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+      for (int h = 0; h < (PREC == PREC_BF16 ? 1 : 2); h++) {
+        const uint32_t e = c * VPC + j * (VPC / 4) + 2 * h;
+        if (e >= d) break;
+        float2 x;
+        if (PREC == PREC_BF16) {
+          x = bf16x2_to_f2(w[j]);
+        } else {
+          x = e4m3x2_to_f2(w[j] >> (16 * h));
+          x.x *= sc[e];
+          x.y *= sc[e + 1];
+        }
+        if (MT == MT_L2) {
+          const float t0 = x.x - q[e], t1 = x.y - q[e + 1];
+          a0 = fmaf(t0, t0, a0);
+          a1 = fmaf(t1, t1, a1);
+        } else {
+          a0 = fmaf(x.x, q[e], a0);
+          a1 = fmaf(x.y, q[e + 1], a1);
+        }
+      }
+    }
+  }
+  return MT == MT_L2 ? a0 + a1 : -(a0 + a1);
+}
+
+// Seen-set slots of a query with beam L: (L + 16) * nel * 1.35 rounded up to
+// a multiple of 32, within [4 (R + 1), 16384] (not a power of two: slots are
+// chosen by multiplicative range reduction); a query stops early (flagged) when
+// its set reaches 15/16 of that. Per query, so a batch answers each query as a
+// search with that query's beam alone would.
+__host__ __device__ inline uint32_t tile_seen_slots(uint32_t L, uint32_t nel, uint32_t R) {
+  uint64_t s = ((uint64_t)(L + 16) * nel * 135 / 100 + 31) & ~31ull;
+  const uint64_t lo = 4ull * (R + 1);
+  if (s < lo) s = (lo + 31) & ~31ull;
+  if (s > 16384) s = 16384;
+  return (uint32_t)s;
+}
+
+// Home slot in [0, S) of an id (Fibonacci hashing, then range reduction).
+__device__ __forceinline__ uint32_t tile_slot(uint32_t id, uint32_t S) { return __umulhi(id * 0x9E3779B1u, S); }
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem_src) : "memory");
+}
+
+template <int MT, int PREC>
+__global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t W, uint32_t S, uint32_t CW) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const TileLayout ly = tile_layout(a.d, a.L, CW, S, a.lp_stride);
+  float* qf = reinterpret_cast<float*>(smem + ly.q);
+  float* sc = reinterpret_cast<float*>(smem + ly.sc);
+  uint64_t* frA = reinterpret_cast<uint64_t*>(smem + ly.fr);
+  uint64_t* frB = reinterpret_cast<uint64_t*>(smem + ly.fr2);
+  uint64_t* cand = reinterpret_cast<uint64_t*>(smem + ly.cand);
+  uint32_t* cid = reinterpret_cast<uint32_t*>(smem + ly.cid);
+  uint32_t* table = reinterpret_cast<uint32_t*>(smem + ly.table);
+  uint8_t* stage = smem + ly.stage;
+  uint32_t* misc = reinterpret_cast<uint32_t*>(smem + ly.misc);
+  // misc: [0] job  [1] new ids  [2] kept candidates  [3] parents  [4] table entries  [5..8] parent ids
+  //       [9] truncated
+  uint32_t* par = misc + 5;
+  const uint32_t nel = a.dl < a.R ? a.dl : a.R;
+  if (PREC == PREC_FP8)
+    for (uint32_t i = tid; i < a.d; i += blockDim.x) sc[i] = a.lp_scales[i];
+  const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) misc[0] = atomicAdd(a.job_counter, 1u);
+    __syncthreads();
+    const uint32_t job = misc[0];
+    if (job >= njobs) break;
+    const uint32_t qi = a.job_list ? a.job_list[job] : job;
+    const uint32_t L = a.qL ? a.qL[qi] : a.L;
+    const uint32_t kq = a.qk ? a.qk[qi] : a.k;
+    const uint32_t Sq = a.qL ? tile_seen_slots(L, nel, a.R) : S;  // <= S
+    const uint32_t fill_limit = Sq - Sq / 16;
+    const float* qsrc = reinterpret_cast<const float*>(a.queries + (uint64_t)qi * a.stride);
+    for (uint32_t i = tid; i < a.d; i += blockDim.x) qf[i] = qsrc[i];
+    for (uint32_t i = tid; i < Sq; i += blockDim.x) table[i] = PANN_PAD;
+    if (tid < 15) misc[1 + tid] = 0;
+    __syncthreads();
+    // start points: approximate distances from global rows, all in the seen set
+    for (uint32_t s = tid; s < a.n_start; s += blockDim.x) {
+      const uint32_t id = a.starts[s];
+      const float dd = tile_row_dist<MT, PREC>(a.lp_rows + (uint64_t)id * a.lp_stride, qf, sc, a.d, a.lp_chunks);
+      cand[s] = make_key(dd, id);
+      uint32_t h = tile_slot(id, Sq);
+      for (uint32_t p = 0; p < Sq; p++) {
+        const uint32_t old = atomicCAS(table + h, PANN_PAD, id);
+        if (old == PANN_PAD || old == id) break;
+        h = h + 1 == Sq ? 0 : h + 1;
+      }
+    }
+    __syncthreads();
+    for (uint32_t s = tid; s < a.n_start; s += blockDim.x) {
+      uint32_t r = 0;
+      for (uint32_t j = 0; j < a.n_start; j++) r += cand[j] < cand[s];
+      frA[r] = cand[s];
+    }
+    if (tid == 0) misc[4] = a.n_start;
+    uint64_t* fr = frA;
+    uint64_t* fr2 = frB;
+    uint32_t fn = a.n_start;
+    uint64_t nvis = 0;
+    uint32_t cmps = a.n_start;
+    __syncthreads();
+
+    for (;;) {
+      // ---- the best `parents` unvisited frontier entries (warp 0)
+      const uint64_t room = a.limit > nvis ? a.limit - nvis : 0;
+      const uint32_t wlim = (uint32_t)(room < W ? room : W);
+      if (warp == 0) {
+        uint32_t np = 0;
+        for (uint32_t b = 0; b < fn && np < wlim; b += 32) {
+          const uint32_t i = b + lane;
+          unsigned m = __ballot_sync(FULL, i < fn && !(fr[i] & PANN_VFLAG));
+          while (m && np < wlim) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            if (lane == 0) {
+              par[np] = key_id(fr[b + j]);
+              fr[b + j] |= PANN_VFLAG;
+            }
+            np++;
+          }
+        }
+        if (lane == 0) {
+          misc[3] = misc[9] ? 0u : np;
+          misc[1] = 0;
+          misc[2] = 0;
+        }
+      }
+      __syncthreads();
+      const uint32_t np = misc[3];
+      if (np == 0) break;
+      nvis += np;
+      // ---- adjacency rows of the parents; new neighbours into the tile
+      for (uint32_t x = tid; x < np * nel; x += blockDim.x) {
+        const uint32_t p = x / nel, j = x - p * nel;
+        const uint32_t id = a.graph[(uint64_t)par[p] * a.R + j];
+        if (id == PANN_PAD) continue;
+        uint32_t h = tile_slot(id, Sq);
+        for (uint32_t probe = 0; probe < Sq; probe++) {
+          const uint32_t old = atomicCAS(table + h, PANN_PAD, id);
+          if (old == id) break;
+          if (old == PANN_PAD) {
+            const uint32_t e = atomicAdd(misc + 4, 1u);
+            if (e >= fill_limit) misc[9] = 1;  // stop after this step: the table is nearly full
+            cid[atomicAdd(misc + 1, 1u)] = id;
+            break;
+          }
+          h = h + 1 == Sq ? 0 : h + 1;
+        }
+      }
+      __syncthreads();
+      const uint32_t ncand = misc[1];
+      // ---- stage the tile's rows (one round trip)
+      for (uint32_t x = tid; x < ncand * a.lp_chunks; x += blockDim.x) {
+        const uint32_t r = x / a.lp_chunks, c = x - r * a.lp_chunks;
+        cp_async16(stage + (size_t)r * ly.sstride + 16 * c, a.lp_rows + (uint64_t)cid[r] * a.lp_stride + 16 * c);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncthreads();
+      // ---- score; keep those below the cutoff of a full frontier (beamSearch.h:173-182)
+      const float cutoff = fn == L ? key_dist(fr[L - 1]) : 3.40282346638528859812e+38F;
+      for (uint32_t r = tid; r < ncand; r += blockDim.x) {
+        const float dd = tile_row_dist<MT, PREC>(stage + (size_t)r * ly.sstride, qf, sc, a.d, a.lp_chunks);
+        if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[r]);
+      }
+      cmps += ncand;
+      __syncthreads();
+      const uint32_t nc = misc[2];
+      if (nc > 0) {
+        // ---- merge by rank: keys are distinct (ids are), visited flags ignored in the order
+        for (uint32_t i = tid; i < fn; i += blockDim.x) {
+          const uint64_t key = fr[i], mk = key & PANN_KEYMASK;
+          uint32_t r = i;
+          for (uint32_t j = 0; j < nc; j++) r += cand[j] < mk;
+          if (r < L) fr2[r] = key;
+        }
+        for (uint32_t j = tid; j < nc; j += blockDim.x) {
+          const uint64_t ck = cand[j];
+          uint32_t lo = 0, hi = fn;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if ((fr[mid] & PANN_KEYMASK) < ck) lo = mid + 1; else hi = mid;
+          }
+          uint32_t r = lo;
+          for (uint32_t t = 0; t < nc; t++) r += cand[t] < ck;
+          if (r < L) fr2[r] = ck;
+        }
+        fn = fn + nc < L ? fn + nc : L;
+        uint64_t* t = fr; fr = fr2; fr2 = t;
+      }
+      __syncthreads();
+    }
+
+    // ---- exact float32 re-rank of the best entries, then the top k
+    const uint32_t rr = a.rerank ? a.rerank : 4 * kq;
+    const uint32_t nr = fn < (rr > kq ? rr : kq) ? fn : (rr > kq ? rr : kq);
+    for (uint32_t i = tid; i < nr; i += blockDim.x) {
+      const uint32_t id = key_id(fr[i]);
+      const float dd = exact_f32_dist<MT>(reinterpret_cast<const float*>(a.points + (uint64_t)id * a.stride), qf, a.d);
+      cand[i] = make_key(dd, id);
+    }
+    __syncthreads();
+    uint32_t* const oid = a.out_ids + (uint64_t)qi * a.kstride;
+    float* const odist = a.out_dists ? a.out_dists + (uint64_t)qi * a.kstride : nullptr;
+    for (uint32_t i = tid; i < nr; i += blockDim.x) {
+      const uint64_t key = cand[i];
+      uint32_t r = 0;
+      for (uint32_t j = 0; j < nr; j++) r += cand[j] < key;
+      if (r < kq) {
+        oid[r] = key_id(key);
+        if (odist) odist[r] = key_dist(key);
+      }
+    }
+    for (uint32_t j = (nr < kq ? nr : kq) + tid; j < a.kstride; j += blockDim.x) {
+      oid[j] = PANN_PAD;
+      if (odist) odist[j] = 0.0f;
+    }
+    if (tid == 0) {
+      uint32_t status = 0;
+      if (fn < kq) status |= QS_SHORT;
+      if (misc[9]) status |= QS_TRUNCATED;
+      if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;
+      if (a.out_cmps) a.out_cmps[qi] = cmps;
+      if (a.out_status) a.out_status[qi] = status;
+    }
+  }
+}
+
+template <int MT, int PREC>
+static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W, uint32_t S, uint32_t CW,
+                         size_t smem, cudaStream_t st) {
+  auto k = search_tile_kernel<MT, PREC>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
+  if (e != cudaSuccess) return cuda_fail(e, "tile kernel attribute");
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem);
+  if (e != cudaSuccess || occ <= 0) occ = 1;
+  const uint64_t want = a.nq;
+  const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count));
+  k<<<blocks, 128, smem, st>>>(a, W, S, CW);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "tile kernel launch");
+  return PANN_OK;
+}
+
+// Sizes and launches the tile kernel; returns PANN_EINVAL (and does nothing)
+// when its state does not fit in shared memory, so the caller can take the
+// single-parent path.
+int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
+                 int precision, uint32_t rerank, cudaStream_t st) {
+  const uint32_t nel = std::min(plan.dl, idx->R);
+  uint32_t W = std::max<uint32_t>(1, std::min<uint32_t>(parents, 4));
+  const uint32_t S = tile_seen_slots(plan.L, nel, idx->R);
+  TileLayout ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride);
+  while (ly.total > idx->smem_optin && W > 1) {
+    W--;
+    ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride);
+  }
+  if (ly.total > idx->smem_optin) return fail(PANN_EINVAL, "tile search state does not fit in shared memory");
+  a.lp_rows = idx->lp_rows.as<uint8_t>();
+  a.lp_stride = idx->lp_stride;
+  a.lp_chunks = idx->lp_chunks;
+  a.lp_scales = idx->lp_scales.as<float>();
+  a.rerank = rerank;
+  a.job_counter = job_counter;
+  PANN_CUDA(cudaMemsetAsync(job_counter, 0, 4, st));
+  const int mt = idx->metric;
+  if (mt == MT_L2 && precision == PREC_BF16) return launch_tile_t<MT_L2, PREC_BF16>(idx, a, W, S, W * nel, ly.total, st);
+  if (mt == MT_IP && precision == PREC_BF16) return launch_tile_t<MT_IP, PREC_BF16>(idx, a, W, S, W * nel, ly.total, st);
+  if (mt == MT_L2 && precision == PREC_FP8) return launch_tile_t<MT_L2, PREC_FP8>(idx, a, W, S, W * nel, ly.total, st);
+  if (mt == MT_IP && precision == PREC_FP8) return launch_tile_t<MT_IP, PREC_FP8>(idx, a, W, S, W * nel, ly.total, st);
+  return fail(PANN_EINVAL, "the tile search needs a bfloat16 or FP8 precision");
+}
+
+}  // namespace pann

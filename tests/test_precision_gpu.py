@@ -57,3 +57,45 @@ def test_precision_requires_float_points(lib_built):
     with pytest.raises(P.PannError):
         idx.set_precision(P.PREC_BF16)
     idx.close()
+
+
+@pytest.mark.parametrize("metric", [P.L2, P.MIPS], ids=["l2", "mips"])
+@pytest.mark.parametrize("prec", [P.PREC_BF16, P.PREC_FP8], ids=["bf16", "fp8"])
+@pytest.mark.parametrize("parents", [1, 2, 4])
+def test_tile_search_recall_and_exact_rerank(mix_index, metric, prec, parents):
+    """The multi-parent tile search (one CTA per query, `parents` nodes
+    expanded per step): recall against FP64 brute force within the same
+    bound as the single-parent precision form, exact float32 distances in the
+    answer, deterministic, and the batched form gives the same answers."""
+    base, q, out = mix_index
+    idx, gt = out[metric]
+    exact = idx.search(q, 10, 40)
+    idx.set_precision(prec)
+    r = idx.search(q, 10, 40, precision=prec, parents=parents)
+    r2 = idx.search(q, 10, 40, precision=prec, parents=parents)
+    np.testing.assert_array_equal(r.ids, r2.ids)
+    rec_exact = P.recall_at_k(exact.ids, gt, 10)
+    rec = P.recall_at_k(r.ids, gt, 10)
+    # a different visiting order (several parents a step, no deferral): a looser bound
+    assert rec >= rec_exact - RECALL_LOSS[prec] - 0.03, (rec, rec_exact)
+    assert (r.visited > 0).all() and (r.cmps > 0).all()
+    for i in range(0, q.shape[0], 25):
+        assert len(set(r.ids[i].tolist())) == 10
+        for j in range(10):
+            v = int(r.ids[i, j])
+            dd = O.olib().oracle_distance(2, metric, 96, base[v].ctypes.data, q[i].ctypes.data)
+            assert r.dists[i, j] == np.float32(dd)
+        assert np.all(np.diff(r.dists[i]) >= 0)
+    # batched with per-query k and beam: each query as its own plain tile search
+    rng = np.random.default_rng(9)
+    ks = rng.choice(np.array([1, 10], np.uint32), len(q)).astype(np.uint32)
+    Ls = np.array([rng.integers(max(10, kk), 4 * max(10, kk) + 1) for kk in ks], np.uint32)
+    b = idx.batch(len(q), 10, int(Ls.max()), precision=prec, parents=parents)
+    rb = b.run(q, ks, Ls)
+    for kk, LL in sorted(set(zip(ks.tolist(), Ls.tolist()))):
+        sel = np.where((ks == kk) & (Ls == LL))[0]
+        p = idx.search(q[sel], kk, LL, precision=prec, parents=parents)
+        np.testing.assert_array_equal(rb.ids[sel, :kk], p.ids)
+        np.testing.assert_array_equal(rb.visited[sel], p.visited)
+    b.close()
+    idx.set_precision(P.PREC_F32)
