@@ -100,6 +100,17 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
 // re-inserted in old-slot order (num_entries counts each re-insertion), then
 // the key that triggered the growth continues from its old-mask slot
 // (:39-47). Returns false if the grown table does not fit this tier.
+//
+// The re-insertion is computed cluster by cluster. With linear probing the
+// set of occupied slots does not depend on the insertion order; only which
+// key sits where inside a cluster (a maximal run of occupied slots) does, and
+// a key only ever lands in the cluster that holds its home. So: (A) the keys'
+// ranks in old-slot order are placed in any order (lanes take ranks far apart,
+// so they seldom share slots), which fixes the clusters; (B) the lane whose
+// key starts a cluster replays that cluster's keys in rank order, each at the
+// first free slot from its home. A key that is in the old table twice (the
+// hashset can hold one) and a cluster longer than 64 send the re-insertion
+// to a plain sequential pass instead.
 __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool* a_seen) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t size = 1u << h.bits, nsize = size * 2;
@@ -109,9 +120,8 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
   for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
   __syncwarp();
   const uint32_t oldmask = size - 1, nmask = nsize - 1;
-  // re-insert in old-slot order: first compact the old table's keys to its
-  // front (order kept; writes never pass the chunk being read), then insert
-  // them 32 at a time with the ordered rounds
+  // the old table's keys compacted to its front in slot order (writes never
+  // pass the chunk being read): keys[r] is the key of rank r
   uint32_t cnt = 0;
   for (uint32_t base = 0; base < size; base += 32) {
     uint32_t k = h.cur[base + lane];
@@ -122,13 +132,120 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
     cnt += __popc(m);
     __syncwarp();
   }
-  for (uint32_t b = 0; b < cnt; b += 32) {
-    const bool v = b + lane < cnt;
-    const uint32_t k = v ? h.cur[b + lane] : PANN_PAD;
-    bool ins;
-    uint32_t pos;
-    emu_probe_rounds(other, nmask, k, v, ref_slot(k, nmask), lane, &ins, &pos);
+  uint32_t* keys = h.cur;
+  // (A) ranks into the new table, lane l taking rank l * nb + b in batch b
+  const uint32_t nb = (cnt + 31) / 32;
+  bool dup = false;
+  for (uint32_t b = 0; b < nb; b++) {
+    const uint32_t r = (uint32_t)lane * nb + b;
+    bool done = r >= cnt;
+    const uint32_t k = done ? PANN_PAD : keys[r];
+    uint32_t p = ref_slot(k, nmask);
+    for (;;) {
+      if (!done) {
+        uint32_t w = other[p];
+        while (w != PANN_PAD && keys[w] != k) { p = (p + 1) & nmask; w = other[p]; }
+        if (w != PANN_PAD) { done = true; dup = true; }
+      }
+      const unsigned want = __ballot_sync(FULL, !done);
+      if (!want) break;
+      const unsigned grp = __match_any_sync(FULL, done ? (0x80000000u | (uint32_t)lane) : p);
+      if (!done && (__ffs(grp & want) - 1) == lane) {
+        other[p] = r;
+        done = true;
+      }
+      __syncwarp();
+    }
   }
+  bool fallback = __any_sync(FULL, dup);
+  // (B) owners: keys that start a cluster, one bit per rank in the old table's
+  // free tail; then each owner replays its cluster (up to 8 keys in registers,
+  // up to 64 through a per-lane scratch row also in the free tail)
+  const uint32_t words = nb;
+  uint32_t* owner = keys + ((cnt + 3) & ~3u);
+  uint32_t* scratch = owner + ((words + 3) & ~3u);
+  const bool scratch_ok = (size_t)(scratch - keys) + 32ull * 64 <= size;
+  if (!fallback) {
+    for (uint32_t b = 0; b < nb; b++) {
+      const uint32_t r = b * 32 + lane;
+      bool own = false;
+      if (r < cnt) {
+        uint32_t p = ref_slot(keys[r], nmask);
+        while (other[p] != r) p = (p + 1) & nmask;
+        own = other[(p - 1) & nmask] == PANN_PAD;
+      }
+      const unsigned om = __ballot_sync(FULL, own);
+      if (lane == 0) owner[b] = om;
+    }
+    __syncwarp();
+    bool long_run = false;
+    for (uint32_t b = 0; b < nb; b++) {
+      const uint32_t r = b * 32 + lane;
+      if (r < cnt && ((owner[b] >> lane) & 1u)) {
+        uint32_t s0 = ref_slot(keys[r], nmask);
+        while (other[s0] != r) s0 = (s0 + 1) & nmask;
+        uint32_t m = 1;
+        while (m <= 64 && other[(s0 + m) & nmask] != PANN_PAD) m++;
+        if (m == 1) {
+          other[s0] = keys[r];
+        } else if (m <= 8) {
+          uint32_t ix[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) ix[j] = (uint32_t)j < m ? other[(s0 + j) & nmask] : 0xFFFFFFFFu;
+          uint32_t taken = 0, used = 0;
+          for (uint32_t t = 0; t < m; t++) {
+            uint32_t best = 0xFFFFFFFFu, bj = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+              if (!((used >> j) & 1u) && ix[j] < best) { best = ix[j]; bj = (uint32_t)j; }
+            used |= 1u << bj;
+            const uint32_t key = keys[best];
+            const uint32_t o = (ref_slot(key, nmask) - s0) & nmask;  // inside the cluster
+            const uint32_t pos = (uint32_t)(__ffs(~taken & (~0u << o)) - 1);
+            taken |= 1u << pos;
+            other[(s0 + pos) & nmask] = key;
+          }
+        } else if (m <= 64 && scratch_ok) {
+          uint32_t* row = scratch + (size_t)lane * 64;
+          uint64_t taken = 0;
+          uint32_t last = 0xFFFFFFFFu;  // no rank taken yet
+          for (uint32_t t = 0; t < m; t++) {
+            uint32_t best = 0xFFFFFFFFu;
+            for (uint32_t j = 0; j < m; j++) {
+              const uint32_t w = other[(s0 + j) & nmask];
+              if ((last == 0xFFFFFFFFu || w > last) && w < best) best = w;
+            }
+            last = best;
+            const uint32_t key = keys[best];
+            const uint32_t o = (ref_slot(key, nmask) - s0) & nmask;
+            const uint32_t pos = (uint32_t)(__ffsll((long long)(~taken & (~0ull << o))) - 1);
+            taken |= 1ull << pos;
+            row[pos] = key;
+          }
+          for (uint32_t j = 0; j < m; j++) other[(s0 + j) & nmask] = row[j];
+        } else {
+          long_run = true;
+        }
+      }
+      __syncwarp();
+    }
+    fallback = __any_sync(FULL, long_run);
+  }
+  if (fallback) {
+    // the plain sequential re-insertion
+    for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
+    __syncwarp();
+    if (lane == 0) {
+      for (uint32_t i = 0; i < cnt; i++) {
+        const uint32_t k = keys[i];
+        uint32_t p = ref_slot(k, nmask);
+        while (other[p] != PANN_PAD && other[p] != k) p = (p + 1) & nmask;
+        other[p] = k;
+      }
+    }
+    __syncwarp();
+  }
+  __threadfence_block();
   const long long added = cnt;
   h.num_entries += added;
   uint32_t* t = h.cur; h.cur = h.other; h.other = t;
