@@ -375,11 +375,12 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         rel = np.abs(dists[:1000].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
         return float(rel.max()), float(rel.mean())
 
+    want = set(args.forms.split(","))
     # ---- precision form (+ batched): smallest beam with recall >= 0.95, device QPS through a batch object
     prec_out = {}
     exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, gd, k)
-    for name, prec, parents in (("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
-                                ("fp8_tile2", P.PREC_FP8, 2)):
+    for name, prec, parents in ((("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
+                                 ("fp8_tile2", P.PREC_FP8, 2)) if "precision" in want or "serving" in want else ()):
         idx.set_precision(prec)
         pbeam, prec_rec, pres = None, None, None
         for L in BEAMS:
@@ -419,9 +420,44 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
                           "reported_distance_rel_error_vs_fp64": {"max": mx, "mean": mean}}
         b.close()
     idx.set_precision(P.PREC_F32)
-    out["precision_batched"] = prec_out
+    if prec_out:
+        out["precision_batched"] = prec_out
+    if "batched" in want:
+        out["batched_uneven"] = run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib)
+    radius = range_radius(base, q)
+    if "range" in want:
+        nr = 200
+        t0 = time.perf_counter()
+        rr = idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)
+        t_r = time.perf_counter() - t0
+        sizes = np.array([len(x) for x in rr["ids"]])
+        out["range"] = {"queries": nr, "beam": 20, "type": "greedy", "radius_quantile": 0.01, "radius": radius,
+                        "qps_e2e": round(nr / t_r, 1), "mean_answer": float(sizes.mean()),
+                        "answer_ids_per_s": round(float(sizes.sum()) / t_r, 1)}
+    if "serving" in want:
+        out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
+    return out
 
-    # ---- batched form with uneven shapes: k in {1,10,100}, beam uniform in [k, 4k] (beam >= 10 for k = 1)
+
+def range_radius(base, q):
+    """The 1%-quantile of sampled base-query distances (squared L2)."""
+    samp = []
+    rs = np.random.default_rng(6)
+    for i in rs.choice(q.shape[0], 16, replace=False):
+        cols = rs.choice(base.shape[0], 4000, replace=False)
+        samp.append(((base[cols] - q[i]) ** 2).sum(1))
+    return float(np.quantile(np.concatenate(samp), 0.01))
+
+
+def run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib):
+    """Per-query k in {1,10,100} and beam in [k, 4k] through one batch object
+    (graph replay), against the plain form run per (k, beam) group."""
+    import torch
+
+    import parlayann_b200 as P
+
+    nq = q.shape[0]
+    starts = np.zeros(1, np.uint32)
     rng = np.random.default_rng(5)
     ks = rng.choice(np.array([1, 10, 100], np.uint32), nq).astype(np.uint32)
     Ls = np.array([rng.integers(max(kk, 1), 4 * kk + 1) for kk in ks], np.uint32)
@@ -460,29 +496,16 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     t_p = _timed(step_plain_groups, flush, stream, steps, 3)
     exact = all(np.array_equal(ids_u[np.array(v), :key[0]], gout[key].cpu().numpy().astype(np.uint32))
                 for key, v in groups.items())
-    out["batched_uneven"] = {"queries": nq, "k": "uniform in {1,10,100}", "beam": "uniform in [k, 4k]",
-                             "qps_batched_graph": round(nq / t_b, 1), "qps_plain_per_shape": round(nq / t_p, 1),
-                             "shape_groups": len(groups), "speedup": round(t_p / t_b, 3),
-                             "bit_exact_with_plain": bool(exact)}
+    return {"queries": nq, "k": "uniform in {1,10,100}", "beam": "uniform in [k, 4k]",
+            "qps_batched_graph": round(nq / t_b, 1), "qps_plain_per_shape": round(nq / t_p, 1),
+            "shape_groups": len(groups), "speedup": round(t_p / t_b, 3), "bit_exact_with_plain": bool(exact)}
 
-    # ---- range search: radius = the 1%-quantile of sampled base-query distances
-    samp = []
-    rs = np.random.default_rng(6)
-    for i in rs.choice(nq, 16, replace=False):
-        cols = rs.choice(W["n"], 4000, replace=False)
-        samp.append(((base[cols] - q[i]) ** 2).sum(1))
-    radius = float(np.quantile(np.concatenate(samp), 0.01))
-    nr = 200
-    t0 = time.perf_counter()
-    rr = idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)
-    t_r = time.perf_counter() - t0
-    sizes = np.array([len(x) for x in rr["ids"]])
-    out["range"] = {"queries": nr, "beam": 20, "type": "greedy", "radius_quantile": 0.01, "radius": radius,
-                    "qps_e2e": round(nr / t_r, 1), "mean_answer": float(sizes.mean()),
-                    "answer_ids_per_s": round(float(sizes.sum()) / t_r, 1)}
 
-    # ---- serving form: open-loop Poisson arrivals at 5 offered rates, for the
-    # plain form and for the fastest precision form found above
+def run_serving(idx, q, nq, beam, radius, prec_out):
+    """Open-loop Poisson arrivals at 5 offered rates, for the plain form and
+    for the fastest precision form found above."""
+    import parlayann_b200 as P
+
     rng = np.random.default_rng(7)
     rp = P.RangeParams(20, P.RANGE_GREEDY, radius, 0.0, 0)
     forms = [("plain", P.PREC_F32, 0, beam)]
@@ -529,10 +552,9 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         serving[fname] = {"precision": int(prec), "parents": parents, "beam_k10": kbeam,
                           "capacity_qps_closed": round(cap_qps, 1), "rates": rates}
     idx.set_precision(P.PREC_F32)
-    out["serving"] = {"requests": "1-256 queries, k in {10,100} (beam for recall@10 >= 0.95 / 200), 1% range "
-                                  "requests (1 query, beam 20, greedy, radius at the 1% distance quantile)",
-                      "slots": 3, "batch_queries": 4096, "forms": serving}
-    return out
+    return {"requests": "1-256 queries, k in {10,100} (beam for recall@10 >= 0.95 / 200), 1% range "
+                        "requests (1 query, beam 20, greedy, radius at the 1% distance quantile)",
+            "slots": 3, "batch_queries": 4096, "forms": serving}
 
 
 def cpu_baseline(base, q, graph, beam, args):
@@ -619,6 +641,8 @@ def main():
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / batched / range / serving forms")
+    ap.add_argument("--forms", default="precision,batched,range,serving",
+                    help="comma list of the forms to run (precision, batched, range, serving)")
     ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
     ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
     args = ap.parse_args()

@@ -12,6 +12,8 @@
 //   stats<indexType>                  algorithms/utils/stats.h:120-155
 //   groundTruth<T>                    algorithms/utils/types.h:38-107
 //   beam_search, searchAll, qsearchAll algorithms/utils/beamSearch.h:420-646
+//   RangeSearch, DoubleBeamRangeSearch algorithms/utils/rangeSearch.h:183-276,
+//                                     algorithms/utils/doublingSearch.h:50-157
 //   knn_index<PR,QPR,indexType>::build_index   algorithms/vamana/index.h:42-186
 //
 // Points and graphs live on the host as in the reference; the first search or
@@ -21,6 +23,7 @@
 #pragma once
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -46,6 +49,8 @@ inline void pann_check(int rc, const char* where) {
 }
 
 // ---------------------------------------------------------------- params
+enum rangeQueryType { None, Greedy, Doubling, Beam };  // types.h:153
+
 struct QueryParams {
   long k;
   long beamSize;
@@ -53,8 +58,18 @@ struct QueryParams {
   long degree_limit;
   double rerank_factor = 100;
   double batch_factor = .125;
+  bool is_early_stop = false;
+  double early_stopping_radius = 0;
+  double early_stopping_count = 0;
+  rangeQueryType range_query_type = None;
+  double radius = 0;
   QueryParams(long k, long Q, long limit, long dg, double rerank_factor = 100, double batch_factor = .125)
       : k(k), beamSize(Q), limit(limit), degree_limit(dg), rerank_factor(rerank_factor), batch_factor(batch_factor) {}
+  // range search (types.h:254-259)
+  QueryParams(long k, long Q, long limit, long dg, long es, double esr, long esc, rangeQueryType range_query_type,
+              double radius)
+      : k(k), beamSize(Q), limit(limit), degree_limit(dg), is_early_stop(es), early_stopping_radius(esr),
+        early_stopping_count((double)esc), range_query_type(range_query_type), radius(radius) {}
   QueryParams() : k(0), beamSize(0), limit(0), degree_limit(0) {}
   pann_query_params c() const {
     pann_query_params q;
@@ -493,6 +508,86 @@ std::vector<std::vector<indexType>> qsearchAll(const PR& Query_Points, const QPR
   (void)QQ_Query_Points;
   return pann_batch(Query_Points, G, Base_Points, QueryStats, std::vector<indexType>{starting_point}, QP,
                     "qsearchAll");
+}
+
+// ---------------------------------------------------------------- range search
+// One pann_range_search over the given query rows; answers in the reference's
+// order, QueryStats incremented as the reference does.
+template <typename PointRange_, typename indexType>
+std::vector<std::vector<indexType>> pann_range_batch(const PointRange_& Query_Points, const std::vector<long>& rows,
+                                                     const Graph<indexType>& G, const PointRange_& Base_Points,
+                                                     stats<indexType>& QueryStats, indexType start,
+                                                     const QueryParams& QP, int type) {
+  pann_index* idx = G.device(Base_Points);
+  using T = typename PointRange_::T;
+  const size_t nq = rows.size(), d = (size_t)Query_Points.dimension();
+  std::vector<T> q(nq * d);
+  for (size_t i = 0; i < nq; i++) std::memcpy(&q[i * d], Query_Points.data() + (size_t)rows[i] * d, sizeof(T) * d);
+  pann_range_params rp;
+  rp.beam = (uint32_t)QP.beamSize;
+  rp.type = type;
+  rp.radius = QP.radius;
+  rp.early_stopping_radius = QP.early_stopping_radius;
+  rp.early_stopping_count = (uint32_t)QP.early_stopping_count;
+  std::vector<uint64_t> offs(nq + 1);
+  std::vector<uint32_t> vis(nq), cmps(nq), ids(nq * (size_t)QP.beamSize + 16);
+  int rc = pann_range_search(idx, q.data(), (uint32_t)nq, &rp, (uint32_t)start, offs.data(), ids.data(), ids.size(),
+                             vis.data(), cmps.data(), nullptr);
+  if (rc == PANN_EOVERFLOW && offs[nq] > ids.size()) {
+    ids.resize(offs[nq]);
+    rc = pann_range_search(idx, q.data(), (uint32_t)nq, &rp, (uint32_t)start, offs.data(), ids.data(), ids.size(),
+                           vis.data(), cmps.data(), nullptr);
+  }
+  pann_check(rc, "range search");
+  std::vector<std::vector<indexType>> out(nq);
+  for (size_t i = 0; i < nq; i++) {
+    out[i].assign(ids.begin() + (long)offs[i], ids.begin() + (long)offs[i + 1]);
+    if (QueryStats.visited.size() > i) {
+      QueryStats.increment_visited((indexType)i, vis[i]);
+      QueryStats.increment_dist((indexType)i, cmps[i]);
+    }
+  }
+  return out;
+}
+
+// RangeSearch (rangeSearch.h:183-276) on unquantized points; the second
+// element is (seconds, 0), the reference's (beam, other) time split.
+template <typename Point, typename PointRange_, typename QPointRange, typename indexType>
+std::pair<std::vector<std::vector<indexType>>, std::pair<double, double>>
+RangeSearch(Graph<indexType>& G, PointRange_& Query_Points, PointRange_& Base_Points, QPointRange& Q_Query_Points,
+            QPointRange& Q_Base_Points, stats<indexType>& QueryStats, indexType starting_point, QueryParams& QP) {
+  if ((const void*)&Q_Base_Points != (const void*)&Base_Points) {
+    std::cout << "ERROR: RangeSearch supports unquantized points" << std::endl;
+    std::abort();
+  }
+  (void)Q_Query_Points;
+  std::vector<long> rows(Query_Points.size());
+  for (size_t i = 0; i < rows.size(); i++) rows[i] = (long)i;
+  const int type = QP.range_query_type == Beam ? PANN_RANGE_BEAM : PANN_RANGE_GREEDY;
+  auto t0 = std::chrono::steady_clock::now();
+  auto out = pann_range_batch(Query_Points, rows, G, Base_Points, QueryStats, starting_point, QP, type);
+  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return {out, {secs, 0.0}};
+}
+
+// DoubleBeamRangeSearch (doublingSearch.h:50-157) over active_indices.
+template <typename PointRange_, typename QPointRange, typename indexType>
+std::pair<std::vector<std::vector<indexType>>, std::pair<double, double>>
+DoubleBeamRangeSearch(Graph<indexType>& G, PointRange_& Query_Points, PointRange_& Base_Points,
+                      QPointRange& Q_Query_Points, QPointRange& Q_Base_Points, stats<indexType>& QueryStats,
+                      std::vector<indexType> starting_points, QueryParams& QP,
+                      std::vector<indexType> active_indices) {
+  if ((const void*)&Q_Base_Points != (const void*)&Base_Points || starting_points.size() != 1) {
+    std::cout << "ERROR: DoubleBeamRangeSearch supports unquantized points and one start point" << std::endl;
+    std::abort();
+  }
+  (void)Q_Query_Points;
+  std::vector<long> rows(active_indices.begin(), active_indices.end());
+  auto t0 = std::chrono::steady_clock::now();
+  auto out = pann_range_batch(Query_Points, rows, G, Base_Points, QueryStats, starting_points[0], QP,
+                              PANN_RANGE_DOUBLING);
+  double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return {out, {secs, 0.0}};
 }
 
 // ---------------------------------------------------------------- build

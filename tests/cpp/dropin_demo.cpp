@@ -2,6 +2,7 @@
 // build a Vamana index, save/load the graph, search, check recall) written
 // against include/parlayANN/parlayann.hpp. Exit status 0 when recall@10 of
 // qsearchAll is >= 0.9 and beam_search agrees with qsearchAll.
+#include <algorithm>
 #include <cstdio>
 #include <set>
 #include <string>
@@ -54,5 +55,33 @@ int main(int argc, char** argv) {
   for (int t = 0; t < 10 && same; t++) same = lists.first[t].first == all[0][t];
   std::printf("recall@10 %.4f  visited avg %u p99 %u  cmps avg %u p99 %u  beam_search agrees %d\n", recall, vs[0], vs[1],
               cs[0], cs[1], (int)same);
-  return (recall >= 0.9 && same) ? 0 : 1;
+
+  // range search (RangeSearch, greedy; DoubleBeamRangeSearch), radius at the
+  // 20th nearest distance of query 0: every answer is within the radius, and
+  // most points within it are found
+  std::vector<float> d0;
+  for (size_t j = 0; j < n; j++) d0.push_back(Query_Points[0].distance(Points[j]));
+  std::nth_element(d0.begin(), d0.begin() + 20, d0.end());
+  const double radius = d0[20];
+  QueryParams RQ(10, 10, (long)n, 32, 0, 0.0, 0, Greedy, radius);
+  stats<unsigned int> RS(nq);
+  auto [rr, rt] = RangeSearch<Point>(G2, Query_Points, Points, Query_Points, Points, RS, 0u, RQ);
+  long found = 0, truth_n = 0;
+  bool within = true;
+  for (size_t i = 0; i < nq; i++) {
+    for (auto id : rr[i]) within &= Query_Points[i].distance(Points[id]) <= radius;
+    for (size_t j = 0; j < n; j++) truth_n += Query_Points[i].distance(Points[j]) <= radius;
+    found += (long)std::set<unsigned>(rr[i].begin(), rr[i].end()).size();
+  }
+  std::vector<unsigned int> active(nq);
+  for (size_t i = 0; i < nq; i++) active[i] = (unsigned)i;
+  QueryParams DQ(10, 10, (long)n, 32, 0, 0.0, 0, Doubling, radius);
+  stats<unsigned int> DS(nq);
+  auto [dr, dt] = DoubleBeamRangeSearch(G2, Query_Points, Points, Query_Points, Points, DS,
+                                        std::vector<unsigned int>{0u}, DQ, active);
+  for (size_t i = 0; i < nq; i++)
+    for (auto id : dr[i]) within &= Query_Points[i].distance(Points[id]) <= radius;
+  double range_recall = truth_n ? (double)found / (double)truth_n : 1.0;
+  std::printf("range: cumulative recall %.4f  all within radius %d\n", range_recall, (int)within);
+  return (recall >= 0.9 && same && within && range_recall >= 0.8) ? 0 : 1;
 }
