@@ -344,9 +344,12 @@ __global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
       if (spilled && entries - entries_sh + nel > spill_limit) { status |= QS_TABLE_FULL; break; }
       int nnew = 0;
       uint32_t ins = 0;
+      // the next 32 ids are loaded before this chunk's seen-set work, so a
+      // row longer than one warp costs one round trip, not one per chunk
+      uint32_t vnext = (uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD;
       for (uint32_t b = 0; b < nel; b += 32) {
-        uint32_t j = b + lane;
-        uint32_t v = (j < nel) ? __ldg(grow + j) : PANN_PAD;
+        const uint32_t v = vnext;
+        vnext = (b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD;
         int inserted = 0;
         if (v != PANN_PAD) {
           if (!spilled) inserted = table_insert(table, mask, v);

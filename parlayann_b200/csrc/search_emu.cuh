@@ -492,9 +492,11 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       // adjacency ids looked up in order, 32 calls per batch (:153-159)
       int nnew = 0;
       bool full_tab = false;
+      const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
+      uint32_t vnext = (uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD;  // one chunk ahead
       for (uint32_t b = 0; b < nel; b += 32) {
-        uint32_t j = b + lane;
-        uint32_t v = j < nel ? __ldg(a.graph + (uint64_t)cid * a.R + j) : PANN_PAD;
+        const uint32_t v = vnext;
+        vnext = (b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD;
         bool seen = false;
         if (!emu_batch(h, v, v != PANN_PAD, lane, &seen)) { full_tab = true; break; }
         bool isnew = v != PANN_PAD && !seen && v != self;
@@ -518,7 +520,7 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
           v0 = nbuf[i0];
           v1 = i1 < nnew ? nbuf[i1] : 0u;
           // one warp per SM here: registers are plentiful, load whole rows at once
-          point_dist2<DT, MT, 24>(a.points + (uint64_t)v0 * a.stride,
+          point_dist2<DT, MT, 12>(a.points + (uint64_t)v0 * a.stride,
                               i1 < nnew ? a.points + (uint64_t)v1 * a.stride : nullptr, qs, a.nchunks, qq, d0, d1,
                               a.opaque_zero);
         }
