@@ -108,9 +108,8 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
 // ranks in old-slot order are placed in any order (lanes take ranks far apart,
 // so they seldom share slots), which fixes the clusters; (B) the lane whose
 // key starts a cluster replays that cluster's keys in rank order, each at the
-// first free slot from its home. A key that is in the old table twice (the
-// hashset can hold one) and a cluster longer than 64 send the re-insertion
-// to a plain sequential pass instead.
+// first free slot from its home. A cluster longer than 64 sends the
+// re-insertion to a plain sequential pass instead.
 __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool* a_seen) {
   const unsigned FULL = 0xFFFFFFFFu;
   const uint32_t size = 1u << h.bits, nsize = size * 2;
@@ -123,19 +122,35 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
   // the old table's keys compacted to its front in slot order (writes never
   // pass the chunk being read): keys[r] is the key of rank r
   uint32_t cnt = 0;
-  for (uint32_t base = 0; base < size; base += 32) {
-    uint32_t k = h.cur[base + lane];
-    bool v = k != PANN_PAD;
-    unsigned m = __ballot_sync(FULL, v);
+  for (uint32_t base = 0; base < size; base += 128) {  // 4 slots per lane per step
+    uint32_t k4[4];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t i = base + 4 * (uint32_t)lane + (uint32_t)j;
+      k4[j] = i < size ? h.cur[i] : PANN_PAD;
+      c += k4[j] != PANN_PAD;
+    }
+    uint32_t pre = c;  // inclusive prefix over lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, pre, d);
+      if (lane >= d) pre += t;
+    }
+    const uint32_t total = __shfl_sync(FULL, pre, 31);
     __syncwarp();
-    if (v) h.cur[cnt + __popc(m & ((1u << lane) - 1))] = k;
-    cnt += __popc(m);
+    uint32_t at = cnt + pre - c;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k4[j] != PANN_PAD) h.cur[at++] = k4[j];
+    cnt += total;
     __syncwarp();
   }
   uint32_t* keys = h.cur;
-  // (A) ranks into the new table, lane l taking rank l * nb + b in batch b
+  // (A) ranks into the new table, lane l taking rank l * nb + b in batch b; a
+  // key the old table holds twice keeps the smaller rank (its first copy in
+  // old-slot order, the one the reference inserts; the other copy finds it)
   const uint32_t nb = (cnt + 31) / 32;
-  bool dup = false;
   for (uint32_t b = 0; b < nb; b++) {
     const uint32_t r = (uint32_t)lane * nb + b;
     bool done = r >= cnt;
@@ -145,7 +160,10 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
       if (!done) {
         uint32_t w = other[p];
         while (w != PANN_PAD && keys[w] != k) { p = (p + 1) & nmask; w = other[p]; }
-        if (w != PANN_PAD) { done = true; dup = true; }
+        if (w != PANN_PAD) {
+          done = true;
+          if (r < w) atomicMin(other + p, r);
+        }
       }
       const unsigned want = __ballot_sync(FULL, !done);
       if (!want) break;
@@ -157,7 +175,9 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
       __syncwarp();
     }
   }
-  bool fallback = __any_sync(FULL, dup);
+  __syncwarp();
+  __threadfence_block();
+  bool fallback = false;
   // (B) owners: keys that start a cluster, one bit per rank in the old table's
   // free tail; then each owner replays its cluster (up to 8 keys in registers,
   // up to 64 through a per-lane scratch row also in the free tail)
@@ -170,9 +190,11 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
       const uint32_t r = b * 32 + lane;
       bool own = false;
       if (r < cnt) {
-        uint32_t p = ref_slot(keys[r], nmask);
-        while (other[p] != r) p = (p + 1) & nmask;
-        own = other[(p - 1) & nmask] == PANN_PAD;
+        const uint32_t k = keys[r];
+        uint32_t p = ref_slot(k, nmask);
+        uint32_t w = other[p];
+        while (w != r && keys[w] != k) { p = (p + 1) & nmask; w = other[p]; }
+        own = w == r && other[(p - 1) & nmask] == PANN_PAD;  // a second copy of a key owns nothing
       }
       const unsigned om = __ballot_sync(FULL, own);
       if (lane == 0) owner[b] = om;
