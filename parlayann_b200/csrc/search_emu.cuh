@@ -151,8 +151,9 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
   // key the old table holds twice keeps the smaller rank (its first copy in
   // old-slot order, the one the reference inserts; the other copy finds it)
   const uint32_t nb = (cnt + 31) / 32;
-  for (uint32_t b = 0; b < nb; b++) {
-    const uint32_t r = (uint32_t)lane * nb + b;
+  const uint32_t stride = nb | 1u;  // odd: the 32 lanes' ranks fall in 32 different banks
+  for (uint32_t b = 0; b < stride; b++) {
+    const uint32_t r = (uint32_t)lane * stride + b;
     bool done = r >= cnt;
     const uint32_t k = done ? PANN_PAD : keys[r];
     uint32_t p = ref_slot(k, nmask);
@@ -211,9 +212,14 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
         if (m == 1) {
           other[s0] = keys[r];
         } else if (m <= 8) {
-          uint32_t ix[8];
+          uint32_t ix[8], kx[8], ox[8];
 #pragma unroll
           for (int j = 0; j < 8; j++) ix[j] = (uint32_t)j < m ? other[(s0 + j) & nmask] : 0xFFFFFFFFu;
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            kx[j] = (uint32_t)j < m ? keys[ix[j]] : 0u;
+            ox[j] = (ref_slot(kx[j], nmask) - s0) & nmask;  // home offset inside the cluster
+          }
           uint32_t taken = 0, used = 0;
           for (uint32_t t = 0; t < m; t++) {
             uint32_t best = 0xFFFFFFFFu, bj = 0;
@@ -221,8 +227,10 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
             for (int j = 0; j < 8; j++)
               if (!((used >> j) & 1u) && ix[j] < best) { best = ix[j]; bj = (uint32_t)j; }
             used |= 1u << bj;
-            const uint32_t key = keys[best];
-            const uint32_t o = (ref_slot(key, nmask) - s0) & nmask;  // inside the cluster
+            uint32_t key = 0, o = 0;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+              if ((uint32_t)j == bj) { key = kx[j]; o = ox[j]; }
             const uint32_t pos = (uint32_t)(__ffs(~taken & (~0u << o)) - 1);
             taken |= 1u << pos;
             other[(s0 + pos) & nmask] = key;
