@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
       const uint64_t room = a.limit > nvis ? a.limit - nvis : 0;
       const uint32_t wlim = (uint32_t)(room < W ? room : W);
       if (warp == 0) {
-        uint32_t np = 0;
-        for (uint32_t b = 0; b < fn && np < wlim; b += 32) {
+        uint32_t np = 0, npre = 0;
+        for (uint32_t b = 0; b < fn && npre < W; b += 32) {
           const uint32_t i = b + lane;
           unsigned m = __ballot_sync(FULL, i < fn && !(fr[i] & PANN_VFLAG));
           while (m && np < wlim) {
@@ -216,6 +216,15 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
               fr[b + j] |= PANN_VFLAG;
             }
             np++;
+          }
+          // the next best unvisited entries are the likely parents of the
+          // next step: start their adjacency rows on their way to L2
+          while (m && npre < W) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            if (lane == (int)npre)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[b + j]) * a.R));
+            npre++;
           }
         }
         if (lane == 0) {
