@@ -2,8 +2,10 @@
 from __future__ import annotations
 
 import os
+import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -26,13 +28,35 @@ def needs_rebuild() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (one nvcc per file), then link."""
     if not force and not needs_rebuild():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, *[os.path.join(CSRC, s) for s in SOURCES], "-o", OUT + ".tmp"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True, cwd=CSRC)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    objdir = tempfile.mkdtemp(prefix="pann_build_")
+    try:
+        objs, procs = [], []
+        for src in SOURCES:
+            obj = os.path.join(objdir, src + ".o")
+            cmd = [nvcc, *compile_flags, "-c", os.path.join(CSRC, src), "-o", obj]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            procs.append((src, subprocess.Popen(cmd, cwd=CSRC, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+            objs.append(obj)
+        failed = []
+        for src, pr in procs:
+            out, _ = pr.communicate()
+            if pr.returncode != 0:
+                failed.append(src)
+                sys.stderr.write(out.decode(errors="replace"))
+        if failed:
+            raise subprocess.CalledProcessError(1, "nvcc " + " ".join(failed))
+        link = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", OUT + ".tmp"]
+        if verbose:
+            print(" ".join(link), file=sys.stderr)
+        subprocess.run(link, check=True, cwd=CSRC)
+    finally:
+        shutil.rmtree(objdir, ignore_errors=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 
