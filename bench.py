@@ -427,6 +427,7 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     radius = range_radius(base, q)
     if "range" in want:
         nr = 200
+        idx.range_search(q[:8], 20, radius, P.RANGE_GREEDY)  # warm-up
         t0 = time.perf_counter()
         rr = idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)
         t_r = time.perf_counter() - t0
@@ -434,6 +435,22 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         out["range"] = {"queries": nr, "beam": 20, "type": "greedy", "radius_quantile": 0.01, "radius": radius,
                         "qps_e2e": round(nr / t_r, 1), "mean_answer": float(sizes.mean()),
                         "answer_ids_per_s": round(float(sizes.sum()) / t_r, 1)}
+        # the reference's RangeSearch (compiled in place) on the host cores, same graph and queries
+        try:
+            from oracle import oracle as O
+
+            if O.have_ref() and not args.no_cpu_baseline:
+                g = idx.get_graph()
+                nc = 40
+                t0 = time.perf_counter()
+                ro = O.range_search("ref", base, q[:nc], g, 20, radius, O.RANGE_GREEDY, cap=int(sizes.max() * 4) + 64)
+                t_c = time.perf_counter() - t0
+                same = all(np.array_equal(a, b) for a, b in zip(ro["ids"], rr["ids"][:nc]))
+                out["range"]["cpu_reference"] = {"queries": nc, "qps": round(nc / t_c, 1),
+                                                 "cores": int(O.rlib().ref_num_workers()),
+                                                 "answers_identical": bool(same)}
+        except Exception as ex:  # noqa: BLE001
+            out["range"]["cpu_reference"] = {"failed": str(ex)}
     if "serving" in want:
         out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
     return out

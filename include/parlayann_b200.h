@@ -283,6 +283,9 @@ int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32
 int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps_per_block, uint32_t* blocks,
                       int32_t* graph_captured);
 
+/* Frees the batch. Device-buffer runs are asynchronous: call this after the
+ * last run's stream work has completed (host-buffer runs are synchronous).
+ * The index may already have been destroyed. */
 int pann_batch_destroy(pann_batch* b);
 
 /* ---------------------------------------------------------------- serving form */
