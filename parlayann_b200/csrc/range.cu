@@ -36,6 +36,7 @@
 namespace pann {
 
 enum RangeStatus : uint32_t { RS_RETRY = 1u, RS_GREW = 2u };
+constexpr int HOME_BATCH = 16;  // home-slot loads in flight per lane
 
 struct RangeArgs {
   const uint8_t* points;
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(32) range_expand_kernel(RangeArgs a) {
   uint8_t* qs = smem;
   uint32_t* kbuf = reinterpret_cast<uint32_t*>(smem + a.stride);
   uint32_t* ubuf = kbuf + a.keybuf;
+  uint32_t* kraw = ubuf + a.keybuf;  // a round's adjacency rows as loaded
   uint32_t* tabA = a.tabs + (size_t)blockIdx.x * 2 * a.cap;
   uint32_t* tabB = tabA + a.cap;
   uint32_t* Q = a.queues + (size_t)blockIdx.x * a.qcap;
@@ -144,40 +146,91 @@ __global__ void __launch_bounds__(32) range_expand_kernel(RangeArgs a) {
     }
     __syncwarp();
 
-    // breadth-first expansion (rangeSearch.h:36-52)
+    // breadth-first expansion (rangeSearch.h:36-52), up to gn queued nodes a
+    // round: their adjacency rows are gathered together (one memory round
+    // trip), the hash homes of all their neighbours and the next round's rows
+    // are prefetched into L2, the hashset calls run in order, and the rows of
+    // the new neighbours are prefetched as the calls find them
+    const uint32_t gn = a.keybuf / a.R > 0 ? a.keybuf / a.R : 1;
+    const uint32_t row_lines = (a.R * 4 + 127) / 128;
     uint32_t pos = 0;
     while (ok && pos < count) {
-      // neighbours of the queued nodes pos.. in order, within the key budget
-      uint32_t nk = 0, end = pos;
-      while (end < count) {
-        const uint32_t node = Q[end];
-        const uint32_t* row = a.graph + (uint64_t)node * a.R;
-        uint32_t deg = 0;
-        for (uint32_t b = 0; b < a.R; b += 32) {
-          const bool in = b + lane < a.R && row[b + lane] != PANN_PAD;
-          deg += __popc(__ballot_sync(FULL, in));
+      const uint32_t end = count - pos < gn ? count : pos + gn;
+      const uint32_t nraw = (end - pos) * a.R;
+      for (uint32_t i = lane; i < nraw; i += 32) {
+        const uint32_t node = Q[pos + i / a.R];
+        kraw[i] = __ldg(a.graph + (uint64_t)node * a.R + (i % a.R));
+      }
+      {  // the next round's rows (nodes queued so far)
+        const uint32_t nend = count - end < gn ? count : end + gn;
+        for (uint32_t i = lane; i < (nend - end) * row_lines; i += 32) {
+          const uint32_t node = Q[end + i / row_lines];
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)node * a.R + 32 * (i % row_lines)));
         }
-        if (end > pos && nk + deg > a.keybuf) break;
-        for (uint32_t b = 0; b < a.R; b += 32) {
-          const uint32_t v = b + lane < a.R ? row[b + lane] : PANN_PAD;
-          const bool in = v != PANN_PAD;
-          const unsigned m = __ballot_sync(FULL, in);
-          if (in) kbuf[nk + __popc(m & lt)] = v;
-          nk += __popc(m);
-        }
-        end++;
       }
       __syncwarp();
+      // the neighbours in order (a row's live entries are those before PAD)
+      uint32_t nk = 0;
+      for (uint32_t b = 0; b < nraw; b += 32) {
+        const uint32_t v = b + lane < nraw ? kraw[b + lane] : PANN_PAD;
+        const bool in = v != PANN_PAD;
+        const unsigned m = __ballot_sync(FULL, in);
+        if (in) {
+          kbuf[nk + __popc(m & lt)] = v;
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(h.cur + ref_slot(v, (1u << h.bits) - 1u)));
+        }
+        nk += __popc(m);
+      }
+      __syncwarp();
+      // A call whose key already sits at its home slot returns true and
+      // changes nothing (hashset.h:23-24). Slots are only ever emptied by a
+      // growth, so a key found at its home now is still found there at its
+      // turn unless the table grows first, and it cannot grow while
+      // num_entries stays at or below half its size (hashset.h:25). When
+      // even the round's other calls all inserting keeps it there, only
+      // those other calls run, in order; otherwise the round runs them all.
+      const uint32_t* calls = kbuf;
+      uint32_t ncalls = nk;
+      {
+        const uint32_t mask0 = (1u << h.bits) - 1u;
+        uint32_t nf = 0;
+        for (uint32_t b0 = 0; b0 < nk; b0 += 32 * HOME_BATCH) {
+          uint32_t hv[HOME_BATCH];
+#pragma unroll
+          for (int j = 0; j < HOME_BATCH; j++) {
+            const uint32_t i = b0 + 32 * j + lane;
+            hv[j] = i < nk ? h.cur[ref_slot(kbuf[i], mask0)] : PANN_PAD;
+          }
+#pragma unroll
+          for (int j = 0; j < HOME_BATCH; j++) {
+            const uint32_t i = b0 + 32 * j + lane;
+            const uint32_t key = i < nk ? kbuf[i] : PANN_PAD;
+            const bool keep = i < nk && hv[j] != key;
+            const unsigned m = __ballot_sync(FULL, keep);
+            if (keep) kraw[nf + __popc(m & lt)] = key;
+            nf += __popc(m);
+          }
+        }
+        __syncwarp();
+        if (h.num_entries + (long long)nf <= (long long)((1u << h.bits) / 2)) {
+          calls = kraw;
+          ncalls = nf;
+        }
+      }
       // the hashset calls, in order
       uint32_t nun = 0;
-      for (uint32_t k0 = 0; k0 < nk && ok; k0 += 32) {
-        const bool valid = k0 + lane < nk;
-        const uint32_t key = valid ? kbuf[k0 + lane] : PANN_PAD;
+      for (uint32_t k0 = 0; k0 < ncalls && ok; k0 += 32) {
+        const bool valid = k0 + lane < ncalls;
+        const uint32_t key = valid ? calls[k0 + lane] : PANN_PAD;
         bool seen = false;
         ok = emu_batch(h, key, valid, lane, &seen);
         const bool un = ok && valid && !seen;
         const unsigned m = __ballot_sync(FULL, un);
-        if (un) ubuf[nun + __popc(m & lt)] = key;
+        if (un) {
+          ubuf[nun + __popc(m & lt)] = key;
+          const char* row = reinterpret_cast<const char*>(a.points + (uint64_t)key * a.stride);
+          for (uint32_t o = 0; o < a.stride; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + o));
+        }
         nun += __popc(m);
       }
       __syncwarp();
@@ -354,10 +407,19 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
   // a pool sized up front and grown (with a re-run) if they do not fit
   const uint32_t bits0 = ceil_log2(2ull * beam * 64);
   if (h_njobs > 0) {
+    // The first tier gives each of its slots (a warp running one expansion
+    // after another) the largest tables that fit 4 GB at that slot count, so
+    // that only rare, very large expansions fail there and re-run from the
+    // start in the second tier's 2^24-slot tables. The queue holds a quarter
+    // of a table: a table outgrows its slots before its queue fills.
     struct Tier { uint32_t cap_bits, qcap_bits; int max_slots; };
-    const Tier tiers[2] = {{std::max<uint32_t>(18, bits0 + 2), 16, 2 * idx->sm_count}, {std::max<uint32_t>(24, bits0 + 2), 22, 16}};
-    const uint32_t keybuf = std::max<uint32_t>(256, 4 * idx->R);
-    const size_t smem = idx->stride + 8ull * keybuf;
+    const int slots0 = (int)std::min<uint64_t>(h_njobs, 2ull * idx->sm_count);
+    uint32_t cap0 = 18;
+    while (cap0 < 22 && (uint64_t)slots0 * 4ull * (2ull * (2ull << cap0) + (1ull << (cap0 - 1))) <= (4ull << 30)) cap0++;
+    cap0 = std::max(cap0, bits0 + 2);
+    const Tier tiers[2] = {{cap0, cap0 - 2, 2 * idx->sm_count}, {std::max<uint32_t>(24, bits0 + 2), 22, 16}};
+    const uint32_t keybuf = std::max<uint32_t>(1024, idx->R);
+    const size_t smem = idx->stride + 12ull * keybuf;
     unsigned long long pool_cap = std::max<unsigned long long>(1ull << 22, 256ull * h_njobs);
     for (int attempt = 0; attempt < 3; attempt++) {
       PANN_CUDA(idx->range_pool.ensure(4 * pool_cap));
