@@ -427,13 +427,15 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     radius = range_radius(base, q)
     if "range" in want:
         nr = 200
-        idx.range_search(q[:8], 20, radius, P.RANGE_GREEDY)  # warm-up
+        idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)  # warm-up: the expansion tables are allocated
         t0 = time.perf_counter()
         rr = idx.range_search(q[:nr], 20, radius, P.RANGE_GREEDY)
         t_r = time.perf_counter() - t0
         sizes = np.array([len(x) for x in rr["ids"]])
         out["range"] = {"queries": nr, "beam": 20, "type": "greedy", "radius_quantile": 0.01, "radius": radius,
                         "qps_e2e": round(nr / t_r, 1), "mean_answer": float(sizes.mean()),
+                        "answer_p50_p99_max": [int(np.percentile(sizes, 50)), int(np.percentile(sizes, 99)),
+                                               int(sizes.max())],
                         "answer_ids_per_s": round(float(sizes.sum()) / t_r, 1)}
         # the reference's RangeSearch (compiled in place) on the host cores, same graph and queries
         try:

@@ -533,10 +533,9 @@ std::vector<std::vector<indexType>> pann_range_batch(const PointRange_& Query_Po
   std::vector<uint32_t> vis(nq), cmps(nq), ids(nq * (size_t)QP.beamSize + 16);
   int rc = pann_range_search(idx, q.data(), (uint32_t)nq, &rp, (uint32_t)start, offs.data(), ids.data(), ids.size(),
                              vis.data(), cmps.data(), nullptr);
-  if (rc == PANN_EOVERFLOW && offs[nq] > ids.size()) {
+  if (rc == PANN_EOVERFLOW && offs[nq] > ids.size()) {  // the answers are held on the device
     ids.resize(offs[nq]);
-    rc = pann_range_search(idx, q.data(), (uint32_t)nq, &rp, (uint32_t)start, offs.data(), ids.data(), ids.size(),
-                           vis.data(), cmps.data(), nullptr);
+    rc = pann_range_fetch(idx, ids.data(), ids.size());
   }
   pann_check(rc, "range search");
   std::vector<std::vector<indexType>> out(nq);

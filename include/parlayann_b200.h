@@ -228,14 +228,24 @@ typedef struct {
  * expands from them and its discovery order is the answer (duplicates that
  * the reference's hashset lets through included). Host buffers: answer i is
  * out_ids[out_offsets[i] .. out_offsets[i+1]) (out_offsets has nq + 1
- * entries). If the answers need more than ids_cap ids, out_offsets is filled,
- * out_ids is not, and PANN_EOVERFLOW is returned: call again with room for
- * out_offsets[nq]. out_visited / out_cmps (may be NULL) get the QueryStats
+ * entries). If the answers need more than ids_cap ids (or out_ids is NULL
+ * and ids_cap 0, to learn the size), out_offsets and the counts are filled,
+ * out_ids is not, PANN_EOVERFLOW is returned, and the answers stay on the
+ * device for pann_range_fetch. out_visited / out_cmps (may be NULL) get the QueryStats
  * counts; out_flags (may be NULL): bit 0 = the beam's hashset grew, bit 1 =
  * the expansion's hashset grew (both reproduced exactly). */
 int pann_range_search(pann_index* idx, const void* queries, uint32_t nq, const pann_range_params* rp,
                       uint32_t start_point, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
                       uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags);
+
+/* The answers of the last pann_range_search on this index that returned
+ * PANN_EOVERFLOW for want of room, into out_ids (ids_cap >= the
+ * out_offsets[nq] that call reported), without searching again. The reference
+ * sizes each answer vector as it fills (all_neighbors, rangeSearch.h:193,
+ * :242-257); a caller with fixed host buffers asks for the size first and
+ * fetches the held answers with this. They are held until the next
+ * pann_range_search on the index; PANN_EINVAL if none are held. */
+int pann_range_fetch(pann_index* idx, uint32_t* out_ids, uint64_t ids_cap);
 
 /* ---------------------------------------------------------------- batched form */
 

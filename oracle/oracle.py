@@ -61,6 +61,8 @@ def olib():
         L.oracle_range_search.restype = _I
         L.oracle_range_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _I, _D, _D, _U32,
                                           _P, _P, _U64, _P, _P, _P]
+        L.oracle_range_groundtruth.restype = _I
+        L.oracle_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
         L.oracle_distance.restype = ctypes.c_float
         L.oracle_distance.argtypes = [_I, _I, ctypes.c_uint, _P, _P]
         _olib = L
@@ -87,6 +89,8 @@ def rlib():
         L.ref_range_search.restype = _I
         L.ref_range_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _I, _D, _D, _U32, _P,
                                        _P, _U64, _P, _P]
+        L.ref_range_groundtruth.restype = _I
+        L.ref_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
         L.ref_num_workers.restype = _I
         L.ref_num_workers.argtypes = []
         _rlib = L
@@ -169,6 +173,26 @@ def range_search(impl, base, queries, graph, beam, radius, rtype=RANGE_GREEDY, s
     out.update(ids=[ids[i, : int(cnt[i])].copy() for i in range(nq)], visited=vis,
                cmps=(cmps & 0xFFFFFFFF).astype(np.uint32))
     return out
+
+
+def range_groundtruth(impl, base, queries, radius, metric=0):
+    """Every base id within `radius` of each query, in id order ('oracle': pann_oracle.c; 'ref':
+    compute_range_groundtruth compiled in place). Returns (offsets[nq + 1], ids)."""
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    n, d = base.shape
+    nq = queries.shape[0]
+    fn = olib().oracle_range_groundtruth if impl == "oracle" else rlib().ref_range_groundtruth
+    offs = np.zeros(nq + 1, np.uint64)
+    cap = 0
+    for _ in range(2):
+        ids = np.zeros(max(cap, 1), np.uint32)
+        rc = fn(_DT[base.dtype], metric, n, d, _p(base), nq, _p(queries), radius, _p(offs), _p(ids), cap)
+        assert rc in (0, 1), rc
+        if rc == 0:
+            return offs, ids[: int(offs[nq])]
+        cap = int(offs[nq])
+    raise AssertionError("range groundtruth did not fit")
 
 
 def robust_prune(impl, base, graph, p, cand_ids, cand_d, alpha, add=True, metric=0):

@@ -456,6 +456,32 @@ int oracle_range_search(int dtype, int metric, uint32_t n, uint32_t d, const voi
   return 0;
 }
 
+/* ------------------------------------------------------------ range groundtruth */
+/* compute_range_groundtruth (data_tools/compute_range_groundtruth.cpp:14-30):
+ * answer i = every base id j, in increasing order, whose float distance
+ * Q[i].distance(B[j]) is <= the float radius. out_offsets has nq + 1 entries;
+ * ids past cap are counted, not written. Returns 1 if they did not fit. */
+int oracle_range_groundtruth(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+                             const void* queries, float radius, uint64_t* out_offsets, uint32_t* out_ids,
+                             uint64_t cap) {
+  pts_t P = {dtype, metric, d, d * elem_size(dtype), (const uint8_t*)base};
+  pts_t Q = {dtype, metric, d, d * elem_size(dtype), (const uint8_t*)queries};
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < nq; i++) {
+    out_offsets[i] = total;
+    const void* q = row(&Q, i);
+    for (uint32_t j = 0; j < n; j++) {
+      const float dd = dist(&P, q, row(&P, j));
+      if (dd <= radius) {
+        if (total < cap) out_ids[total] = j;
+        total++;
+      }
+    }
+  }
+  out_offsets[nq] = total;
+  return total > cap ? 1 : 0;
+}
+
 /* ------------------------------------------------------------ robustPrune */
 /* knn_index::robustPrune (index.h:63-120): candidates = cand ++ (if add) the
  * current out-neighbours of p with their distances; sort by (dist, id);

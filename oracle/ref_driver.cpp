@@ -15,6 +15,8 @@
 //   ref_build        knn_index::build_index()          (index.h:150-186)
 //   ref_range_search RangeSearch() / DoubleBeamRangeSearch()
 //                                        (rangeSearch.h:183-276, doublingSearch.h:50-157)
+//   ref_range_groundtruth compute_range_groundtruth() (data_tools/compute_range_groundtruth.cpp:14-30;
+//                    the tool's file is included with its main() renamed)
 //   ref_num_workers  threads used by parallel_for
 #include <cstdint>
 #include <cstring>
@@ -29,6 +31,10 @@
 #include "vamana/index.h"
 #include "utils/rangeSearch.h"
 #include "utils/doublingSearch.h"
+
+#define main pann_ref_range_groundtruth_tool_main
+#include "../data_tools/compute_range_groundtruth.cpp"
+#undef main
 
 using namespace parlayANN;
 
@@ -220,6 +226,24 @@ int range_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* q
   return 0;
 }
 
+template <typename Point>
+int range_gt_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries, float radius,
+               uint64_t* out_offsets, uint32_t* out_ids, uint64_t cap) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto ans = compute_range_groundtruth<PR>(B, Q, radius);
+  uint64_t total = 0;
+  for (size_t i = 0; i < nq; i++) {
+    out_offsets[i] = total;
+    for (size_t j = 0; j < ans[i].size(); j++)
+      if (total + j < cap) out_ids[total + j] = (uint32_t)ans[i][j];
+    total += ans[i].size();
+  }
+  out_offsets[nq] = total;
+  return total > cap ? 1 : 0;
+}
+
 }  // namespace
 
 #define DISPATCH(dtype, metric, FN, ...)                                                  \
@@ -285,6 +309,13 @@ int ref_range_search(int dtype, int metric, uint32_t n, uint32_t d, const void* 
                      uint64_t cap, uint32_t* out_visited, uint64_t* out_cmps) {
   DISPATCH(dtype, metric, range_t, n, d, base, nq, queries, R, graph, beam, start, type, radius, esr, esc,
            out_count, out_ids, cap, out_visited, out_cmps);
+  return -1;
+}
+
+int ref_range_groundtruth(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+                          const void* queries, float radius, uint64_t* out_offsets, uint32_t* out_ids,
+                          uint64_t cap) {
+  DISPATCH(dtype, metric, range_gt_t, n, d, base, nq, queries, radius, out_offsets, out_ids, cap);
   return -1;
 }
 

@@ -127,6 +127,7 @@ SIGNATURES = {
     "pann_search_ex": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.POINTER(SearchOptions), _P, _U32, _P,
                             _P, _P, _P, _P, _I, _P]),
     "pann_range_search": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, _P, _P, _U64, _P, _P, _P]),
+    "pann_range_fetch": (_I, [_P, _P, _U64]),
     "pann_server_create": (_I, [ctypes.POINTER(_P), _P, ctypes.POINTER(ServerOptions), _P, _U32]),
     "pann_server_submit_knn": (_I, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U64)]),
     "pann_server_submit_range": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, ctypes.POINTER(_U64)]),
@@ -330,15 +331,13 @@ class Index:
         cmps = np.zeros(nq, np.uint32)
         flags = np.zeros(nq, np.uint32)
         cap = max(1, nq * beam * 4)
-        for _ in range(2):
-            ids = np.zeros(cap, np.uint32)
-            rc = lib().pann_range_search(self._h, _ptr(queries), nq, ctypes.byref(rp), start, _ptr(offs), _ptr(ids),
-                                         cap, _ptr(vis), _ptr(cmps), _ptr(flags))
-            if rc == PANN_EOVERFLOW and int(offs[nq]) > cap:
-                cap = int(offs[nq])
-                continue
-            _check(rc)
-            break
+        ids = np.zeros(cap, np.uint32)
+        rc = lib().pann_range_search(self._h, _ptr(queries), nq, ctypes.byref(rp), start, _ptr(offs), _ptr(ids),
+                                     cap, _ptr(vis), _ptr(cmps), _ptr(flags))
+        if rc == PANN_EOVERFLOW and int(offs[nq]) > cap:   # the answers are held on the device
+            ids = np.zeros(int(offs[nq]), np.uint32)
+            rc = lib().pann_range_fetch(self._h, _ptr(ids), len(ids))
+        _check(rc)
         lists = [ids[int(offs[i]):int(offs[i + 1])].copy() for i in range(nq)]
         return dict(ids=lists, offsets=offs, visited=vis, cmps=cmps, flags=flags)
 

@@ -64,6 +64,7 @@ struct pann_index {
   pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, gtables2, emu, handoff, starts, tmp;
   // range search: per-query metadata, expansion tables and queues, answer pool, CSR output
   pann::DevBuf range_meta, range_tabs, range_pool, range_out;
+  uint64_t range_held = 0;  // ids in range_out left for pann_range_fetch (0: none)
   // precision form: low-precision copy of float32 points (lowprec.cuh)
   pann::DevBuf lp_rows, lp_scales;
   int lp_prec = 0;

@@ -36,7 +36,8 @@
 namespace pann {
 
 enum RangeStatus : uint32_t { RS_RETRY = 1u, RS_GREW = 2u };
-constexpr int HOME_BATCH = 16;  // home-slot loads in flight per lane
+constexpr int HOME_BATCH = 8;      // table loads in flight per thread
+constexpr int EXPAND_THREADS = 128;  // one block per expansion
 
 struct RangeArgs {
   const uint8_t* points;
@@ -96,55 +97,118 @@ __global__ void range_classify_kernel(const uint32_t* __restrict__ fr_ids, const
   }
 }
 
+// Block-wide ordered compaction: the entries of tmp[0, n) other than PAD, in
+// order, to out[0, cap); returns how many there are (possibly above cap) to
+// every thread. ccnt holds n / 32 + 1 words of shared memory, tot one.
+__device__ __forceinline__ uint32_t block_compact(const uint32_t* tmp, uint32_t n, uint32_t* out, uint32_t cap,
+                                                  uint32_t* ccnt, uint32_t* tot) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const uint32_t nch = (n + 31) / 32;
+  for (uint32_t c = warp; c < nch; c += nw) {
+    const uint32_t i = c * 32 + lane;
+    const unsigned m = __ballot_sync(FULL, i < n && tmp[i] != PANN_PAD);
+    if (lane == 0) ccnt[c] = __popc(m);
+  }
+  __syncthreads();
+  if (warp == 0) {  // exclusive scan of the chunk counts
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < nch; c0 += 32) {
+      const uint32_t v = c0 + lane < nch ? ccnt[c0 + lane] : 0u;
+      uint32_t incl = v;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, incl, d);
+        if (lane >= d) incl += t;
+      }
+      if (c0 + lane < nch) ccnt[c0 + lane] = carry + incl - v;
+      carry += __shfl_sync(FULL, incl, 31);
+    }
+    if (lane == 0) *tot = carry;
+  }
+  __syncthreads();
+  for (uint32_t c = warp; c < nch; c += nw) {
+    const uint32_t i = c * 32 + lane;
+    const bool keep = i < n && tmp[i] != PANN_PAD;
+    const unsigned m = __ballot_sync(FULL, keep);
+    const uint32_t o = ccnt[c] + __popc(m & lt);
+    if (keep && o < cap) out[o] = tmp[i];
+  }
+  const uint32_t total = *tot;
+  __syncthreads();
+  return total;
+}
+
+enum : uint32_t { CTL_JOB = 0, CTL_OK, CTL_COUNT, CTL_NUN, CTL_NCALLS, CTL_FILTERED, CTL_BITS, CTL_TOT, CTL_CUR, CTL_WORDS = 16 };
+
+// One block per query (EXPAND_THREADS threads). Warp 0 owns the emulated
+// hashset and makes its calls in order; every warp gathers adjacency rows,
+// looks keys up in the table as it stands, scores new neighbours and takes
+// part in the ordered compactions.
 template <int DT, int MT>
-__global__ void __launch_bounds__(32) range_expand_kernel(RangeArgs a) {
+__global__ void __launch_bounds__(EXPAND_THREADS) range_expand_kernel(RangeArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const unsigned FULL = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t nthr = blockDim.x;
   const unsigned lt = (1u << lane) - 1u;
   uint8_t* qs = smem;
   uint32_t* kbuf = reinterpret_cast<uint32_t*>(smem + a.stride);
   uint32_t* ubuf = kbuf + a.keybuf;
   uint32_t* kraw = ubuf + a.keybuf;  // a round's adjacency rows as loaded
+  uint32_t* ctl = kraw + a.keybuf;
+  uint32_t* ccnt = ctl + CTL_WORDS;
   uint32_t* tabA = a.tabs + (size_t)blockIdx.x * 2 * a.cap;
   uint32_t* tabB = tabA + a.cap;
   uint32_t* Q = a.queues + (size_t)blockIdx.x * a.qcap;
   const uint32_t njobs = *a.njobs;
 
   for (;;) {
-    uint32_t job = 0;
-    if (lane == 0) job = atomicAdd(a.job_counter, 1u);
-    job = __shfl_sync(FULL, job, 0);
+    __syncthreads();
+    if (tid == 0) ctl[CTL_JOB] = atomicAdd(a.job_counter, 1u);
+    __syncthreads();
+    const uint32_t job = ctl[CTL_JOB];
     if (job >= njobs) break;
     const uint32_t qi = a.jobs[job];
-    stage_query<DT, MT>(qs, a.queries + (uint64_t)qi * a.stride, (int)a.nchunks, lane);
-    for (uint32_t i = lane; i < (1u << a.bits0); i += 32) tabA[i] = PANN_PAD;
-    __syncwarp();
-    __threadfence_block();
+    if (warp == 0) stage_query<DT, MT>(qs, a.queries + (uint64_t)qi * a.stride, (int)a.nchunks, lane);
+    for (uint32_t i = tid; i < (1u << a.bits0); i += nthr) tabA[i] = PANN_PAD;
+    __syncthreads();
     int32_t qq = 0;
     if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), a.nchunks);
-    EmuHash h;
+    EmuHash h;  // warp 0's copy is the hashset; the others read bits and table from ctl
     h.cur = tabA; h.other = tabB; h.cur_cap = a.cap; h.other_cap = a.cap;
     h.bits = a.bits0; h.num_entries = 0;
-    bool ok = true;
-    uint32_t count = 0, cmps = 0;
+    uint32_t cmps = 0;
 
     // seeds: every frontier entry goes through the hashset; new and in range
     // ones start the queue (rangeSearch.h:30-33)
-    for (uint32_t s0 = 0; s0 < a.beam && ok; s0 += 32) {
-      const bool valid = s0 + lane < a.beam;
-      const uint32_t id = valid ? a.fr_ids[(uint64_t)qi * a.beam + s0 + lane] : PANN_PAD;
-      const float dd = valid ? a.fr_d[(uint64_t)qi * a.beam + s0 + lane] : 0.0f;
-      bool seen = false;
-      ok = emu_batch(h, id, valid, lane, &seen);
-      if (!ok) break;
-      const bool keep = valid && !seen && !((double)dd > a.radius);
-      const unsigned m = __ballot_sync(FULL, keep);
-      if (keep && count + __popc(m & lt) < a.qcap) Q[count + __popc(m & lt)] = id;
-      count += __popc(m);
-      if (count > a.qcap) ok = false;
+    if (warp == 0) {
+      bool ok = true;
+      uint32_t count = 0;
+      for (uint32_t s0 = 0; s0 < a.beam && ok; s0 += 32) {
+        const bool valid = s0 + lane < a.beam;
+        const uint32_t id = valid ? a.fr_ids[(uint64_t)qi * a.beam + s0 + lane] : PANN_PAD;
+        const float dd = valid ? a.fr_d[(uint64_t)qi * a.beam + s0 + lane] : 0.0f;
+        bool seen = false;
+        ok = emu_batch(h, id, valid, lane, &seen);
+        if (!ok) break;
+        const bool keep = valid && !seen && !((double)dd > a.radius);
+        const unsigned m = __ballot_sync(FULL, keep);
+        if (keep && count + __popc(m & lt) < a.qcap) Q[count + __popc(m & lt)] = id;
+        count += __popc(m);
+        if (count > a.qcap) ok = false;
+      }
+      if (lane == 0) {
+        ctl[CTL_OK] = ok;
+        ctl[CTL_COUNT] = count;
+        ctl[CTL_BITS] = h.bits;
+        *reinterpret_cast<uint32_t**>(ctl + CTL_CUR) = h.cur;
+      }
     }
-    __syncwarp();
+    __syncthreads();
+    bool ok = ctl[CTL_OK] != 0;
+    uint32_t count = ctl[CTL_COUNT];
 
     // breadth-first expansion (rangeSearch.h:36-52), up to gn queued nodes a
     // round: their adjacency rows are gathered together (one memory round
@@ -157,122 +221,127 @@ __global__ void __launch_bounds__(32) range_expand_kernel(RangeArgs a) {
     while (ok && pos < count) {
       const uint32_t end = count - pos < gn ? count : pos + gn;
       const uint32_t nraw = (end - pos) * a.R;
-      for (uint32_t i = lane; i < nraw; i += 32) {
+      const uint32_t bits = ctl[CTL_BITS];
+      const uint32_t* tab = *reinterpret_cast<uint32_t* const*>(ctl + CTL_CUR);
+      const uint32_t mask0 = (1u << bits) - 1u;
+      for (uint32_t i = tid; i < nraw; i += nthr) {
         const uint32_t node = Q[pos + i / a.R];
-        kraw[i] = __ldg(a.graph + (uint64_t)node * a.R + (i % a.R));
+        const uint32_t v = __ldg(a.graph + (uint64_t)node * a.R + (i % a.R));
+        kraw[i] = v;
+        if (v != PANN_PAD) asm volatile("prefetch.global.L2 [%0];" ::"l"(tab + ref_slot(v, mask0)));
       }
       {  // the next round's rows (nodes queued so far)
         const uint32_t nend = count - end < gn ? count : end + gn;
-        for (uint32_t i = lane; i < (nend - end) * row_lines; i += 32) {
+        for (uint32_t i = tid; i < (nend - end) * row_lines; i += nthr) {
           const uint32_t node = Q[end + i / row_lines];
           asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)node * a.R + 32 * (i % row_lines)));
         }
       }
-      __syncwarp();
+      __syncthreads();
       // the neighbours in order (a row's live entries are those before PAD)
-      uint32_t nk = 0;
-      for (uint32_t b = 0; b < nraw; b += 32) {
-        const uint32_t v = b + lane < nraw ? kraw[b + lane] : PANN_PAD;
-        const bool in = v != PANN_PAD;
-        const unsigned m = __ballot_sync(FULL, in);
-        if (in) {
-          kbuf[nk + __popc(m & lt)] = v;
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(h.cur + ref_slot(v, (1u << h.bits) - 1u)));
+      const uint32_t nk = block_compact(kraw, nraw, kbuf, a.keybuf, ccnt, ctl + CTL_TOT);
+      // A call whose key the table already holds on its probe path (its home
+      // slot, then the slots after it up to the first empty one) returns true
+      // and changes nothing (hashset.h:22-24,39-44) unless the table grows
+      // first (hashset.h:25). Slots are only ever emptied by a growth, and the
+      // table cannot grow while num_entries stays at or below half its size.
+      // So the round's calls are looked up against the table as it stands;
+      // when even every call not found there inserting keeps num_entries at
+      // or below half, only those calls run, in order; otherwise all of them.
+      for (uint32_t b0 = 0; b0 < nk; b0 += nthr * HOME_BATCH) {
+        uint32_t hv[HOME_BATCH];
+#pragma unroll
+        for (int j = 0; j < HOME_BATCH; j++) {
+          const uint32_t i = b0 + nthr * j + tid;
+          hv[j] = i < nk ? tab[ref_slot(kbuf[i], mask0)] : PANN_PAD;
         }
-        nk += __popc(m);
+#pragma unroll
+        for (int j = 0; j < HOME_BATCH; j++) {
+          const uint32_t i = b0 + nthr * j + tid;
+          if (i < nk) {
+            const uint32_t key = kbuf[i];
+            uint32_t v = hv[j];
+            uint32_t p = ref_slot(key, mask0);
+            for (uint32_t s = 0; v != PANN_PAD && v != key && s < mask0; s++) {
+              p = (p + 1) & mask0;
+              v = tab[p];
+            }
+            kraw[i] = v == key ? PANN_PAD : key;
+          }
+        }
       }
-      __syncwarp();
-      // A call whose key already sits at its home slot returns true and
-      // changes nothing (hashset.h:23-24). Slots are only ever emptied by a
-      // growth, so a key found at its home now is still found there at its
-      // turn unless the table grows first, and it cannot grow while
-      // num_entries stays at or below half its size (hashset.h:25). When
-      // even the round's other calls all inserting keeps it there, only
-      // those other calls run, in order; otherwise the round runs them all.
-      const uint32_t* calls = kbuf;
-      uint32_t ncalls = nk;
-      {
-        const uint32_t mask0 = (1u << h.bits) - 1u;
+      __syncthreads();
+      // warp 0 decides; the kept calls replace kbuf only on the fast path
+      if (warp == 0) {
         uint32_t nf = 0;
-        for (uint32_t b0 = 0; b0 < nk; b0 += 32 * HOME_BATCH) {
-          uint32_t hv[HOME_BATCH];
-#pragma unroll
-          for (int j = 0; j < HOME_BATCH; j++) {
-            const uint32_t i = b0 + 32 * j + lane;
-            hv[j] = i < nk ? h.cur[ref_slot(kbuf[i], mask0)] : PANN_PAD;
+        for (uint32_t c0 = 0; c0 < nk; c0 += 32)
+          nf += __popc(__ballot_sync(FULL, c0 + lane < nk && kraw[c0 + lane] != PANN_PAD));
+        if (lane == 0) ctl[CTL_FILTERED] = h.num_entries + (long long)nf <= (long long)((1u << h.bits) / 2);
+      }
+      __syncthreads();
+      uint32_t ncalls = nk;
+      if (ctl[CTL_FILTERED]) ncalls = block_compact(kraw, nk, kbuf, a.keybuf, ccnt, ctl + CTL_TOT);
+      // the hashset calls, in order (warp 0)
+      if (warp == 0) {
+        uint32_t nun = 0;
+        bool wok = true;
+        for (uint32_t k0 = 0; k0 < ncalls && wok; k0 += 32) {
+          const bool valid = k0 + lane < ncalls;
+          const uint32_t key = valid ? kbuf[k0 + lane] : PANN_PAD;
+          bool seen = false;
+          wok = emu_batch(h, key, valid, lane, &seen);
+          const bool un = wok && valid && !seen;
+          const unsigned m = __ballot_sync(FULL, un);
+          if (un) {
+            ubuf[nun + __popc(m & lt)] = key;
+            const char* row = reinterpret_cast<const char*>(a.points + (uint64_t)key * a.stride);
+            for (uint32_t o = 0; o < a.stride; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + o));
           }
-#pragma unroll
-          for (int j = 0; j < HOME_BATCH; j++) {
-            const uint32_t i = b0 + 32 * j + lane;
-            const uint32_t key = i < nk ? kbuf[i] : PANN_PAD;
-            const bool keep = i < nk && hv[j] != key;
-            const unsigned m = __ballot_sync(FULL, keep);
-            if (keep) kraw[nf + __popc(m & lt)] = key;
-            nf += __popc(m);
-          }
+          nun += __popc(m);
         }
-        __syncwarp();
-        if (h.num_entries + (long long)nf <= (long long)((1u << h.bits) / 2)) {
-          calls = kraw;
-          ncalls = nf;
+        if (lane == 0) {
+          ctl[CTL_OK] = wok;
+          ctl[CTL_NUN] = nun;
+          ctl[CTL_BITS] = h.bits;
+          *reinterpret_cast<uint32_t**>(ctl + CTL_CUR) = h.cur;
         }
       }
-      // the hashset calls, in order
-      uint32_t nun = 0;
-      for (uint32_t k0 = 0; k0 < ncalls && ok; k0 += 32) {
-        const bool valid = k0 + lane < ncalls;
-        const uint32_t key = valid ? calls[k0 + lane] : PANN_PAD;
-        bool seen = false;
-        ok = emu_batch(h, key, valid, lane, &seen);
-        const bool un = ok && valid && !seen;
-        const unsigned m = __ballot_sync(FULL, un);
-        if (un) {
-          ubuf[nun + __popc(m & lt)] = key;
-          const char* row = reinterpret_cast<const char*>(a.points + (uint64_t)key * a.stride);
-          for (uint32_t o = 0; o < a.stride; o += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + o));
-        }
-        nun += __popc(m);
-      }
-      __syncwarp();
+      __syncthreads();
+      ok = ctl[CTL_OK] != 0;
       if (!ok) break;
+      const uint32_t nun = ctl[CTL_NUN];
       cmps += nun;
       // distances of the new neighbours; in-range ones join the queue in order
-      for (uint32_t u0 = 0; u0 < nun; u0 += 32) {
-        const bool valid = u0 + lane < nun;
-        const uint32_t id = valid ? ubuf[u0 + lane] : PANN_PAD;
-        float dd = 0.0f;
-        if (valid) dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, (int)a.d, (int)a.nchunks, qq);
-        const bool inr = valid && (double)dd <= a.radius;
-        const unsigned m = __ballot_sync(FULL, inr);
-        if (inr && count + __popc(m & lt) < a.qcap) Q[count + __popc(m & lt)] = id;
-        count += __popc(m);
+      for (uint32_t u = tid; u < nun; u += nthr) {
+        const uint32_t id = ubuf[u];
+        const float dd = point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, (int)a.d, (int)a.nchunks, qq);
+        kbuf[u] = (double)dd <= a.radius ? id : PANN_PAD;
       }
-      __syncwarp();
+      __syncthreads();
+      count += block_compact(kbuf, nun, Q + count, a.qcap - count, ccnt, ctl + CTL_TOT);
       if (count > a.qcap) ok = false;
       pos = end;
     }
 
     if (!ok) {
       // the table or the queue outgrew this tier: the next tier re-runs it
-      if (lane == 0) {
+      if (tid == 0) {
         if (a.retry) a.retry[atomicAdd(a.retry_count, 1u)] = qi;
         a.res_status[qi] |= RS_RETRY;
       }
-      __syncwarp();
       continue;
     }
-    unsigned long long off = 0;
-    if (lane == 0) off = atomicAdd(a.pool_count, (unsigned long long)count);
-    off = __shfl_sync(FULL, off, 0);
+    if (tid == 0) *reinterpret_cast<unsigned long long*>(ctl + CTL_CUR + 2) = atomicAdd(a.pool_count, (unsigned long long)count);
+    __syncthreads();
+    const unsigned long long off = *reinterpret_cast<unsigned long long*>(ctl + CTL_CUR + 2);
     if (off + count <= a.pool_cap)
-      for (uint32_t i = lane; i < count; i += 32) a.pool[off + i] = Q[i];
-    if (lane == 0) {
+      for (uint32_t i = tid; i < count; i += nthr) a.pool[off + i] = Q[i];
+    if (tid == 0) {
       a.res_off[qi] = off;
       a.res_n[qi] = count;
       a.res_cmps[qi] = cmps;
-      a.res_status[qi] = h.bits != a.bits0 ? RS_GREW : 0u;
+      a.res_status[qi] = ctl[CTL_BITS] != a.bits0 ? RS_GREW : 0u;
     }
-    __syncwarp();
   }
 }
 
@@ -294,7 +363,7 @@ static cudaError_t launch_expand_t(const RangeArgs& a, int slots, size_t smem, c
   auto k = range_expand_kernel<DT, MT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return e;
-  k<<<slots, 32, smem, st>>>(a);
+  k<<<slots, EXPAND_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -325,6 +394,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
                                  uint32_t start_point, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
                                  uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags) {
   if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points (pann_index_set_points)");
+  idx->range_held = 0;
   if (!rp) return fail(PANN_EINVAL, "range params are NULL");
   if (rp->type < PANN_RANGE_GREEDY || rp->type > PANN_RANGE_BEAM)
     return fail(PANN_EINVAL, "range type must be PANN_RANGE_GREEDY, PANN_RANGE_DOUBLING or PANN_RANGE_BEAM");
@@ -418,8 +488,8 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     while (cap0 < 22 && (uint64_t)slots0 * 4ull * (2ull * (2ull << cap0) + (1ull << (cap0 - 1))) <= (4ull << 30)) cap0++;
     cap0 = std::max(cap0, bits0 + 2);
     const Tier tiers[2] = {{cap0, cap0 - 2, 2 * idx->sm_count}, {std::max<uint32_t>(24, bits0 + 2), 22, 16}};
-    const uint32_t keybuf = std::max<uint32_t>(1024, idx->R);
-    const size_t smem = idx->stride + 12ull * keybuf;
+    const uint32_t keybuf = (std::max<uint32_t>(1024, idx->R) + 31) & ~31u;  // 8-byte aligned control words
+    const size_t smem = idx->stride + 12ull * keybuf + 4ull * (CTL_WORDS + keybuf / 32 + 2);
     unsigned long long pool_cap = std::max<unsigned long long>(1ull << 22, 256ull * h_njobs);
     for (int attempt = 0; attempt < 3; attempt++) {
       PANN_CUDA(idx->range_pool.ensure(4 * pool_cap));
@@ -513,10 +583,8 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     if (out_flags) out_flags[i] = ((h_st[i] & QS_REF_WOULD_GROW) ? 1u : 0u) | ((h_rst[i] & RS_GREW) ? 2u : 0u);
   }
   out_offsets[nq] = total;
-  if (total > ids_cap) return fail(PANN_EOVERFLOW, "range answers need " + std::to_string(total) + " ids; out_ids holds " +
-                                                       std::to_string(ids_cap));
   if (total == 0) return PANN_OK;
-  if (!out_ids) return fail(PANN_EINVAL, "out_ids is NULL");
+  if (total <= ids_cap && !out_ids) return fail(PANN_EINVAL, "out_ids is NULL");
   PANN_CUDA(idx->range_out.ensure(4 * total));
   PANN_CUDA(cudaMemcpyAsync(d_offsets, out_offsets, 8ull * (nq + 1), cudaMemcpyHostToDevice, st));
   {
@@ -526,7 +594,28 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
                                                   idx->ids.as<uint32_t>(), beam, idx->range_out.as<uint32_t>());
     PANN_CUDA(cudaGetLastError());
   }
+  if (total > ids_cap) {
+    PANN_CUDA(cudaStreamSynchronize(st));
+    idx->range_held = total;
+    return fail(PANN_EOVERFLOW, "range answers need " + std::to_string(total) + " ids; out_ids holds " +
+                                    std::to_string(ids_cap) + " (pann_range_fetch copies them)");
+  }
   PANN_CUDA(cudaMemcpyAsync(out_ids, idx->range_out.p, 4 * total, cudaMemcpyDeviceToHost, st));
   PANN_CUDA(cudaStreamSynchronize(st));
+  return PANN_OK;
+}
+
+extern "C" int pann_range_fetch(pann_index* idx, uint32_t* out_ids, uint64_t ids_cap) {
+  if (!idx) return fail(PANN_EINVAL, "index is NULL");
+  if (idx->range_held == 0) return fail(PANN_EINVAL, "no range answers are held (pann_range_fetch follows a "
+                                                     "pann_range_search that returned PANN_EOVERFLOW)");
+  const uint64_t total = idx->range_held;
+  if (ids_cap < total)
+    return fail(PANN_EOVERFLOW, "range answers need " + std::to_string(total) + " ids; out_ids holds " +
+                                    std::to_string(ids_cap));
+  if (!out_ids) return fail(PANN_EINVAL, "out_ids is NULL");
+  PANN_CUDA(cudaMemcpyAsync(out_ids, idx->range_out.p, 4 * total, cudaMemcpyDeviceToHost, idx->stream));
+  PANN_CUDA(cudaStreamSynchronize(idx->stream));
+  idx->range_held = 0;
   return PANN_OK;
 }

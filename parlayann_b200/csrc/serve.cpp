@@ -233,8 +233,7 @@ void ranger_main(pann_server* s) {
                                nullptr, nullptr);
     if (rc == PANN_EOVERFLOW && offs[nq] > ids.size()) {
       ids.resize(offs[nq]);
-      rc = pann_range_search(s->idx, qs.data(), nq, &f->rp, f->start, offs.data(), ids.data(), ids.size(), nullptr,
-                             nullptr, nullptr);
+      rc = pann_range_fetch(s->idx, ids.data(), ids.size());
     }
     std::string msg = rc ? pann_last_error() : "";
     lk.lock();

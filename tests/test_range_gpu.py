@@ -122,3 +122,37 @@ def test_range_search_edge_cases(lib_built):
     with pytest.raises(P.PannError):
         idx.range_search(q, 4, 1.0, start=600)
     idx.close()
+
+
+def test_range_fetch_returns_the_held_answers(lib_built):
+    """A call with no room for the answers (or out_ids NULL, cap 0) fills the
+    offsets and counts and leaves the answers on the device; pann_range_fetch
+    copies them, equal to a call given enough room."""
+    import ctypes
+
+    base = random_points(np.uint8, 20000, 8, 1)
+    q = random_points(np.uint8, 24, 8, 2)
+    g = O.random_graph(20000, 32, 3)
+    idx = P.Index(base, 32)
+    idx.set_graph(g)
+    radius = sample_radius(base, q, P.L2, 0.05)
+    want = idx.range_search(q, 16, radius, P.RANGE_GREEDY)
+    total = int(want["offsets"][-1])
+    assert total > len(q) * 16 * 4            # the wrapper itself went through the fetch
+    lib = P.lib()
+    rp = P.RangeParams(16, P.RANGE_GREEDY, radius, 0.0, 0)
+    offs = np.zeros(len(q) + 1, np.uint64)
+    vis = np.zeros(len(q), np.uint32)
+    ptr = lambda a: ctypes.c_void_p(a.ctypes.data)   # noqa: E731
+    rc = lib.pann_range_search(idx.handle, ptr(q), len(q), ctypes.byref(rp), 0, ptr(offs), None, 0, ptr(vis),
+                               None, None)
+    assert rc == P.PANN_EOVERFLOW
+    np.testing.assert_array_equal(offs, want["offsets"])
+    np.testing.assert_array_equal(vis, want["visited"])
+    small = np.zeros(total - 1, np.uint32)
+    assert lib.pann_range_fetch(idx.handle, ptr(small), len(small)) == P.PANN_EOVERFLOW
+    ids = np.zeros(total, np.uint32)
+    assert lib.pann_range_fetch(idx.handle, ptr(ids), total) == 0
+    np.testing.assert_array_equal(ids, np.concatenate(want["ids"]))
+    assert lib.pann_range_fetch(idx.handle, ptr(ids), total) == P.PANN_EINVAL   # taken: nothing held
+    idx.close()
