@@ -453,6 +453,28 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
                                                  "answers_identical": bool(same)}
         except Exception as ex:  # noqa: BLE001
             out["range"]["cpu_reference"] = {"failed": str(ex)}
+        # exact range groundtruth (full scan) and the range recall of check_range_recall.h:44-54
+        t0 = time.perf_counter()
+        gt_offs, gt_ids = idx.range_groundtruth(q[:nr], radius)
+        t_g = time.perf_counter() - t0
+        actual = np.diff(gt_offs).astype(np.float64)
+        nz = actual > 0
+        gt = {"queries": nr, "seconds": round(t_g, 4), "qps_e2e": round(nr / t_g, 1),
+              "recall_point": round(float(np.mean(sizes[nz] / actual[nz])), 4) if nz.any() else None,
+              "recall_cumulative": round(float(sizes.sum() / actual.sum()), 4) if actual.sum() else None}
+        try:
+            from oracle import oracle as O
+
+            if O.have_ref() and not args.no_cpu_baseline:
+                nc = 16
+                t0 = time.perf_counter()
+                ro, ri = O.range_groundtruth("ref", base, q[:nc], radius)
+                t_c = time.perf_counter() - t0
+                gt["cpu_reference"] = {"queries": nc, "qps": round(nc / t_c, 2), "tool": "compute_range_groundtruth",
+                                       "answers_identical": bool(np.array_equal(ri, gt_ids[: int(gt_offs[nc])]))}
+        except Exception as ex:  # noqa: BLE001
+            gt["cpu_reference"] = {"failed": str(ex)}
+        out["range"]["groundtruth"] = gt
     if "serving" in want:
         out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
     return out

@@ -368,6 +368,17 @@ int pann_build(pann_index* idx, const pann_build_params* bp, const uint32_t* per
 int pann_groundtruth(pann_index* idx, const void* queries, uint32_t nq, uint32_t k, uint32_t* out_ids,
                      double* out_dists);
 
+/* Exact range groundtruth by full scan (compute_range_groundtruth,
+ * data_tools/compute_range_groundtruth.cpp:14-30): answer i = every base id j,
+ * in increasing order, whose distance to query i as Point::distance computes
+ * it (a float) is <= radius (a float, as the tool's -r). Host buffers: answer
+ * i is out_ids[out_offsets[i] .. out_offsets[i+1]) (out_offsets has nq + 1
+ * entries). With too little room (out_ids NULL and ids_cap 0 to learn the
+ * size), out_offsets is filled and PANN_EOVERFLOW returned after the counting
+ * pass alone. At most 524280 queries per call. */
+int pann_range_groundtruth(pann_index* idx, const void* queries, uint32_t nq, float radius, uint64_t* out_offsets,
+                           uint32_t* out_ids, uint64_t ids_cap);
+
 /* ---------------------------------------------------------------- misc */
 
 /* Message of the last failing call on this thread ("" if none). */

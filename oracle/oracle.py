@@ -8,8 +8,10 @@ module, as the checker / the timed reference. The product never imports it.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
+import sys
 import subprocess
 
 import numpy as np
@@ -175,9 +177,23 @@ def range_search(impl, base, queries, graph, beam, radius, rtype=RANGE_GREEDY, s
     return out
 
 
+@contextlib.contextmanager
+def _stdout_to_stderr():
+    """The reference's tools print progress on stdout; keep it off a caller's stdout."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(2, 1)
+        yield
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def range_groundtruth(impl, base, queries, radius, metric=0):
     """Every base id within `radius` of each query, in id order ('oracle': pann_oracle.c; 'ref':
-    compute_range_groundtruth compiled in place). Returns (offsets[nq + 1], ids)."""
+    compute_range_groundtruth compiled in place, its progress line sent to stderr). Returns
+    (offsets[nq + 1], ids)."""
     base = np.ascontiguousarray(base)
     queries = np.ascontiguousarray(queries, dtype=base.dtype)
     n, d = base.shape
@@ -187,7 +203,8 @@ def range_groundtruth(impl, base, queries, radius, metric=0):
     cap = 0
     for _ in range(2):
         ids = np.zeros(max(cap, 1), np.uint32)
-        rc = fn(_DT[base.dtype], metric, n, d, _p(base), nq, _p(queries), radius, _p(offs), _p(ids), cap)
+        with _stdout_to_stderr():
+            rc = fn(_DT[base.dtype], metric, n, d, _p(base), nq, _p(queries), radius, _p(offs), _p(ids), cap)
         assert rc in (0, 1), rc
         if rc == 0:
             return offs, ids[: int(offs[nq])]

@@ -128,6 +128,7 @@ SIGNATURES = {
                             _P, _P, _P, _P, _I, _P]),
     "pann_range_search": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, _P, _P, _U64, _P, _P, _P]),
     "pann_range_fetch": (_I, [_P, _P, _U64]),
+    "pann_range_groundtruth": (_I, [_P, _P, _U32, ctypes.c_float, _P, _P, _U64]),
     "pann_server_create": (_I, [ctypes.POINTER(_P), _P, ctypes.POINTER(ServerOptions), _P, _U32]),
     "pann_server_submit_knn": (_I, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U64)]),
     "pann_server_submit_range": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, ctypes.POINTER(_U64)]),
@@ -367,6 +368,20 @@ class Index:
         dd = np.empty((queries.shape[0], k), np.float64)
         _check(lib().pann_groundtruth(self._h, _ptr(queries), queries.shape[0], k, _ptr(ids), _ptr(dd)))
         return ids, dd
+
+    def range_groundtruth(self, queries: np.ndarray, radius: float):
+        """Every base id within `radius` of each query, in id order (pann_range_groundtruth). Returns
+        (offsets[nq + 1], ids): answer i = ids[offsets[i]:offsets[i + 1]]."""
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        nq = queries.shape[0]
+        offs = np.zeros(nq + 1, np.uint64)
+        rc = lib().pann_range_groundtruth(self._h, _ptr(queries), nq, radius, _ptr(offs), None, 0)
+        if rc != PANN_EOVERFLOW:
+            _check(rc)
+            return offs, np.zeros(0, np.uint32)
+        ids = np.zeros(int(offs[nq]), np.uint32)
+        _check(lib().pann_range_groundtruth(self._h, _ptr(queries), nq, radius, _ptr(offs), _ptr(ids), len(ids)))
+        return offs, ids
 
 
 class Batch:

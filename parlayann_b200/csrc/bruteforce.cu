@@ -8,6 +8,7 @@
 // as a sorted list in shared memory.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -104,9 +105,134 @@ __global__ void __launch_bounds__(256) bruteforce_kernel(const uint8_t* __restri
     }
 }
 
+// Range groundtruth (compute_range_groundtruth,
+// data_tools/compute_range_groundtruth.cpp:14-30): answer i = every base id j
+// with Q[i].distance(B[j]) <= radius, in increasing j. A block of 8 warps
+// serves 8 queries against one tile of RGT_TILE base rows (the warps read the
+// tile's rows in the same order, so L1 serves seven of the eight reads). Pass
+// 0 counts each (query, tile)'s answers; pass 1, given the offsets, writes
+// them in id order. Distances are the reference's float distances.
+constexpr uint32_t RGT_TILE = 8192;
+
+template <int DT, int MT>
+__global__ void __launch_bounds__(256) range_gt_kernel(const uint8_t* __restrict__ points, uint64_t n, uint64_t stride,
+                                                       int d, int nchunks, const uint8_t* __restrict__ queries,
+                                                       uint32_t nq, float radius, uint32_t ntiles, uint32_t* counts,
+                                                       const unsigned long long* __restrict__ offs, uint32_t* out) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const unsigned FULL = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const uint32_t qi = blockIdx.y * 8 + warp;
+  if (qi >= nq) return;  // warp-uniform; no block barrier follows
+  uint8_t* qs = smem + (size_t)warp * stride;
+  stage_query<DT, MT>(qs, queries + (uint64_t)qi * stride, nchunks, lane);
+  __syncwarp();
+  int32_t qq = 0;
+  if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);
+  const uint64_t t0 = (uint64_t)blockIdx.x * RGT_TILE;
+  const uint64_t end = t0 + RGT_TILE < n ? t0 + RGT_TILE : n;
+  const uint64_t slot = (uint64_t)qi * ntiles + blockIdx.x;
+  const unsigned long long o = offs ? offs[slot] : 0ull;
+  uint32_t cnt = 0;
+  for (uint64_t j0 = t0; j0 < end; j0 += 32) {
+    const uint64_t j = j0 + (uint64_t)lane;
+    bool inr = false;
+    if (j < end) inr = point_dist<DT, MT>(points + j * stride, qs, d, nchunks, qq) <= radius;
+    const unsigned m = __ballot_sync(FULL, inr);
+    if (offs && inr) out[o + cnt + __popc(m & lt)] = (uint32_t)j;
+    cnt += __popc(m);
+  }
+  if (!offs && lane == 0) counts[slot] = cnt;
+}
+
 }  // namespace pann
 
 using namespace pann;
+
+extern "C" int pann_range_groundtruth(pann_index* idx, const void* queries, uint32_t nq, float radius,
+                                      uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap) {
+  if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points");
+  if (!out_offsets) return fail(PANN_EINVAL, "out_offsets is NULL");
+  if (nq && !queries) return fail(PANN_EINVAL, "queries is NULL");
+  out_offsets[0] = 0;
+  if (nq == 0) return PANN_OK;
+  if ((nq + 7) / 8 > 65535u) return fail(PANN_EINVAL, "at most 524280 queries per call");
+  cudaStream_t st = idx->stream;
+  const size_t rb = (size_t)idx->d * idx->esize;
+  const uint32_t ntiles = (uint32_t)((idx->n + RGT_TILE - 1) / RGT_TILE);
+  const uint64_t nslots = (uint64_t)nq * ntiles;
+  const size_t smem = 8 * idx->stride;
+  if (smem > idx->smem_optin) return fail(PANN_EINVAL, "rows too long for the range groundtruth kernel");
+  uint8_t* dq = nullptr;
+  uint32_t* dcounts = nullptr;
+  unsigned long long* doffs = nullptr;
+  uint32_t* dout = nullptr;
+  std::vector<uint32_t> counts(nslots);
+  std::vector<unsigned long long> offs(nslots);
+  uint64_t total = 0;
+  cudaError_t e = cudaMalloc(&dq, idx->stride * (size_t)nq);
+  if (e == cudaSuccess) e = cudaMalloc(&dcounts, 4 * nslots);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dq, 0, idx->stride * (size_t)nq, st);
+  if (e == cudaSuccess) e = cudaMemcpy2DAsync(dq, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st);
+  const dim3 grid(ntiles, (nq + 7) / 8);
+  auto launch = [&](const unsigned long long* o, uint32_t* out) -> cudaError_t {
+#define PANN_RGT_CASE(DT, MT)                                                                               \
+  if (idx->dtype == DT && idx->metric == MT) {                                                              \
+    auto kern = range_gt_kernel<DT, MT>;                                                                    \
+    cudaError_t fe = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max()); \
+    if (fe != cudaSuccess) return fe;                                                                       \
+    kern<<<grid, 256, smem, st>>>(idx->d_points, idx->n, idx->stride, (int)idx->d, (int)idx->nchunks, dq, nq, \
+                                  radius, ntiles, dcounts, o, out);                                          \
+    return cudaGetLastError();                                                                              \
+  }
+    PANN_RGT_CASE(DT_U8, MT_L2)
+    PANN_RGT_CASE(DT_U8, MT_IP)
+    PANN_RGT_CASE(DT_I8, MT_L2)
+    PANN_RGT_CASE(DT_I8, MT_IP)
+    PANN_RGT_CASE(DT_F32, MT_L2)
+    PANN_RGT_CASE(DT_F32, MT_IP)
+#undef PANN_RGT_CASE
+    return cudaErrorInvalidValue;
+  };
+  // pass 0: counts per (query, tile); offsets in (query, tile) order
+  if (e == cudaSuccess) e = launch(nullptr, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(counts.data(), dcounts, 4 * nslots, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    for (uint32_t i = 0; i < nq; i++) {
+      out_offsets[i] = total;
+      for (uint32_t t = 0; t < ntiles; t++) {
+        offs[(uint64_t)i * ntiles + t] = total;
+        total += counts[(uint64_t)i * ntiles + t];
+      }
+    }
+    out_offsets[nq] = total;
+  }
+  int rc = PANN_OK;
+  if (e == cudaSuccess && total > 0) {
+    if (total > ids_cap) {
+      rc = fail(PANN_EOVERFLOW, "range groundtruth needs " + std::to_string(total) + " ids; out_ids holds " +
+                                    std::to_string(ids_cap));
+    } else if (!out_ids) {
+      rc = fail(PANN_EINVAL, "out_ids is NULL");
+    } else {
+      // pass 1: the ids, in id order per query
+      e = cudaMalloc(&doffs, 8 * nslots);
+      if (e == cudaSuccess) e = cudaMalloc(&dout, 4 * total);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(doffs, offs.data(), 8 * nslots, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = launch(doffs, dout);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(out_ids, dout, 4 * total, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+  }
+  cudaFree(dq);
+  cudaFree(dcounts);
+  cudaFree(doffs);
+  cudaFree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "range groundtruth");
+  return rc;
+}
 
 extern "C" int pann_groundtruth(pann_index* idx, const void* queries, uint32_t nq, uint32_t k, uint32_t* out_ids,
                                 double* out_dists) {

@@ -94,7 +94,27 @@ def main():
         name = f"range_{np.dtype(dtype).name}_{'l2' if metric == 0 else 'mips'}"
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         cases.append(name)
+    cases += range_groundtruth_fixtures()
     print("\n".join(cases))
+
+
+def range_groundtruth_fixtures():
+    """compute_range_groundtruth (data_tools/compute_range_groundtruth.cpp:14-30), the tool's own code:
+    every base id within the radius, in id order."""
+    cases = []
+    for ci, (dtype, metric, quant) in enumerate([(np.uint8, 0, 0.02), (np.int8, 1, 0.01), (np.float32, 0, 0.03),
+                                                 (np.float32, 1, 0.02)]):
+        base = pts(dtype, 2000, 11, 900 + ci)
+        q = pts(dtype, 12, 11, 950 + ci)
+        samp = [O.olib().oracle_distance(O._DT[base.dtype], metric, 11, q[i].ctypes.data, base[j].ctypes.data)
+                for i in range(4) for j in range(0, 2000, 7)]
+        radius = np.float32(np.quantile(samp, quant))
+        offs, ids = O.range_groundtruth("ref", base, q, float(radius), metric=metric)
+        name = f"rangegt_{np.dtype(dtype).name}_{'l2' if metric == 0 else 'mips'}"
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), base=base, queries=q, radius=radius, metric=metric,
+                            offsets=offs, ids=ids)
+        cases.append(name)
+    return cases
 
 
 if __name__ == "__main__":

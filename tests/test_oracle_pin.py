@@ -178,3 +178,27 @@ def test_oracle_range_search_matches_reference(dtype, metric, lib_built):
                 np.testing.assert_array_equal(a["cmps"], b["cmps"])
                 grew += int(a["hash_grew"].sum())
     assert grew > 0   # the greedy expansion's seen-set grew somewhere
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "rangegt_*.npz"))), ids=os.path.basename)
+def test_oracle_range_groundtruth_matches_golden(path, lib_built):
+    """compute_range_groundtruth (data_tools/compute_range_groundtruth.cpp:14-30): every base id within the
+    radius, in id order, as the tool itself computed it."""
+    z = np.load(path)
+    offs, ids = O.range_groundtruth("oracle", z["base"], z["queries"], float(z["radius"]), metric=int(z["metric"]))
+    np.testing.assert_array_equal(offs, z["offsets"])
+    np.testing.assert_array_equal(ids, z["ids"])
+    assert len(ids) > 0
+
+
+@needs_ref
+@pytest.mark.parametrize("dtype,metric", [(np.uint8, 0), (np.int8, 1), (np.float32, 0), (np.float32, 1)])
+def test_oracle_range_groundtruth_matches_reference(dtype, metric, lib_built):
+    base = random_points(dtype, 3000, 9, 131)
+    q = random_points(dtype, 16, 9, 132)
+    for quant in (0.001, 0.05):
+        radius = sample_radius(base, q, metric, quant)
+        a = O.range_groundtruth("oracle", base, q, radius, metric=metric)
+        b = O.range_groundtruth("ref", base, q, radius, metric=metric)
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1], b[1])

@@ -156,3 +156,26 @@ def test_range_fetch_returns_the_held_answers(lib_built):
     np.testing.assert_array_equal(ids, np.concatenate(want["ids"]))
     assert lib.pann_range_fetch(idx.handle, ptr(ids), total) == P.PANN_EINVAL   # taken: nothing held
     idx.close()
+
+
+@pytest.mark.parametrize("dtype,metric", [(np.uint8, P.L2), (np.int8, P.MIPS), (np.float32, P.L2),
+                                          (np.float32, P.MIPS)], ids=["u8-l2", "i8-mips", "f32-l2", "f32-mips"])
+def test_range_groundtruth_matches_oracle(dtype, metric, lib_built):
+    """pann_range_groundtruth against the oracle's compute_range_groundtruth
+    (pinned to the tool itself in test_oracle_pin): the same ids in id order,
+    over several tiles of base rows and an odd dimension."""
+    base = random_points(dtype, 20000, 9, 121)
+    q = random_points(dtype, 37, 9, 122)
+    idx = P.Index(base, 8, metric)
+    for quant in (0.0005, 0.02):
+        radius = sample_radius(base, q, metric, quant)
+        offs, ids = idx.range_groundtruth(q, radius)
+        o_offs, o_ids = O.range_groundtruth("oracle", base, q, radius, metric=metric)
+        np.testing.assert_array_equal(offs, o_offs, err_msg=f"offsets quant={quant}")
+        np.testing.assert_array_equal(ids, o_ids, err_msg=f"ids quant={quant}")
+        assert len(ids) > 0
+    offs, ids = idx.range_groundtruth(q, -1e30)      # nothing in range
+    assert int(offs[-1]) == 0 and len(ids) == 0
+    offs, ids = idx.range_groundtruth(q[:0], 1.0)
+    assert offs.tolist() == [0]
+    idx.close()
