@@ -454,6 +454,7 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         except Exception as ex:  # noqa: BLE001
             out["range"]["cpu_reference"] = {"failed": str(ex)}
         # exact range groundtruth (full scan) and the range recall of check_range_recall.h:44-54
+        idx.range_groundtruth(q[:nr], radius)   # warm-up: buffers sized
         t0 = time.perf_counter()
         gt_offs, gt_ids = idx.range_groundtruth(q[:nr], radius)
         t_g = time.perf_counter() - t0

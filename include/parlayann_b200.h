@@ -238,13 +238,13 @@ int pann_range_search(pann_index* idx, const void* queries, uint32_t nq, const p
                       uint32_t start_point, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
                       uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags);
 
-/* The answers of the last pann_range_search on this index that returned
- * PANN_EOVERFLOW for want of room, into out_ids (ids_cap >= the
+/* The answers of the last pann_range_search (or pann_range_groundtruth) on
+ * this index that returned PANN_EOVERFLOW for want of room, into out_ids (ids_cap >= the
  * out_offsets[nq] that call reported), without searching again. The reference
  * sizes each answer vector as it fills (all_neighbors, rangeSearch.h:193,
  * :242-257); a caller with fixed host buffers asks for the size first and
  * fetches the held answers with this. They are held until the next
- * pann_range_search on the index; PANN_EINVAL if none are held. */
+ * range search or range groundtruth on the index; PANN_EINVAL if none are held. */
 int pann_range_fetch(pann_index* idx, uint32_t* out_ids, uint64_t ids_cap);
 
 /* ---------------------------------------------------------------- batched form */
@@ -374,8 +374,9 @@ int pann_groundtruth(pann_index* idx, const void* queries, uint32_t nq, uint32_t
  * it (a float) is <= radius (a float, as the tool's -r). Host buffers: answer
  * i is out_ids[out_offsets[i] .. out_offsets[i+1]) (out_offsets has nq + 1
  * entries). With too little room (out_ids NULL and ids_cap 0 to learn the
- * size), out_offsets is filled and PANN_EOVERFLOW returned after the counting
- * pass alone. At most 524280 queries per call. */
+ * size), out_offsets is filled, PANN_EOVERFLOW returned, and the answers stay
+ * on the device for pann_range_fetch, as after pann_range_search. At most
+ * 524280 queries per call. */
 int pann_range_groundtruth(pann_index* idx, const void* queries, uint32_t nq, float radius, uint64_t* out_offsets,
                            uint32_t* out_ids, uint64_t ids_cap);
 

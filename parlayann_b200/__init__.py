@@ -379,8 +379,8 @@ class Index:
         if rc != PANN_EOVERFLOW:
             _check(rc)
             return offs, np.zeros(0, np.uint32)
-        ids = np.zeros(int(offs[nq]), np.uint32)
-        _check(lib().pann_range_groundtruth(self._h, _ptr(queries), nq, radius, _ptr(offs), _ptr(ids), len(ids)))
+        ids = np.zeros(int(offs[nq]), np.uint32)   # the answers are held on the device
+        _check(lib().pann_range_fetch(self._h, _ptr(ids), len(ids)))
         return offs, ids
 
 

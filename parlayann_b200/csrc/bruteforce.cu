@@ -109,7 +109,9 @@ __global__ void __launch_bounds__(256) bruteforce_kernel(const uint8_t* __restri
 // data_tools/compute_range_groundtruth.cpp:14-30): answer i = every base id j
 // with Q[i].distance(B[j]) <= radius, in increasing j. A block of 8 warps
 // serves 8 queries against one tile of RGT_TILE base rows (the warps read the
-// tile's rows in the same order, so L1 serves seven of the eight reads). Pass
+// tile's rows in the same order, so L1 serves seven of the eight reads; each
+// lane scores two rows at once, opaque_zero keeping products and sums
+// unfused as the reference computes them). Pass
 // 0 counts each (query, tile)'s answers; pass 1, given the offsets, writes
 // them in id order. Distances are the reference's float distances.
 constexpr uint32_t RGT_TILE = 8192;
@@ -118,7 +120,8 @@ template <int DT, int MT>
 __global__ void __launch_bounds__(256) range_gt_kernel(const uint8_t* __restrict__ points, uint64_t n, uint64_t stride,
                                                        int d, int nchunks, const uint8_t* __restrict__ queries,
                                                        uint32_t nq, float radius, uint32_t ntiles, uint32_t* counts,
-                                                       const unsigned long long* __restrict__ offs, uint32_t* out) {
+                                                       const unsigned long long* __restrict__ offs, uint32_t* out,
+                                                       uint64_t opaque_zero) {
   extern __shared__ __align__(16) uint8_t smem[];
   const unsigned FULL = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -135,13 +138,18 @@ __global__ void __launch_bounds__(256) range_gt_kernel(const uint8_t* __restrict
   const uint64_t slot = (uint64_t)qi * ntiles + blockIdx.x;
   const unsigned long long o = offs ? offs[slot] : 0ull;
   uint32_t cnt = 0;
-  for (uint64_t j0 = t0; j0 < end; j0 += 32) {
-    const uint64_t j = j0 + (uint64_t)lane;
-    bool inr = false;
-    if (j < end) inr = point_dist<DT, MT>(points + j * stride, qs, d, nchunks, qq) <= radius;
-    const unsigned m = __ballot_sync(FULL, inr);
-    if (offs && inr) out[o + cnt + __popc(m & lt)] = (uint32_t)j;
-    cnt += __popc(m);
+  for (uint64_t j0 = t0; j0 < end; j0 += 64) {  // two rows per lane, their loads interleaved
+    const uint64_t ja = j0 + (uint64_t)lane, jb = ja + 32;
+    float da = 0.0f, db = 0.0f;
+    if (ja < end)
+      point_dist2<DT, MT>(points + ja * stride, jb < end ? points + jb * stride : nullptr, qs, nchunks, qq, da, db,
+                          opaque_zero);
+    const bool ina = ja < end && da <= radius, inb = jb < end && db <= radius;
+    const unsigned ma = __ballot_sync(FULL, ina), mb = __ballot_sync(FULL, inb);
+    if (offs && ina) out[o + cnt + __popc(ma & lt)] = (uint32_t)ja;
+    cnt += __popc(ma);
+    if (offs && inb) out[o + cnt + __popc(mb & lt)] = (uint32_t)jb;
+    cnt += __popc(mb);
   }
   if (!offs && lane == 0) counts[slot] = cnt;
 }
@@ -153,6 +161,7 @@ using namespace pann;
 extern "C" int pann_range_groundtruth(pann_index* idx, const void* queries, uint32_t nq, float radius,
                                       uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap) {
   if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points");
+  idx->range_held = 0;
   if (!out_offsets) return fail(PANN_EINVAL, "out_offsets is NULL");
   if (nq && !queries) return fail(PANN_EINVAL, "queries is NULL");
   out_offsets[0] = 0;
@@ -164,17 +173,14 @@ extern "C" int pann_range_groundtruth(pann_index* idx, const void* queries, uint
   const uint64_t nslots = (uint64_t)nq * ntiles;
   const size_t smem = 8 * idx->stride;
   if (smem > idx->smem_optin) return fail(PANN_EINVAL, "rows too long for the range groundtruth kernel");
-  uint8_t* dq = nullptr;
-  uint32_t* dcounts = nullptr;
-  unsigned long long* doffs = nullptr;
-  uint32_t* dout = nullptr;
-  std::vector<uint32_t> counts(nslots);
-  std::vector<unsigned long long> offs(nslots);
-  uint64_t total = 0;
-  cudaError_t e = cudaMalloc(&dq, idx->stride * (size_t)nq);
-  if (e == cudaSuccess) e = cudaMalloc(&dcounts, 4 * nslots);
-  if (e == cudaSuccess) e = cudaMemsetAsync(dq, 0, idx->stride * (size_t)nq, st);
-  if (e == cudaSuccess) e = cudaMemcpy2DAsync(dq, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st);
+  // the index's resident buffers: staged queries, then per (query, tile) counts and offsets
+  PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
+  PANN_CUDA(idx->range_meta.ensure(12 * nslots + 8));
+  uint8_t* dq = idx->q.as<uint8_t>();
+  unsigned long long* doffs = idx->range_meta.as<unsigned long long>();
+  uint32_t* dcounts = reinterpret_cast<uint32_t*>(doffs + nslots);
+  if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(dq, 0, idx->stride * (size_t)nq, st));
+  PANN_CUDA(cudaMemcpy2DAsync(dq, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
   const dim3 grid(ntiles, (nq + 7) / 8);
   auto launch = [&](const unsigned long long* o, uint32_t* out) -> cudaError_t {
 #define PANN_RGT_CASE(DT, MT)                                                                               \
@@ -183,7 +189,7 @@ extern "C" int pann_range_groundtruth(pann_index* idx, const void* queries, uint
     cudaError_t fe = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max()); \
     if (fe != cudaSuccess) return fe;                                                                       \
     kern<<<grid, 256, smem, st>>>(idx->d_points, idx->n, idx->stride, (int)idx->d, (int)idx->nchunks, dq, nq, \
-                                  radius, ntiles, dcounts, o, out);                                          \
+                                  radius, ntiles, dcounts, o, out, 0ull);                                    \
     return cudaGetLastError();                                                                              \
   }
     PANN_RGT_CASE(DT_U8, MT_L2)
@@ -196,42 +202,35 @@ extern "C" int pann_range_groundtruth(pann_index* idx, const void* queries, uint
     return cudaErrorInvalidValue;
   };
   // pass 0: counts per (query, tile); offsets in (query, tile) order
-  if (e == cudaSuccess) e = launch(nullptr, nullptr);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(counts.data(), dcounts, 4 * nslots, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) {
-    for (uint32_t i = 0; i < nq; i++) {
-      out_offsets[i] = total;
-      for (uint32_t t = 0; t < ntiles; t++) {
-        offs[(uint64_t)i * ntiles + t] = total;
-        total += counts[(uint64_t)i * ntiles + t];
-      }
-    }
-    out_offsets[nq] = total;
-  }
-  int rc = PANN_OK;
-  if (e == cudaSuccess && total > 0) {
-    if (total > ids_cap) {
-      rc = fail(PANN_EOVERFLOW, "range groundtruth needs " + std::to_string(total) + " ids; out_ids holds " +
-                                    std::to_string(ids_cap));
-    } else if (!out_ids) {
-      rc = fail(PANN_EINVAL, "out_ids is NULL");
-    } else {
-      // pass 1: the ids, in id order per query
-      e = cudaMalloc(&doffs, 8 * nslots);
-      if (e == cudaSuccess) e = cudaMalloc(&dout, 4 * total);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(doffs, offs.data(), 8 * nslots, cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = launch(doffs, dout);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(out_ids, dout, 4 * total, cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  std::vector<uint32_t> counts(nslots);
+  std::vector<unsigned long long> offs(nslots);
+  PANN_CUDA(launch(nullptr, nullptr));
+  PANN_CUDA(cudaMemcpyAsync(counts.data(), dcounts, 4 * nslots, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < nq; i++) {
+    out_offsets[i] = total;
+    for (uint32_t t = 0; t < ntiles; t++) {
+      offs[(uint64_t)i * ntiles + t] = total;
+      total += counts[(uint64_t)i * ntiles + t];
     }
   }
-  cudaFree(dq);
-  cudaFree(dcounts);
-  cudaFree(doffs);
-  cudaFree(dout);
-  if (e != cudaSuccess) return cuda_fail(e, "range groundtruth");
-  return rc;
+  out_offsets[nq] = total;
+  if (total == 0) return PANN_OK;
+  if (total <= ids_cap && !out_ids) return fail(PANN_EINVAL, "out_ids is NULL");
+  // pass 1: the ids, in id order per query, into the index's answer buffer
+  PANN_CUDA(idx->range_out.ensure(4 * total));
+  PANN_CUDA(cudaMemcpyAsync(doffs, offs.data(), 8 * nslots, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(launch(doffs, idx->range_out.as<uint32_t>()));
+  if (total > ids_cap) {
+    PANN_CUDA(cudaStreamSynchronize(st));
+    idx->range_held = total;
+    return fail(PANN_EOVERFLOW, "range groundtruth needs " + std::to_string(total) + " ids; out_ids holds " +
+                                    std::to_string(ids_cap) + " (pann_range_fetch copies them)");
+  }
+  PANN_CUDA(cudaMemcpyAsync(out_ids, idx->range_out.p, 4 * total, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  return PANN_OK;
 }
 
 extern "C" int pann_groundtruth(pann_index* idx, const void* queries, uint32_t nq, uint32_t k, uint32_t* out_ids,
