@@ -420,6 +420,39 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
                           "reported_distance_rel_error_vs_fp64": {"max": mx, "mean": mean}}
         b.close()
     idx.set_precision(P.PREC_F32)
+    if "precision" in want:
+        # the reference's own mixed precision: search over one-byte scalar-quantized points, float re-rank of
+        # min(k * 100, beam) frontier entries (beam_search_rerank), bit-exact with the reference's code
+        idx.set_quantized()
+        qbeam, qrec = None, None
+        for L in BEAMS:
+            if L < beam - 10:
+                continue
+            rec = P.recall_with_ties(idx.search_quantized(q, k, L).ids, gt, gd, k)
+            if rec >= 0.95:
+                qbeam, qrec = L, rec
+                break
+        if qbeam is not None:
+            rq = idx.search_quantized(q, k, qbeam)
+            t0 = time.perf_counter()
+            for _ in range(3):
+                idx.search_quantized(q, k, qbeam)
+            t_q = (time.perf_counter() - t0) / 3
+            qent = {"beam": qbeam, "rerank_factor": 100, "recall_at_10": round(qrec, 4), "qps_e2e": round(nq / t_q, 1),
+                    "slope_offset": list(idx.quant_params())}
+            try:
+                from oracle import oracle as O
+
+                if O.have_ref() and not args.no_cpu_baseline:
+                    ro = O.search_quantized("ref", base, q, idx.get_graph(), k, qbeam)
+                    qent["cpu_reference"] = {"qps": round(nq / ro["seconds"], 1),
+                                             "cores": int(O.rlib().ref_num_workers()),
+                                             "code": "beam_search_rerank over Euclidian_Point<uint8_t>",
+                                             "answers_identical": bool(np.array_equal(ro["ids"], rq.ids) and
+                                                                       np.array_equal(ro["visited"], rq.visited))}
+            except Exception as ex:  # noqa: BLE001
+                qent["cpu_reference"] = {"failed": str(ex)}
+            out["quantized_rerank"] = qent
     if prec_out:
         out["precision_batched"] = prec_out
     if "batched" in want:

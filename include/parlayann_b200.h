@@ -247,6 +247,35 @@ int pann_range_search(pann_index* idx, const void* queries, uint32_t nq, const p
  * range search or range groundtruth on the index; PANN_EINVAL if none are held. */
 int pann_range_fetch(pann_index* idx, uint32_t* out_ids, uint64_t ids_cap);
 
+/* ---------------------------------------------------------------- quantized search */
+
+/* The reference's own mixed-precision search for float Euclidian indexes: the
+ * beam search runs on one-byte scalar-quantized points and the frontier is
+ * re-ranked with float distances (beam_search_rerank, beamSearch.h:529-597,
+ * as GraphIndex::search_dispatch calls it, python/graph_index.cpp:140-160).
+ *
+ * pann_index_set_quantized builds the quantized copy as
+ * PointRange<Euclidian_Point<uint8_t>>(Points) does (euclidian_point.h:186-240):
+ * slope = 255 / (max - min) over every value with 0 included (all
+ * non-negative integers: [0, 255]), offset = round(min * slope), each value
+ * round(x * slope) - offset clamped to [0, 255]. Float Euclidean indexes only;
+ * call it again after pann_index_set_points. pann_index_quant_params returns
+ * the slope and offset. */
+int pann_index_set_quantized(pann_index* idx);
+int pann_index_quant_params(const pann_index* idx, float* slope, int32_t* offset);
+
+/* Host buffers, float queries (nq x d). The queries are quantized the same
+ * way, the search over the quantized points (QueryParams qp, exact as
+ * pann_search on a uint8 index) keeps min(k * rerank_factor, beam) frontier
+ * entries, these are re-scored with the float distance and ordered by
+ * (distance, id), and the first k written (out_ids/out_dists nq x k).
+ * out_visited / out_cmps (may be NULL) are the quantized search's counts, as
+ * QueryStats records them. PANN_ESHORT if a frontier holds fewer than k
+ * entries (the reference aborts, beamSearch.h:557-562). */
+int pann_search_quantized(pann_index* idx, const void* queries, uint32_t nq, const pann_query_params* qp,
+                          double rerank_factor, const uint32_t* starts, uint32_t n_start, uint32_t* out_ids,
+                          float* out_dists, uint32_t* out_visited, uint32_t* out_cmps);
+
 /* ---------------------------------------------------------------- batched form */
 
 /* A batch object: a reusable launch sequence for many queries whose k and beam

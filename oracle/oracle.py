@@ -65,6 +65,11 @@ def olib():
                                           _P, _P, _U64, _P, _P, _P]
         L.oracle_range_groundtruth.restype = _I
         L.oracle_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
+        L.oracle_search_quantized.restype = _I
+        L.oracle_search_quantized.argtypes = [_U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _D,
+                                              _U32, _P, _P, _P, _P]
+        L.oracle_quant_params.restype = None
+        L.oracle_quant_params.argtypes = [_U32, _U32, _P, _P, _P]
         L.oracle_distance.restype = ctypes.c_float
         L.oracle_distance.argtypes = [_I, _I, ctypes.c_uint, _P, _P]
         _olib = L
@@ -93,6 +98,9 @@ def rlib():
                                        _P, _U64, _P, _P]
         L.ref_range_groundtruth.restype = _I
         L.ref_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
+        L.ref_search_quantized.restype = _I
+        L.ref_search_quantized.argtypes = [_U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _D, _U32,
+                                           _P, _P, _P, _P, _P, _P, _P]
         L.ref_num_workers.restype = _I
         L.ref_num_workers.argtypes = []
         _rlib = L
@@ -210,6 +218,42 @@ def range_groundtruth(impl, base, queries, radius, metric=0):
             return offs, ids[: int(offs[nq])]
         cap = int(offs[nq])
     raise AssertionError("range groundtruth did not fit")
+
+
+def search_quantized(impl, base, queries, graph, k, L, rerank_factor=100.0, limit=None, degree_limit=None,
+                     batch_factor=0.125, start=0):
+    """beam_search_rerank over one-byte scalar-quantized float points with a float re-rank ('oracle':
+    pann_oracle.c; 'ref': the reference compiled in place). Returns dict(ids, dists, visited, cmps, slope,
+    offset[, seconds])."""
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    queries = np.ascontiguousarray(queries, dtype=np.float32)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    nq = queries.shape[0]
+    limit = n if limit is None else limit
+    degree_limit = R if degree_limit is None else degree_limit
+    ids = np.zeros((nq, k), np.uint32)
+    dists = np.zeros((nq, k), np.float32)
+    vis = np.zeros(nq, np.uint32)
+    cmps = np.zeros(nq, np.uint32)
+    slope = np.zeros(1, np.float32)
+    offset = np.zeros(1, np.int32)
+    out = {}
+    if impl == "oracle":
+        rc = olib().oracle_search_quantized(n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit, degree_limit,
+                                            rerank_factor, batch_factor, start, _p(ids), _p(dists), _p(vis), _p(cmps))
+        olib().oracle_quant_params(n, d, _p(base), _p(slope), _p(offset))
+    else:
+        secs = np.zeros(1, np.float64)
+        with _stdout_to_stderr():
+            rc = rlib().ref_search_quantized(n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit,
+                                             degree_limit, rerank_factor, batch_factor, start, _p(ids), _p(dists),
+                                             _p(vis), _p(cmps), _p(slope), _p(offset), _p(secs))
+        out["seconds"] = float(secs[0])
+    assert rc == 0, rc
+    out.update(ids=ids, dists=dists, visited=vis, cmps=cmps, slope=float(slope[0]), offset=int(offset[0]))
+    return out
 
 
 def robust_prune(impl, base, graph, p, cand_ids, cand_d, alpha, add=True, metric=0):

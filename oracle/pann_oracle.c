@@ -456,6 +456,91 @@ int oracle_range_search(int dtype, int metric, uint32_t n, uint32_t d, const voi
   return 0;
 }
 
+/* ------------------------------------------------------------ quantized search + re-rank */
+/* Euclidian_Point<uint8_t>::generate_parameters (euclidian_point.h:214-240):
+ * min and max over every value with 0.0 as the starting point of both; when
+ * every value is a non-negative integer, [0, 255]. parameters(min, max, d)
+ * (:104-107): slope = 255 / (max - min) in float, offset = round(min * slope). */
+void oracle_quant_params(uint32_t n, uint32_t d, const float* base, float* slope, int32_t* offset) {
+  float mn = 0.0f, mx = 0.0f;
+  int all_ints = 1;
+  for (size_t i = 0; i < (size_t)n * d; i++) {
+    const float x = base[i];
+    all_ints = all_ints && (x >= 0) && (x - (float)(long)x) == 0;
+    if (x < mn) mn = x;
+    if (x > mx) mx = x;
+  }
+  if (all_ints) {
+    if (mx < 256) mx = 255;
+    mn = 0;
+  }
+  const float s = 255.0f / (mx - mn);
+  *slope = s;
+  *offset = (int32_t)roundf(mn * s);
+}
+
+/* translate_point (euclidian_point.h:188-212): round(x * slope) - offset,
+ * clamped to [0, 255]. */
+static void quant_row(const float* x, uint32_t d, float slope, int32_t offset, uint8_t* out) {
+  for (uint32_t j = 0; j < d; j++) {
+    if (slope == 1.0f && offset == 0) { out[j] = (uint8_t)x[j]; continue; }
+    int64_t r = (int64_t)roundf(x[j] * slope) - offset;
+    if (r < 0) r = 0;
+    if (r > 255) r = 255;
+    out[j] = (uint8_t)r;
+  }
+}
+
+/* beam_search_rerank (beamSearch.h:529-597) for a float Euclidian index with
+ * one-byte quantized points, no filtering: the beam search runs on the
+ * quantized points and query; the first min(k * rerank_factor, |frontier|)
+ * frontier entries are re-scored with the float distance, sorted by
+ * (distance, id), and the first k kept. Returns -2 if the frontier holds
+ * fewer than k entries (the reference aborts). */
+int oracle_search_quantized(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
+                            const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
+                            double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids,
+                            float* out_dists, uint32_t* out_visited, uint32_t* out_cmps) {
+  float slope;
+  int32_t offset;
+  oracle_quant_params(n, d, base, &slope, &offset);
+  uint8_t* qb = (uint8_t*)malloc((size_t)n * d);
+  for (uint32_t i = 0; i < n; i++) quant_row(base + (size_t)i * d, d, slope, offset, qb + (size_t)i * d);
+  pts_t QP8 = {0, 0, d, d, qb};
+  pts_t PF = {2, 0, d, 4 * (size_t)d, (const uint8_t*)base};
+  qparams_t QP = {k, L, degree_limit, limit, batch_factor, 0.0, 0.0, 0.0};
+  uint8_t* qq = (uint8_t*)malloc(d);
+  int rc = 0;
+  for (uint32_t i = 0; i < nq && rc == 0; i++) {
+    const float* q = queries + (size_t)i * d;
+    quant_row(q, d, slope, offset, qq);
+    bs_out_t o;
+    if (beam_search_one(&QP8, graph, R, qq, EMPTY32, &start, 1, &QP, &o) != 0) { rc = -1; break; }
+    if (o.frontier_n < k) rc = -2;
+    int num_check = (int)(k * rerank_factor);
+    if ((uint32_t)num_check > o.frontier_n) num_check = (int)o.frontier_n;
+    pair_t* pts = (pair_t*)malloc(sizeof(pair_t) * (num_check > 0 ? num_check : 1));
+    for (int j = 0; j < num_check; j++) {
+      uint32_t id = o.frontier[j].id;
+      pair_t e = {id, dist(&PF, q, row(&PF, id))};
+      pts[j] = e;
+    }
+    qsort(pts, (size_t)num_check, sizeof(pair_t), cmp_pair);
+    for (uint32_t j = 0; j < k; j++) {
+      out_ids[(size_t)i * k + j] = (int)j < num_check ? pts[j].id : EMPTY32;
+      out_dists[(size_t)i * k + j] = (int)j < num_check ? pts[j].d : 0.0f;
+    }
+    out_visited[i] = o.visited_n;
+    out_cmps[i] = (uint32_t)o.cmps;
+    free(pts);
+    free(o.frontier);
+    free(o.visited);
+  }
+  free(qq);
+  free(qb);
+  return rc;
+}
+
 /* ------------------------------------------------------------ range groundtruth */
 /* compute_range_groundtruth (data_tools/compute_range_groundtruth.cpp:14-30):
  * answer i = every base id j, in increasing order, whose float distance

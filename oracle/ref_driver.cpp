@@ -17,6 +17,10 @@
 //                                        (rangeSearch.h:183-276, doublingSearch.h:50-157)
 //   ref_range_groundtruth compute_range_groundtruth() (data_tools/compute_range_groundtruth.cpp:14-30;
 //                    the tool's file is included with its main() renamed)
+//   ref_search_quantized beam_search_rerank() over one-byte scalar-quantized
+//                    points with a float re-rank, as GraphIndex::search_dispatch
+//                    calls it for float Euclidian indexes (beamSearch.h:529-597,
+//                    python/graph_index.cpp:140-160, euclidian_point.h:186-240)
 //   ref_num_workers  threads used by parallel_for
 #include <cstdint>
 #include <cstring>
@@ -244,6 +248,41 @@ int range_gt_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void
   return total > cap ? 1 : 0;
 }
 
+int quantized_t(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
+                const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
+                double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids, float* out_dists,
+                uint32_t* out_visited, uint32_t* out_cmps, float* out_slope, int32_t* out_offset, double* seconds) {
+  using Point = Euclidian_Point<float>;
+  using QPoint = Euclidian_Point<uint8_t>;
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto G = make_graph(graph, n, R);
+  PointRange<QPoint> QB(B);  // generate_parameters + translate_point per row
+  *out_slope = QB.params.slope;
+  *out_offset = QB.params.offset;
+  QueryParams QP((long)k, (long)L, (long)limit, (long)degree_limit, rerank_factor, batch_factor);
+  stats<unsigned int> QS(nq);
+  QS.clear();
+  parlay::sequence<unsigned int> starts = {start};
+  auto t0 = std::chrono::steady_clock::now();
+  parlay::parallel_for(0, nq, [&](size_t i) {
+    std::vector<uint8_t> buf(d);
+    QPoint::translate_point(buf.data(), Q[i], QB.params);
+    QPoint qq(buf.data(), (long)i, QB.params);
+    auto res = beam_search_rerank(Q[i], qq, qq, G, B, QB, QB, QS, starts, QP, true);
+    for (size_t j = 0; j < k; j++) {
+      out_ids[i * k + j] = res[j].first;
+      out_dists[i * k + j] = res[j].second;
+    }
+  });
+  *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  for (size_t i = 0; i < nq; i++) {
+    out_visited[i] = QS.visited[i];
+    out_cmps[i] = QS.distances[i];
+  }
+  return 0;
+}
+
 }  // namespace
 
 #define DISPATCH(dtype, metric, FN, ...)                                                  \
@@ -310,6 +349,15 @@ int ref_range_search(int dtype, int metric, uint32_t n, uint32_t d, const void* 
   DISPATCH(dtype, metric, range_t, n, d, base, nq, queries, R, graph, beam, start, type, radius, esr, esc,
            out_count, out_ids, cap, out_visited, out_cmps);
   return -1;
+}
+
+int ref_search_quantized(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
+                         const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
+                         double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids,
+                         float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, float* out_slope,
+                         int32_t* out_offset, double* seconds) {
+  return quantized_t(n, d, base, nq, queries, R, graph, k, L, limit, degree_limit, rerank_factor, batch_factor, start,
+                     out_ids, out_dists, out_visited, out_cmps, out_slope, out_offset, seconds);
 }
 
 int ref_range_groundtruth(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,

@@ -128,6 +128,10 @@ SIGNATURES = {
                             _P, _P, _P, _P, _I, _P]),
     "pann_range_search": (_I, [_P, _P, _U32, ctypes.POINTER(RangeParams), _U32, _P, _P, _U64, _P, _P, _P]),
     "pann_range_fetch": (_I, [_P, _P, _U64]),
+    "pann_index_set_quantized": (_I, [_P]),
+    "pann_index_quant_params": (_I, [_P, _P, _P]),
+    "pann_search_quantized": (_I, [_P, _P, _U32, ctypes.POINTER(QueryParams), ctypes.c_double, _P, _U32, _P, _P, _P,
+                                   _P]),
     "pann_range_groundtruth": (_I, [_P, _P, _U32, ctypes.c_float, _P, _P, _U64]),
     "pann_server_create": (_I, [ctypes.POINTER(_P), _P, ctypes.POINTER(ServerOptions), _P, _U32]),
     "pann_server_submit_knn": (_I, [_P, _P, _U32, _U32, _U32, ctypes.POINTER(_U64)]),
@@ -283,6 +287,33 @@ class Index:
         p = None if perm is None else np.ascontiguousarray(perm, dtype=np.uint32)
         _check(lib().pann_build(self._h, ctypes.byref(bp), _ptr(p), ctypes.byref(st)))
         return st
+
+    def set_quantized(self):
+        """One-byte scalar-quantized copy of float Euclidean points (pann_index_set_quantized)."""
+        _check(lib().pann_index_set_quantized(self._h))
+
+    def quant_params(self):
+        slope = np.zeros(1, np.float32)
+        offset = np.zeros(1, np.int32)
+        _check(lib().pann_index_quant_params(self._h, _ptr(slope), _ptr(offset)))
+        return float(slope[0]), int(offset[0])
+
+    def search_quantized(self, queries: np.ndarray, k: int, L: int, rerank_factor: float = 100.0,
+                         limit: int | None = None, degree_limit: int | None = None, batch_factor: float = 0.125,
+                         starts=(0,)) -> SearchResult:
+        """The reference's quantized search with a float re-rank (beam_search_rerank, pann_search_quantized)."""
+        queries = np.ascontiguousarray(queries, dtype=np.float32)
+        nq = queries.shape[0]
+        qp = QueryParams(k, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
+                         batch_factor)
+        st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
+        ids = np.empty((nq, k), np.uint32)
+        dists = np.empty((nq, k), np.float32)
+        vis = np.empty(nq, np.uint32)
+        cmps = np.empty(nq, np.uint32)
+        _check(lib().pann_search_quantized(self._h, _ptr(queries), nq, ctypes.byref(qp), rerank_factor, _ptr(st),
+                                           len(st), _ptr(ids), _ptr(dists), _ptr(vis), _ptr(cmps)))
+        return SearchResult(ids, dists, vis, cmps, np.zeros(nq, np.uint32))
 
     def set_precision(self, precision: int):
         """Build the low-precision copy used by the precision form (float32 indexes)."""

@@ -619,8 +619,9 @@ int pann_index_create(pann_index** out, int dtype, int metric, uint64_t n, uint3
 int pann_index_destroy(pann_index* idx) {
   if (!idx) return PANN_OK;
   if (idx->stream) cudaStreamSynchronize(idx->stream);
+  if (idx->quant) pann_index_destroy(idx->quant);
   if (idx->d_points) cudaFree(idx->d_points);
-  if (idx->d_graph) cudaFree(idx->d_graph);
+  if (idx->d_graph && !idx->graph_borrowed) cudaFree(idx->d_graph);
   for (DevBuf* b : {&idx->q, &idx->ids, &idx->dists, &idx->vis, &idx->cmps, &idx->status, &idx->redo,
                     &idx->counters, &idx->gtables, &idx->gtables2, &idx->emu, &idx->handoff, &idx->starts,
                     &idx->tmp, &idx->lp_rows, &idx->lp_scales, &idx->range_meta, &idx->range_tabs,

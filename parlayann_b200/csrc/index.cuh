@@ -70,6 +70,12 @@ struct pann_index {
   int lp_prec = 0;
   uint64_t lp_stride = 0;
   uint32_t lp_chunks = 0;
+  // quantized search: an internal uint8 Euclidean index over the one-byte
+  // quantized points that reads this index's graph (quant.cu)
+  pann_index* quant = nullptr;
+  float q_slope = 1.0f;
+  int32_t q_offset = 0;
+  bool graph_borrowed = false;  // d_graph belongs to another index
   uint32_t starts_cached_n = 0;
   uint32_t starts_cached[64] = {};
 };

@@ -25,9 +25,12 @@ python/graph_index.cpp, python/builder.cpp) over this library.
   `check_recall` (graph_index.cpp:192-300). The reference binding builds its
   QueryParams with arguments in the wrong slots (a visit limit of 1); here
   `visit_limit <= 0` means no limit (G.size()), the degree limit is the
-  graph's, and the start point is 0 as in search_dispatch. `quant=True`
-  selects the precision form (FP8 tile search with an exact float re-rank)
-  on float indexes, where the reference re-ranks from its quantized points.
+  graph's, and the start point is 0 as in search_dispatch. `quant=True` on a
+  float Euclidian index runs the reference's own quantized search
+  (pann_search_quantized: one-byte points, float re-rank of min(100 k, beam)
+  entries, as search_dispatch does); on a float mips index, whose reference
+  quantizer (Quantized_Mips_Point) is not built, it runs the precision form
+  (FP8 tile search with an exact float re-rank) instead.
 """
 from __future__ import annotations
 
@@ -168,6 +171,7 @@ class GraphIndex:
         self.index = Index(points, R, self.metric)
         self.index.load_graph(index_path)
         self._lowprec = False
+        self._quantized = False
 
     def close(self):
         self.index.close()
@@ -177,7 +181,12 @@ class GraphIndex:
         if quant and self.metric == MIPS and queries.dtype == np.float32:
             queries = _normalize(queries)   # search_dispatch normalises the query on its quantized path only
         limit = None if visit_limit is None or visit_limit <= 0 else int(visit_limit)
-        if quant and self.points.dtype == np.float32:
+        if quant and self.points.dtype == np.float32 and self.metric == L2:
+            if not self._quantized:
+                self.index.set_quantized()
+                self._quantized = True
+            r = self.index.search_quantized(queries, int(knn), int(beam_width), limit=limit)
+        elif quant and self.points.dtype == np.float32:
             if not self._lowprec:
                 self.index.set_precision(PREC_FP8)
                 self._lowprec = True

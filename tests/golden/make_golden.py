@@ -95,6 +95,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         cases.append(name)
     cases += range_groundtruth_fixtures()
+    cases += quantized_fixtures()
     print("\n".join(cases))
 
 
@@ -113,6 +114,23 @@ def range_groundtruth_fixtures():
         name = f"rangegt_{np.dtype(dtype).name}_{'l2' if metric == 0 else 'mips'}"
         np.savez_compressed(os.path.join(HERE, name + ".npz"), base=base, queries=q, radius=radius, metric=metric,
                             offsets=offs, ids=ids)
+        cases.append(name)
+    return cases
+
+
+def quantized_fixtures():
+    """beam_search_rerank over one-byte scalar-quantized float points (beamSearch.h:529-597,
+    euclidian_point.h:186-240), as GraphIndex::search_dispatch calls it."""
+    cases = []
+    for ci, (n, d, R, L, k, rf) in enumerate([(1200, 16, 12, 30, 10, 100.0), (1000, 12, 10, 20, 5, 2.0)]):
+        base = pts(np.float32, n, d, 1000 + ci)
+        q = pts(np.float32, 30, d, 1100 + ci)
+        g = O.random_graph(n, R, 1200 + ci)
+        r = O.search_quantized("ref", base, q, g, k, L, rerank_factor=rf)
+        name = f"quant_f32_{ci}"
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), base=base, queries=q, graph=g, k=k, L=L,
+                            rerank_factor=rf, ids=r["ids"], dists=r["dists"], visited=r["visited"], cmps=r["cmps"],
+                            slope=np.float32(r["slope"]), offset=np.int32(r["offset"]))
         cases.append(name)
     return cases
 

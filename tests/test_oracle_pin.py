@@ -202,3 +202,39 @@ def test_oracle_range_groundtruth_matches_reference(dtype, metric, lib_built):
         b = O.range_groundtruth("ref", base, q, radius, metric=metric)
         np.testing.assert_array_equal(a[0], b[0])
         np.testing.assert_array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "quant_*.npz"))), ids=os.path.basename)
+def test_oracle_quantized_search_matches_golden(path, lib_built):
+    """beam_search_rerank over one-byte scalar-quantized points (beamSearch.h:529-597, euclidian_point.h:186-240):
+    quantization parameters, re-ranked ids and float distances, visited and comparison counts."""
+    z = np.load(path)
+    r = O.search_quantized("oracle", z["base"], z["queries"], z["graph"], int(z["k"]), int(z["L"]),
+                           rerank_factor=float(z["rerank_factor"]))
+    assert r["slope"] == float(z["slope"]) and r["offset"] == int(z["offset"])
+    np.testing.assert_array_equal(r["ids"], z["ids"])
+    np.testing.assert_array_equal(r["dists"].view(np.uint32), z["dists"].view(np.uint32))
+    np.testing.assert_array_equal(r["visited"], z["visited"])
+    np.testing.assert_array_equal(r["cmps"], z["cmps"])
+
+
+@needs_ref
+def test_oracle_quantized_search_matches_reference(lib_built):
+    for seed, (n, d, R, L, k, rf) in enumerate([(3000, 16, 20, 40, 10, 100.0), (3000, 24, 24, 30, 5, 2.0)]):
+        base = random_points(np.float32, n, d, 140 + seed)
+        q = random_points(np.float32, 40, d, 150 + seed)
+        g = O.random_graph(n, R, 160 + seed)
+        a = O.search_quantized("oracle", base, q, g, k, L, rerank_factor=rf)
+        b = O.search_quantized("ref", base, q, g, k, L, rerank_factor=rf)
+        assert (a["slope"], a["offset"]) == (b["slope"], b["offset"])
+        for key in ("ids", "visited", "cmps"):
+            np.testing.assert_array_equal(a[key], b[key])
+        np.testing.assert_array_equal(a["dists"].view(np.uint32), b["dists"].view(np.uint32))
+    # every value a non-negative integer: the quantization is the identity
+    base = np.random.default_rng(1).integers(0, 200, (2000, 12)).astype(np.float32)
+    q = np.random.default_rng(2).integers(0, 200, (30, 12)).astype(np.float32)
+    g = O.random_graph(2000, 16, 5)
+    a = O.search_quantized("oracle", base, q, g, 5, 20)
+    b = O.search_quantized("ref", base, q, g, 5, 20)
+    assert (a["slope"], a["offset"]) == (b["slope"], b["offset"]) == (1.0, 0)
+    np.testing.assert_array_equal(a["ids"], b["ids"])

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import parlayann_b200 as P
+from conftest import random_points
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -99,3 +100,47 @@ def test_tile_search_recall_and_exact_rerank(mix_index, metric, prec, parents):
         np.testing.assert_array_equal(rb.visited[sel], p.visited)
     b.close()
     idx.set_precision(P.PREC_F32)
+
+
+@pytest.mark.parametrize("rf,k,L", [(100.0, 10, 40), (100.0, 10, 45), (2.0, 5, 30), (1.0, 8, 8), (3.0, 3, 9)])
+def test_quantized_search_matches_oracle(rf, k, L, lib_built):
+    """pann_search_quantized against the oracle's beam_search_rerank restatement (pinned to the reference):
+    the same quantization parameters, re-ranked ids, float distances bit for bit, visited and comparison
+    counts."""
+    base = random_points(np.float32, 12000, 20, 301)
+    q = random_points(np.float32, 400, 20, 302)
+    g = O.random_graph(12000, 24, 303)
+    idx = P.Index(base, 24)
+    idx.set_graph(g)
+    idx.set_quantized()
+    r = idx.search_quantized(q, k, L, rerank_factor=rf)
+    o = O.search_quantized("oracle", base, q, g, k, L, rerank_factor=rf)
+    assert idx.quant_params() == (o["slope"], o["offset"])
+    np.testing.assert_array_equal(r.ids, o["ids"])
+    np.testing.assert_array_equal(r.dists.view(np.uint32), o["dists"].view(np.uint32))
+    np.testing.assert_array_equal(r.visited, o["visited"])
+    np.testing.assert_array_equal(r.cmps, o["cmps"])
+    idx.close()
+
+
+def test_quantized_search_integer_valued_points_and_errors(lib_built):
+    rng = np.random.default_rng(311)
+    base = rng.integers(0, 256, (5000, 16)).astype(np.float32)
+    q = rng.integers(0, 256, (100, 16)).astype(np.float32)
+    g = O.random_graph(5000, 16, 312)
+    idx = P.Index(base, 16)
+    idx.set_graph(g)
+    with pytest.raises(P.PannError):
+        idx.search_quantized(q, 5, 20)                      # no quantized copy yet
+    idx.set_quantized()
+    assert idx.quant_params() == (1.0, 0)                   # the quantization is the identity
+    r = idx.search_quantized(q, 5, 20)
+    o = O.search_quantized("oracle", base, q, g, 5, 20)
+    np.testing.assert_array_equal(r.ids, o["ids"])
+    with pytest.raises(P.PannError):
+        idx.search_quantized(q, 5, 20, rerank_factor=0.5)   # fewer re-ranked entries than k
+    idx.close()
+    mips = P.Index(base, 16, P.MIPS)
+    with pytest.raises(P.PannError):
+        mips.set_quantized()                                # float Euclidean indexes only
+    mips.close()
