@@ -131,12 +131,51 @@ struct PannPoint {
   using byte = uint8_t;
   static constexpr int pann_metric = METRIC;
   static constexpr bool is_metric = METRIC == PANN_L2;
+  // slope/offset: one-byte scalar quantization (euclidian_point.h:98-108)
   struct parameters {
+    float slope;
+    int32_t offset;
     int dims;
-    parameters() : dims(0) {}
-    parameters(int d) : dims(d) {}
+    parameters() : slope(0), offset(0), dims(0) {}
+    parameters(int d) : slope(1.0f), offset(0), dims(d) {}
+    parameters(float min_val, float max_val, int d)
+        : slope(255.0f / (max_val - min_val)), offset((int32_t)std::round(min_val * slope)), dims(d) {}
     int num_bytes() const { return dims * (int)sizeof(T); }
   };
+  // generate_parameters (euclidian_point.h:214-240) for one-byte points: the
+  // minimum and maximum value with 0 included; all non-negative integers give
+  // [0, 255]
+  template <class PR>
+  static parameters generate_parameters(const PR& pr) {
+    static_assert(std::is_same<T, uint8_t>::value, "scalar quantization targets one-byte points");
+    float min_val = 0.0f, max_val = 0.0f;
+    bool all_ints = true;
+    const auto* v = pr.data();
+    for (size_t i = 0; i < pr.size() * (size_t)pr.dimension(); i++) {
+      const float x = (float)v[i];
+      all_ints = all_ints && (x >= 0) && (x - (float)(long)x) == 0;
+      min_val = std::min(min_val, x);
+      max_val = std::max(max_val, x);
+    }
+    if (all_ints) {
+      if (max_val < 256) max_val = 255;
+      min_val = 0;
+    }
+    return parameters(min_val, max_val, (int)pr.dimension());
+  }
+  // translate_point (euclidian_point.h:188-212): round(x * slope) - offset in [0, 255]
+  template <class SrcPoint>
+  static void translate_point(byte* out, const SrcPoint& p, const parameters& params) {
+    static_assert(std::is_same<T, uint8_t>::value, "scalar quantization targets one-byte points");
+    for (int j = 0; j < params.dims; j++) {
+      if (params.slope == 1.0f && params.offset == 0) {
+        out[j] = (T)p[j];
+        continue;
+      }
+      int64_t r = (int64_t)std::round((float)p[j] * params.slope) - params.offset;
+      out[j] = (T)(r < 0 ? 0 : (r > 255 ? 255 : r));
+    }
+  }
   PannPoint() : values(nullptr), id_(-1), params(0) {}
   PannPoint(byte* v, long id, parameters p) : values((T*)v), id_(id), params(p) {}
   T operator[](long i) const { return values[i]; }
@@ -184,6 +223,15 @@ struct PointRange {
   PointRange(const T* rows, size_t num, int dims) : params(dims), n(num) {
     data_ = std::make_shared<std::vector<T>>(rows, rows + num * (size_t)dims);
   }
+  // a quantized copy of another range (point_range.h:55-71): with the given
+  // parameters, or with parameters generated from that range
+  template <class PR, typename std::enable_if<!std::is_same<typename PR::T, T>::value, int>::type = 0>
+  PointRange(const PR& pr, const parameters& p) : params(p), n(pr.size()) {
+    data_ = std::make_shared<std::vector<T>>(pr.size() * (size_t)p.dims);
+    for (size_t i = 0; i < n; i++) Point::translate_point((uint8_t*)(data_->data() + i * (size_t)p.dims), pr[(long)i], p);
+  }
+  template <class PR, typename std::enable_if<!std::is_same<typename PR::T, T>::value, int>::type = 0>
+  explicit PointRange(const PR& pr) : PointRange(pr, Point::generate_parameters(pr)) {}
   size_t size() const { return n; }
   long dimension() const { return params.dims; }
   unsigned int get_dims() const { return params.dims; }
@@ -206,6 +254,7 @@ struct PannDevice {
   pann_index* idx = nullptr;
   const void* points = nullptr;
   int dtype = -1, metric = -1;
+  bool quantized = false;  // pann_index_set_quantized done on idx
   ~PannDevice() {
     if (idx) pann_index_destroy(idx);
   }
@@ -330,6 +379,7 @@ struct Graph {
       d.points = Points.data();
       d.dtype = dt;
       d.metric = mt;
+      d.quantized = false;
       dirty_->v = true;
     }
     if (dirty_->v) {
@@ -337,6 +387,16 @@ struct Graph {
       dirty_->v = false;
     }
     return d.idx;
+  }
+  // the device index with its one-byte quantized copy (pann_index_set_quantized)
+  template <class PR>
+  pann_index* device_quantized(const PR& Points) const {
+    pann_index* idx = device(Points);
+    if (!dev_->quantized) {
+      pann_check(pann_index_set_quantized(idx), "pann_index_set_quantized");
+      dev_->quantized = true;
+    }
+    return idx;
   }
   void pull_from_device() {
     pann_check(pann_graph_download(dev_->idx, (uint32_t*)rows->data()), "pann_graph_download");
@@ -490,8 +550,13 @@ std::vector<std::vector<indexType>> searchAll(PointRange_& Query_Points, Graph<i
   return pann_batch(Query_Points, G, Base_Points, QueryStats, std::vector<indexType>{starting_point}, QP, "searchAll");
 }
 
-// qsearchAll (beamSearch.h:599-646) without quantization: the three point
-// ranges must be the same (the quantized two-level search is not offered).
+// qsearchAll (beamSearch.h:599-646). Unquantized (the three point ranges the
+// same), or float Euclidian points with one-byte quantized ranges (QPR =
+// PointRange<Euclidian_Point<uint8_t>>, QQ the same range: no second level),
+// where each query runs beam_search_rerank (beamSearch.h:529-597) through
+// pann_search_quantized. The quantized ranges must carry the parameters the
+// device derives from the base points (PointRange<...>(Base_Points), and the
+// queries translated with Q_Base_Points.params).
 template <typename PR, typename QPR, typename QQPR, typename indexType>
 std::vector<std::vector<indexType>> qsearchAll(const PR& Query_Points, const QPR& Q_Query_Points,
                                                const QQPR& QQ_Query_Points, const Graph<indexType>& G,
@@ -499,6 +564,40 @@ std::vector<std::vector<indexType>> qsearchAll(const PR& Query_Points, const QPR
                                                const QQPR& QQ_Base_Points, stats<indexType>& QueryStats,
                                                const indexType starting_point, const QueryParams& QP,
                                                bool random = false) {
+  if constexpr (std::is_same<typename PR::T, float>::value && std::is_same<typename QPR::T, uint8_t>::value &&
+                PR::Point::pann_metric == PANN_L2 && QPR::Point::pann_metric == PANN_L2) {
+    if ((const void*)&QQ_Base_Points != (const void*)&Q_Base_Points || random) {
+      std::cout << "ERROR: qsearchAll supports one quantization level from a fixed start point" << std::endl;
+      std::abort();
+    }
+    (void)Q_Query_Points;
+    (void)QQ_Query_Points;
+    pann_index* idx = G.device_quantized(Base_Points);
+    float slope = 0.0f;
+    int32_t offset = 0;
+    pann_check(pann_index_quant_params(idx, &slope, &offset), "pann_index_quant_params");
+    if (slope != Q_Base_Points.params.slope || offset != Q_Base_Points.params.offset) {
+      std::cout << "ERROR: the quantized base points were not made from Base_Points" << std::endl;
+      std::abort();
+    }
+    const size_t nq = Query_Points.size(), k = (size_t)QP.k;
+    std::vector<uint32_t> ids(nq * k), vis(nq), cmps(nq);
+    std::vector<float> dists(nq * k);
+    const uint32_t start = (uint32_t)starting_point;
+    pann_query_params qp = QP.c();
+    pann_check(pann_search_quantized(idx, Query_Points.data(), (uint32_t)nq, &qp, QP.rerank_factor, &start, 1,
+                                     ids.data(), dists.data(), vis.data(), cmps.data()),
+               "qsearchAll (quantized)");
+    std::vector<std::vector<indexType>> out(nq);
+    for (size_t i = 0; i < nq; i++) {
+      out[i].assign(ids.begin() + (long)(i * k), ids.begin() + (long)((i + 1) * k));
+      if (QueryStats.visited.size() > i) {
+        QueryStats.increment_visited((indexType)i, vis[i]);
+        QueryStats.increment_dist((indexType)i, cmps[i]);
+      }
+    }
+    return out;
+  }
   if ((const void*)&Q_Base_Points != (const void*)&Base_Points ||
       (const void*)&QQ_Base_Points != (const void*)&Base_Points || random) {
     std::cout << "ERROR: qsearchAll supports the unquantized search from a fixed start point" << std::endl;

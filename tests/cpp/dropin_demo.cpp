@@ -83,5 +83,39 @@ int main(int argc, char** argv) {
     for (auto id : dr[i]) within &= Query_Points[i].distance(Points[id]) <= radius;
   double range_recall = truth_n ? (double)found / (double)truth_n : 1.0;
   std::printf("range: cumulative recall %.4f  all within radius %d\n", range_recall, (int)within);
-  return (recall >= 0.9 && same && within && range_recall >= 0.8) ? 0 : 1;
+
+  // the quantized search (ANN_Quantized's shape: float points, one-byte
+  // quantized ranges, beam_search_rerank per query inside qsearchAll)
+  const size_t nf = 8000;
+  std::vector<float> fb(nf * 24), fq(nq * 24);
+  pann_check(pann_synth_mixture(PANN_F32, nf, 24, 16, 3, 0, 0.0, 0.0, 0.3, 1, fb.data()), "synth");
+  pann_check(pann_synth_mixture(PANN_F32, nq, 24, 16, 3, 1, 0.0, 0.0, 0.3, 1, fq.data()), "synth");
+  using FPR = PointRange<Euclidian_Point<float>>;
+  using QR = PointRange<Euclidian_Point<uint8_t>>;
+  FPR FPoints(fb.data(), nf, 24), FQuery(fq.data(), nq, 24);
+  QR QBase(FPoints);                    // generate_parameters + translate_point
+  QR QQuery(FQuery, QBase.params);      // the queries with the base's parameters
+  Graph<unsigned int> GF(24, nf);
+  BuildParams FBP(24, 48, 1.2, 2);
+  knn_index<FPR, FPR, unsigned int> FI(FBP);
+  stats<unsigned int> FBS(nf);
+  FI.build_index(GF, FPoints, FPoints, FBS);
+  QueryParams FQP(10, 48, (long)nf, 24, 100, .125);
+  stats<unsigned int> QS1(nq), QS2(nq);
+  auto exact = qsearchAll(FQuery, FQuery, FQuery, GF, FPoints, FPoints, FPoints, QS1, 0u, FQP);
+  auto quant = qsearchAll(FQuery, QQuery, QQuery, GF, FPoints, QBase, QBase, QS2, 0u, FQP);
+  long qhit = 0, ehit = 0;
+  for (size_t i = 0; i < nq; i++) {
+    std::vector<std::pair<float, unsigned>> ds;
+    for (size_t j = 0; j < nf; j++) ds.push_back({FQuery[i].distance(FPoints[j]), (unsigned)j});
+    std::partial_sort(ds.begin(), ds.begin() + 10, ds.end());
+    std::set<unsigned> truth;
+    for (int t = 0; t < 10; t++) truth.insert(ds[t].second);
+    for (auto id : quant[i]) qhit += truth.count(id);
+    for (auto id : exact[i]) ehit += truth.count(id);
+  }
+  const double qrec = qhit / (10.0 * nq), erec = ehit / (10.0 * nq);
+  std::printf("quantized: slope %.4f offset %d  recall@10 %.4f (float search %.4f)\n", QBase.params.slope,
+              QBase.params.offset, qrec, erec);
+  return (recall >= 0.9 && same && within && range_recall >= 0.8 && qrec >= erec - 0.05 && qrec >= 0.8) ? 0 : 1;
 }
