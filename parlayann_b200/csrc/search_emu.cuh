@@ -491,15 +491,23 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
 
     while (ok) {
       __syncwarp();
-      int first = -1, cnt = 0;
+      int first = -1, second = -1, cnt = 0;
       for (int b = 0; b < fn; b += 32) {
         int i = b + lane;
         bool unv = (i < fn) && !(fr[i] & PANN_VFLAG);
         unsigned m = __ballot_sync(FULL, unv);
-        if (first < 0 && m) first = b + __ffs(m) - 1;
         cnt += __popc(m);
+        if (first < 0 && m) {
+          first = b + __ffs(m) - 1;
+          m &= m - 1;
+        }
+        if (first >= 0 && second < 0 && m) second = b + __ffs(m) - 1;
       }
       if (first < 0 || nvis >= a.limit) break;
+      // the next node to expand is most often the following unvisited entry:
+      // its adjacency row goes to L2 while this visit runs
+      if (second >= 0 && (uint32_t)lane * 32 < a.R)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[second]) * a.R + 32 * lane));
       if (u0_fresh) {
         u0 = key_dist(fr[first]);
         u0_fresh = false;
