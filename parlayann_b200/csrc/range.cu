@@ -140,7 +140,11 @@ __device__ __forceinline__ uint32_t block_compact(const uint32_t* tmp, uint32_t 
   return total;
 }
 
-enum : uint32_t { CTL_JOB = 0, CTL_OK, CTL_COUNT, CTL_NUN, CTL_NCALLS, CTL_FILTERED, CTL_BITS, CTL_TOT, CTL_CUR, CTL_WORDS = 16 };
+// Block control words in shared memory; CTL_CUR (the table pointer) and
+// CTL_OFF (the answer pool offset) are 64-bit, at 8-byte aligned words.
+enum : uint32_t {
+  CTL_JOB = 0, CTL_OK, CTL_COUNT, CTL_NUN, CTL_FILTERED = 5, CTL_BITS, CTL_TOT, CTL_CUR = 8, CTL_OFF = 10, CTL_WORDS = 16
+};
 
 // One block per query (EXPAND_THREADS threads). Warp 0 owns the emulated
 // hashset and makes its calls in order; every warp gathers adjacency rows,
@@ -331,9 +335,9 @@ __global__ void __launch_bounds__(EXPAND_THREADS) range_expand_kernel(RangeArgs 
       }
       continue;
     }
-    if (tid == 0) *reinterpret_cast<unsigned long long*>(ctl + CTL_CUR + 2) = atomicAdd(a.pool_count, (unsigned long long)count);
+    if (tid == 0) *reinterpret_cast<unsigned long long*>(ctl + CTL_OFF) = atomicAdd(a.pool_count, (unsigned long long)count);
     __syncthreads();
-    const unsigned long long off = *reinterpret_cast<unsigned long long*>(ctl + CTL_CUR + 2);
+    const unsigned long long off = *reinterpret_cast<unsigned long long*>(ctl + CTL_OFF);
     if (off + count <= a.pool_cap)
       for (uint32_t i = tid; i < count; i += nthr) a.pool[off + i] = Q[i];
     if (tid == 0) {
