@@ -33,8 +33,10 @@ struct TileLayout {
   uint32_t sstride;  // staged row stride (bytes)
 };
 
+// CW: candidates a step can produce (parents x degree); CWs: rows staged at
+// once (a step with more candidates stages and scores them in rounds).
 __host__ __device__ inline TileLayout tile_layout(uint32_t d, uint32_t L, uint32_t CW, uint32_t S,
-                                                  uint64_t lp_stride) {
+                                                  uint64_t lp_stride, uint32_t CWs) {
   TileLayout t{};
   size_t o = 0;
   const size_t dpad = (d + 3) & ~3u;
@@ -51,7 +53,7 @@ __host__ __device__ inline TileLayout tile_layout(uint32_t d, uint32_t L, uint32
   PANN_TILE_TAKE(cand, 8ull * (CW > L ? CW : L))
   PANN_TILE_TAKE(cid, 4ull * CW)
   PANN_TILE_TAKE(table, 4ull * S)
-  PANN_TILE_TAKE(stage, (size_t)CW * t.sstride)
+  PANN_TILE_TAKE(stage, (size_t)CWs * t.sstride)
   PANN_TILE_TAKE(misc, 64)
 #undef PANN_TILE_TAKE
   t.total = o;
@@ -133,13 +135,14 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 }
 
 template <int MT, int PREC>
-__global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t W, uint32_t S, uint32_t CW) {
+__global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t W, uint32_t S, uint32_t CW,
+                                                          uint32_t CWs) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
   const unsigned FULL = 0xFFFFFFFFu;
-  const TileLayout ly = tile_layout(a.d, a.L, CW, S, a.lp_stride);
+  const TileLayout ly = tile_layout(a.d, a.L, CW, S, a.lp_stride, CWs);
   float* qf = reinterpret_cast<float*>(smem + ly.q);
   float* sc = reinterpret_cast<float*>(smem + ly.sc);
   uint64_t* frA = reinterpret_cast<uint64_t*>(smem + ly.fr);
@@ -257,22 +260,26 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
       }
       __syncthreads();
       const uint32_t ncand = misc[1];
-      // ---- stage the tile's rows (one round trip)
-      for (uint32_t x = tid; x < ncand * a.lp_chunks; x += blockDim.x) {
-        const uint32_t r = x / a.lp_chunks, c = x - r * a.lp_chunks;
-        cp_async16(stage + (size_t)r * ly.sstride + 16 * c, a.lp_rows + (uint64_t)cid[r] * a.lp_stride + 16 * c);
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-      __syncthreads();
-      // ---- score; keep those below the cutoff of a full frontier (beamSearch.h:173-182)
       const float cutoff = fn == L ? key_dist(fr[L - 1]) : 3.40282346638528859812e+38F;
-      for (uint32_t r = tid; r < ncand; r += blockDim.x) {
-        const float dd = tile_row_dist<MT, PREC>(stage + (size_t)r * ly.sstride, qf, sc, a.d, a.lp_chunks);
-        if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[r]);
+      for (uint32_t c0 = 0; c0 < ncand; c0 += CWs) {
+        const uint32_t nr = ncand - c0 < CWs ? ncand - c0 : CWs;
+        // ---- stage the tile's rows (one round trip per CWs rows)
+        for (uint32_t x = tid; x < nr * a.lp_chunks; x += blockDim.x) {
+          const uint32_t r = x / a.lp_chunks, c = x - r * a.lp_chunks;
+          cp_async16(stage + (size_t)r * ly.sstride + 16 * c,
+                     a.lp_rows + (uint64_t)cid[c0 + r] * a.lp_stride + 16 * c);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        // ---- score; keep those below the cutoff of a full frontier (beamSearch.h:173-182)
+        for (uint32_t r = tid; r < nr; r += blockDim.x) {
+          const float dd = tile_row_dist<MT, PREC>(stage + (size_t)r * ly.sstride, qf, sc, a.d, a.lp_chunks);
+          if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[c0 + r]);
+        }
+        __syncthreads();  // the next round overwrites the staged rows
       }
       cmps += ncand;
-      __syncthreads();
       const uint32_t nc = misc[2];
       if (nc > 0) {
         // ---- merge by rank: keys are distinct (ids are), visited flags ignored in the order
@@ -334,18 +341,31 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
   }
 }
 
+// Rows staged at once: the most that still gives the best occupancy among
+// CW, 3/4 CW and 1/2 CW (steps with more new candidates stage in rounds).
 template <int MT, int PREC>
 static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W, uint32_t S, uint32_t CW,
-                         size_t smem, cudaStream_t st) {
+                         cudaStream_t st) {
   auto k = search_tile_kernel<MT, PREC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return cuda_fail(e, "tile kernel attribute");
+  uint32_t CWs = CW;
+  size_t smem = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, CW).total;
   int occ = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem);
-  if (e != cudaSuccess || occ <= 0) occ = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem) != cudaSuccess || occ <= 0) occ = 1;
+  for (uint32_t f = 3; f >= 2; f--) {
+    const uint32_t cws = std::max<uint32_t>(32, (CW * f / 4 + 15) & ~15u);
+    const size_t sm2 = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, cws).total;
+    int occ2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k, 128, sm2) == cudaSuccess && occ2 > occ) {
+      occ = occ2;
+      CWs = cws;
+      smem = sm2;
+    }
+  }
   const uint64_t want = a.nq;
   const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count));
-  k<<<blocks, 128, smem, st>>>(a, W, S, CW);
+  k<<<blocks, 128, smem, st>>>(a, W, S, CW, CWs);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "tile kernel launch");
   return PANN_OK;
@@ -359,10 +379,10 @@ int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, ui
   const uint32_t nel = std::min(plan.dl, idx->R);
   uint32_t W = std::max<uint32_t>(1, std::min<uint32_t>(parents, 4));
   const uint32_t S = tile_seen_slots(plan.L, nel, idx->R);
-  TileLayout ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride);
+  TileLayout ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, W * nel);
   while (ly.total > idx->smem_optin && W > 1) {
     W--;
-    ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride);
+    ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, W * nel);
   }
   if (ly.total > idx->smem_optin) return fail(PANN_EINVAL, "tile search state does not fit in shared memory");
   a.lp_rows = idx->lp_rows.as<uint8_t>();
@@ -373,10 +393,10 @@ int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, ui
   a.job_counter = job_counter;
   PANN_CUDA(cudaMemsetAsync(job_counter, 0, 4, st));
   const int mt = idx->metric;
-  if (mt == MT_L2 && precision == PREC_BF16) return launch_tile_t<MT_L2, PREC_BF16>(idx, a, W, S, W * nel, ly.total, st);
-  if (mt == MT_IP && precision == PREC_BF16) return launch_tile_t<MT_IP, PREC_BF16>(idx, a, W, S, W * nel, ly.total, st);
-  if (mt == MT_L2 && precision == PREC_FP8) return launch_tile_t<MT_L2, PREC_FP8>(idx, a, W, S, W * nel, ly.total, st);
-  if (mt == MT_IP && precision == PREC_FP8) return launch_tile_t<MT_IP, PREC_FP8>(idx, a, W, S, W * nel, ly.total, st);
+  if (mt == MT_L2 && precision == PREC_BF16) return launch_tile_t<MT_L2, PREC_BF16>(idx, a, W, S, W * nel, st);
+  if (mt == MT_IP && precision == PREC_BF16) return launch_tile_t<MT_IP, PREC_BF16>(idx, a, W, S, W * nel, st);
+  if (mt == MT_L2 && precision == PREC_FP8) return launch_tile_t<MT_L2, PREC_FP8>(idx, a, W, S, W * nel, st);
+  if (mt == MT_IP && precision == PREC_FP8) return launch_tile_t<MT_IP, PREC_FP8>(idx, a, W, S, W * nel, st);
   return fail(PANN_EINVAL, "the tile search needs a bfloat16 or FP8 precision");
 }
 
