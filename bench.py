@@ -380,7 +380,8 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     prec_out = {}
     exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, gd, k)
     for name, prec, parents in ((("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
-                                 ("fp8_tile2", P.PREC_FP8, 2)) if "precision" in want or "serving" in want else ()):
+                                 ("fp8_tile2", P.PREC_FP8, 2), ("fp8_tile3", P.PREC_FP8, 3))
+                                if "precision" in want or "serving" in want else ()):
         idx.set_precision(prec)
         pbeam, prec_rec, pres = None, None, None
         for L in BEAMS:
