@@ -7,8 +7,9 @@
 // gives each query a CTA and expands the `parents` best unvisited frontier
 // entries per step: their adjacency rows are read together, the new
 // neighbours (an exact shared-memory seen set) form one candidate tile whose
-// low-precision rows are staged into shared memory with cp.async in a single
-// round trip, all 128 threads score the tile (bfloat16, or FP8 E4M3 with
+// low-precision rows are staged into shared memory with cp.async, one round
+// trip per CWs rows (CWs picked at launch for occupancy), all 128 threads
+// score the tile (bfloat16, or FP8 E4M3 with
 // per-dimension scales, float32 accumulation), and the survivors are merged
 // into the sorted frontier by rank. The best `rerank` (default 4k) frontier
 // entries are re-scored with the exact float32 distance before the top k are
