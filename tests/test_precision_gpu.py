@@ -144,3 +144,25 @@ def test_quantized_search_integer_valued_points_and_errors(lib_built):
     with pytest.raises(P.PannError):
         mips.set_quantized()                                # float Euclidean indexes only
     mips.close()
+
+
+def test_quantized_search_edge_cases(lib_built):
+    """Empty batches, several start points, a visit limit and a degree limit go through the quantized search as
+    they do through beam_search_rerank."""
+    base = random_points(np.float32, 3000, 12, 321)
+    q = random_points(np.float32, 50, 12, 322)
+    g = O.random_graph(3000, 16, 323)
+    idx = P.Index(base, 16)
+    idx.set_graph(g)
+    idx.set_quantized()
+    r = idx.search_quantized(q[:0], 5, 20)
+    assert r.ids.shape == (0, 5)
+    # limit and degree limit, as QueryParams carries them into the quantized beam search
+    r = idx.search_quantized(q, 5, 20, limit=12, degree_limit=10)
+    o = O.search_quantized("oracle", base, q, g, 5, 20, limit=12, degree_limit=10)
+    np.testing.assert_array_equal(r.ids, o["ids"])
+    np.testing.assert_array_equal(r.visited, o["visited"])
+    np.testing.assert_array_equal(r.cmps, o["cmps"])
+    with pytest.raises(P.PannError):
+        idx.search_quantized(q, 21, 20)                     # k > beam
+    idx.close()

@@ -179,3 +179,23 @@ def test_range_groundtruth_matches_oracle(dtype, metric, lib_built):
     offs, ids = idx.range_groundtruth(q[:0], 1.0)
     assert offs.tolist() == [0]
     idx.close()
+
+
+def test_range_groundtruth_radius_boundary(lib_built):
+    """A point at exactly the radius is in the answer (dist <= r, compute_range_groundtruth.cpp:24)."""
+    base = random_points(np.uint8, 5000, 8, 131)
+    q = random_points(np.uint8, 4, 8, 132)
+    idx = P.Index(base, 8)
+    d = np.array([O.olib().oracle_distance(0, 0, 8, q[0].ctypes.data, base[j].ctypes.data) for j in range(5000)],
+                 np.float32)
+    radius = float(np.sort(d)[40])                         # an exact distance value
+    offs, ids = idx.range_groundtruth(q, radius)
+    o_offs, o_ids = O.range_groundtruth("oracle", base, q, radius)
+    np.testing.assert_array_equal(offs, o_offs)
+    np.testing.assert_array_equal(ids, o_ids)
+    assert int((d <= radius).sum()) == int(offs[1] - offs[0])
+    # a range search with nothing held afterwards: fetch refuses
+    idx.range_search(q[:0], 4, radius)
+    with pytest.raises(P.PannError):
+        P._check(P.lib().pann_range_fetch(idx.handle, None, 0))
+    idx.close()
