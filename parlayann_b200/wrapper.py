@@ -154,13 +154,19 @@ def build_vamana_index(metric, dtype, data_dir, index_dir, R, L, alpha, two_pass
 
 # ---------------------------------------------------------------- search
 class GraphIndex:
-    """A graph file and its points on the GPU (GraphIndex, python/graph_index.cpp:49-120)."""
+    """A graph file and its points on the GPU (GraphIndex, python/graph_index.cpp:49-120). The *Index
+    classes fix the point type and metric; GraphIndex itself takes them as keywords."""
+
+    _metric = None
+    _dtype = None
 
     def __init__(self, data_path: str, index_path: str, hnsw: bool = False, *, metric=None, dtype=None):
         if hnsw:
             raise NotImplementedError("HNSW indexes are not part of this library")
         self.metric = self._metric if metric is None else metric
         dt = self._dtype if dtype is None else dtype
+        if self.metric is None or dt is None:
+            raise ValueError("GraphIndex needs metric= and dtype= (or use one of the *Index classes)")
         points = vectors_from_file(data_path, dt)
         if self.metric == MIPS and points.dtype == np.float32:
             points, _ = _mips_prepare(points, 1.0)

@@ -62,3 +62,8 @@ def test_normalize_and_alpha_rule():
     assert W._mips_prepare(x, 1.2)[1] == 1.0                 # < 100 dimensions
     assert W._mips_prepare(random_points(np.float32, 4, 150, 6), 1.2)[1] == 0.98
     assert W._mips_prepare(random_points(np.float32, 4, 256, 7), 1.2)[1] == 1.2
+
+
+def test_graph_index_needs_a_type():
+    with pytest.raises(ValueError):
+        W.GraphIndex("points.bin", "index.graph")
