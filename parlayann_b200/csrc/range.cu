@@ -492,7 +492,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     while (cap0 < 22 && (uint64_t)slots0 * 4ull * (2ull * (2ull << cap0) + (1ull << (cap0 - 1))) <= (4ull << 30)) cap0++;
     cap0 = std::max(cap0, bits0 + 2);
     const Tier tiers[2] = {{cap0, cap0 - 2, 2 * idx->sm_count}, {std::max<uint32_t>(24, bits0 + 2), 22, 16}};
-    const uint32_t keybuf = (std::max<uint32_t>(1024, idx->R) + 31) & ~31u;  // 8-byte aligned control words
+    const uint32_t keybuf = (std::max<uint32_t>(2048, idx->R) + 31) & ~31u;  // 8-byte aligned control words
     const size_t smem = idx->stride + 12ull * keybuf + 4ull * (CTL_WORDS + keybuf / 32 + 2);
     unsigned long long pool_cap = std::max<unsigned long long>(1ull << 22, 256ull * h_njobs);
     for (int attempt = 0; attempt < 3; attempt++) {
