@@ -37,7 +37,7 @@ namespace pann {
 
 enum RangeStatus : uint32_t { RS_RETRY = 1u, RS_GREW = 2u };
 constexpr int HOME_BATCH = 8;      // table loads in flight per thread
-constexpr int EXPAND_THREADS = 128;  // one block per expansion
+constexpr int EXPAND_THREADS = 256;  // one block per expansion
 
 struct RangeArgs {
   const uint8_t* points;
