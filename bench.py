@@ -49,17 +49,38 @@ def env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
-def make_data():
-    import parlayann_b200 as P
+CONFIG = {
+    "workload": "plain beam search, 1M x 96-d f32, 10K queries, Vamana R=64 L=128 alpha=1.2 2 passes",
+    "n": W["n"], "nq": W["nq"], "d": W["d"], "k": W["k"], "data_seed": W["seed"], "components": W["comps"],
+    "graph": "Vamana R=64 L=128 alpha=1.2, two passes, prefix-doubling batches, insertion order "
+             "splitmix64(0x5EED5EED5EED + i), start point 0",
+    "beam_rule": "smallest beam of the reference's sweep list (check_nn_recall.h:214-216) with recall@10 >= 0.95 "
+                 "(checkRecall's ties) against exact FP64 groundtruth",
+    "degree_limit": W["R"], "limit": W["n"], "batch_factor": W["bf"],
+    "cache_flush": "between timed steps: a 256 MB device write (> L2) on the GPU; the reference's 5M-element "
+                   "permutation (check_nn_recall.h:45) on the host",
+}
 
-    base = P.synth_mixture(P.F32, W["n"], W["d"], W["comps"], W["seed"], 0, sigma=W["sigma"], normalize=True)
-    q = P.synth_mixture(P.F32, W["nq"], W["d"], W["comps"], W["seed"], 1, sigma=W["sigma"], normalize=True)
+
+def make_data(gen):
+    """The benchmark's base and query vectors from a seeded generator: the product's
+    pann_synth_mixture, or the same function in the in-place reference library."""
+    base = gen(2, W["n"], W["d"], W["comps"], W["seed"], 0, sigma=W["sigma"], normalize=True)
+    q = gen(2, W["nq"], W["d"], W["comps"], W["seed"], 1, sigma=W["sigma"], normalize=True)
     return base, q
+
+
+def graph_digest(g) -> str:
+    """sha1 of the graph in the reference layout (degree word + padded row, graph.h:138-145)."""
+    import hashlib
+
+    return hashlib.sha1(np.ascontiguousarray(g, dtype=np.uint32).tobytes()).hexdigest()
 
 
 class ClockSampler:
     """SM clock and throttle reasons sampled every 5 ms by a thread (NVML)
-    while the timed region runs; falls back to nvidia-smi at 200 ms."""
+    while the timed region runs; no samples (and no `clocks` key) when NVML
+    is unavailable."""
 
     HW_SLOWDOWN, SW_POWER_CAP, HW_THERMAL, SW_THERMAL = 0x8, 0x4, 0x40, 0x20
 
@@ -158,7 +179,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     dev = torch.device("cuda", local)
     lib = P.lib()
-    base, q = make_data()
+    base, q = make_data(P.synth_mixture)
     idx = P.Index(base, W["R"])
     t0 = time.time()
     build_dev = None
@@ -178,7 +199,7 @@ def run_ours(args):
     beam, recall, sweep, res = None, None, [], None
     for L in ([] if args.beam else BEAMS):
         r = idx.search(q, k, L, batch_factor=W["bf"])
-        rec = P.recall_with_ties(r.ids, gt, gd, k)
+        rec = P.recall_with_ties(r.ids, gt, k, q, base)
         sweep.append((L, round(rec, 4)))
         if rec >= 0.95:
             beam, recall, res = L, rec, r
@@ -186,7 +207,7 @@ def run_ours(args):
     if res is None:
         beam = args.beam or BEAMS[-1]
         res = idx.search(q, k, beam, batch_factor=W["bf"])
-        recall = P.recall_with_ties(res.ids, gt, gd, k)
+        recall = P.recall_with_ties(res.ids, gt, k, q, base)
     nq = q.shape[0]
     mean_vis = float(res.visited.mean())
     mean_cmps = float(res.cmps.mean())
@@ -280,7 +301,7 @@ def run_ours(args):
     if rank == 0 and not args.no_forms:
         forms = run_forms(idx, base, q, gt, gd, beam, qps, dev, flush, args)
     if rank == 0:
-        cpu = cpu_baseline(base, q, g, beam, args) if not args.no_cpu_baseline else None
+        cpu = cpu_baseline(base, q, g, beam, res, args) if not args.no_cpu_baseline else None
         line = {
             "metric": METRIC,
             "value": round(qps, 1),
@@ -294,13 +315,13 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded 256-component Gaussian mixture, L2-normalised)",
-            "config": {"workload": "plain beam search, 1M x 96-d f32, 10K queries, Vamana R=64 L=128 alpha=1.2 2 passes",
-                       "n": W["n"], "nq": nq, "d": W["d"], "k": k, "beam": beam, "recall_at_10": round(recall, 4),
-                       "degree_limit": W["R"], "batch_factor": W["bf"], "l2_flush": "256 MB write between steps",
-                       "parallelism": f"replicas x{world}", "build_seconds_device": build_dev,
-                       "build_seconds_wall": round(build_wall, 3), "mean_visited": round(mean_vis, 2),
-                       "mean_cmps": round(mean_cmps, 2), "flagged_queries": int(res.flags.sum()),
-                       "recall_sweep": sweep},
+            "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+            "details": {"beam": beam, "recall_at_10": round(recall, 4), "recall_sweep": sweep,
+                        "graph_sha1": graph_digest(g), "mean_degree": round(avg_deg, 3),
+                        "build_seconds_device": build_dev, "build_seconds_wall": round(build_wall, 3),
+                        "mean_visited": round(mean_vis, 2), "mean_cmps": round(mean_cmps, 2),
+                        "flagged_queries": int(res.flags.sum()),
+                        "groundtruth": "pann_groundtruth (GPU, FP64 distances, ties by id), 20 per query"},
             "e2e": {"value": round(replica_qps(nq, args.steps, world, t_e2e), 1), "unit": "queries/s",
                     "h2d_bytes_per_step": int(q.nbytes),
                     "d2h_bytes_per_step": int(nq * k * 8 + nq * 12)},
@@ -378,7 +399,7 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     want = set(args.forms.split(","))
     # ---- precision form (+ batched): smallest beam with recall >= 0.95, device QPS through a batch object
     prec_out = {}
-    exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, gd, k)
+    exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, k, q, base)
     for name, prec, parents in ((("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
                                  ("fp8_tile2", P.PREC_FP8, 2), ("fp8_tile3", P.PREC_FP8, 3))
                                 if "precision" in want or "serving" in want else ()):
@@ -388,14 +409,14 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
             if L < beam - 10:
                 continue
             r = idx.search(q, k, L, precision=prec, parents=parents)
-            rec = P.recall_with_ties(r.ids, gt, gd, k)
+            rec = P.recall_with_ties(r.ids, gt, k, q, base)
             if rec >= 0.95:
                 pbeam, prec_rec, pres = L, rec, r
                 break
         if pbeam is None:
             continue
         same_beam = idx.search(q, k, beam, precision=prec, parents=parents)
-        loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, gd, k)
+        loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, k, q, base)
         b = idx.batch(nq, k, pbeam, precision=prec, parents=parents)
         d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
         d_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
@@ -429,7 +450,7 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         for L in BEAMS:
             if L < beam - 10:
                 continue
-            rec = P.recall_with_ties(idx.search_quantized(q, k, L).ids, gt, gd, k)
+            rec = P.recall_with_ties(idx.search_quantized(q, k, L).ids, gt, k, q, base)
             if rec >= 0.95:
                 qbeam, qrec = L, rec
                 break
@@ -633,26 +654,38 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
             "slots": 3, "batch_queries": 4096, "forms": serving}
 
 
-def cpu_baseline(base, q, graph, beam, args):
+def cpu_baseline(base, q, graph, beam, res, args):
     """The reference's qsearchAll (compiled in place) on the host cores, as a
-    reported baseline: a bounded sample of the same workload."""
+    reported baseline, on the same graph, queries and beam as the GPU line; its
+    answers are compared with the GPU's query by query: ids in order, the float
+    distance bits, visited counts and distance comparisons."""
     try:
         from oracle import oracle as O
 
         if not O.have_ref():
             return None
         nq = min(q.shape[0], args.cpu_queries)
-        secs, ids, vis, cmps = O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        secs, ids, vis, cmps, dists = O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        diff = ((ids != res.ids[:nq]).any(1) | (dists.view(np.uint32) != res.dists[:nq].view(np.uint32)).any(1) |
+                (vis != res.visited[:nq]) | (cmps != res.cmps[:nq]))
         return {"value": round(nq / secs, 1), "unit": "queries/s", "cores": int(O.rlib().ref_num_workers()),
                 "kind": "reference",
                 "sample": f"{nq} of the {q.shape[0]} queries, one qsearchAll pass after a cache flush "
-                          f"({secs:.2f} s), same graph and beam {beam}"}
+                          f"({secs:.2f} s), same graph and beam {beam}",
+                "answers_identical": bool(not diff.any()), "queries_compared": int(nq),
+                "queries_differing": int(diff.sum()),
+                "compared": "ids in order, float32 distance bits, visited count, distance comparisons"}
     except Exception as ex:  # noqa: BLE001
         return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
 
 def run_reference(args):
-    """--impl reference: the reference's own build_index and qsearchAll on the host cores."""
+    """--impl reference: the reference's own code on the host cores, end to end:
+    its build_index builds the graph, its checkRecall (recall with the
+    groundtruth's ties, FP64 groundtruth computed on the host) picks the
+    smallest beam of its sweep list with recall@10 >= 0.95, and its qsearchAll
+    is timed there. Only the in-place reference library is loaded (it also
+    generates the data)."""
     rank, world, _ = env_rank()
     if rank != 0:
         return None
@@ -660,28 +693,35 @@ def run_reference(args):
 
     if not O.have_ref():
         return {"impl": "reference", "unavailable": "oracle/_ref/libpann_ref.so was not built (reference checkout absent at build time)"}
-    base, q = make_data()
+    base, q = make_data(O.synth_mixture)
     t0 = time.time()
     graph, _ = O.build_graph("ref", base, W["R"], W["Lb"], W["alpha"], W["passes"], batch_factor=W["bf"])
     build_s = time.time() - t0
-    beam = args.beam or 45
+    t0 = time.time()
+    gt, gd = O.groundtruth_fast(base, q, 20)
+    gt_s = time.time() - t0
+    k = W["k"]
     nq = min(q.shape[0], args.cpu_queries)
+    sweep, beam, rec = [], None, None
+    with tempfile.TemporaryDirectory() as tmp:
+        gt_path = os.path.join(tmp, "gt.ibin")
+        O.write_ibin(gt_path, gt[:nq], gd[:nq])
+        for L in ([args.beam] if args.beam else BEAMS):
+            r = O.check_recall(base, q[:nq], graph, gt_path, k, L, batch_factor=W["bf"])
+            sweep.append((L, round(r["recall"], 4)))
+            if r["recall"] >= 0.95 or args.beam:
+                beam, rec = L, r
+                break
+    if beam is None:
+        beam, rec = BEAMS[-1], {"recall": sweep[-1][1]}
     for _ in range(args.warmup):
-        O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        O.qsearch_time(base, q[:nq], graph, k, beam, batch_factor=W["bf"])
     times = []
-    ids = None
     for _ in range(args.steps):
-        secs, ids, vis, cmps = O.qsearch_time(base, q[:nq], graph, W["k"], beam, batch_factor=W["bf"])
+        secs, ids, vis, cmps, _d = O.qsearch_time(base, q[:nq], graph, k, beam, batch_factor=W["bf"])
         times.append(secs)
     t = sum(times)
     qps = nq * args.steps / t
-    # recall on a query subsample against FP64 brute force (numpy, float64)
-    sub = min(200, nq)
-    qq = q[:sub].astype(np.float64)
-    bb = base.astype(np.float64)
-    d2 = (qq * qq).sum(1)[:, None] + (bb * bb).sum(1)[None, :] - 2.0 * qq @ bb.T
-    gt = np.argsort(d2, axis=1, kind="stable")[:, :10]
-    rec = float(np.mean([len(set(ids[i].tolist()) & set(gt[i].tolist())) / 10.0 for i in range(sub)]))
     cores = int(O.rlib().ref_num_workers())
     return {
         "impl": "reference",
@@ -697,10 +737,13 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded 256-component Gaussian mixture, L2-normalised)",
-        "config": {"workload": "plain beam search, 1M x 96-d f32, 10K queries, Vamana R=64 L=128 alpha=1.2 2 passes",
-                   "n": W["n"], "nq": nq, "d": W["d"], "k": W["k"], "beam": beam,
-                   "recall_at_10_sample": round(rec, 4), "build_seconds_cpu": round(build_s, 2),
-                   "parallelism": "host threads"},
+        "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+        "details": {"beam": beam, "recall_at_10": round(float(rec["recall"]), 4), "recall_sweep": sweep,
+                    "graph_sha1": graph_digest(graph), "build_seconds_cpu": round(build_s, 2),
+                    "mean_visited": round(float(vis.mean()), 2), "mean_cmps": round(float(cmps.mean()), 2),
+                    "groundtruth": f"FP64 on the host cores (float32 candidate pass + FP64 re-rank, {gt_s:.1f} s), "
+                                   "20 per query; recall by the reference's checkRecall",
+                    "ranks_run": 1},
         "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": cores, "kind": "reference",
                          "sample": f"{nq} queries per step (qsearchAll after a cache flush, check_nn_recall.h:46-59)"},
         "e2e": {"value": round(qps, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

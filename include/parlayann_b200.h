@@ -141,10 +141,15 @@ int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, cons
  * routine. A call whose working set does not fit (too many queries, or a
  * beam and degree limit whose seen tables are too large) returns PANN_EINVAL
  * with a message giving the bytes needed; split the batch.
- *  - The first call on each device looks up the array's device address
- *    (which may load the module that holds it) with that device current;
- *    make that first call before any stream capture. The index's device must
- *    be the current device.
+ *  - Every call looks up the array's device address with the index's device
+ *    current (the first lookup on a device may load the module that holds
+ *    it; make that first call before any stream capture). The address is
+ *    not cached, so after a device reset the next call uses the new
+ *    context's array. The index's device must be the current device.
+ *  - starts is a HOST array copied with cudaMemcpyAsync on `stream`: from
+ *    pageable memory the copy is staged before the call returns; from
+ *    page-locked memory it is not, so keep the array unchanged until the
+ *    stream has reached this call.
  *  - Every call shares the array and finds the previous call's contents in
  *    it; each call clears what must start at zero. Calls that overlap on the
  *    GPU (on different streams, or for different indexes on one device) race

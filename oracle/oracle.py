@@ -88,7 +88,12 @@ def rlib():
         L.ref_search.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _U32, _P, _P,
                                  _P, _P, _P, _P, _P, _P, _U32, _P, _P]
         L.ref_qsearch_time.restype = _D
-        L.ref_qsearch_time.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _D, _P, _P, _P]
+        L.ref_qsearch_time.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _D, _P, _P, _P, _P]
+        L.ref_check_recall.restype = _I
+        L.ref_check_recall.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _P, ctypes.c_char_p, _U32, _U32, _U64,
+                                       _U32, _D, _P]
+        L.ref_synth_mixture.restype = _I
+        L.ref_synth_mixture.argtypes = [_I, _U64, _U32, _U32, _U64, _U32, _D, _D, _D, _I, _P]
         L.ref_robust_prune.restype = _I
         L.ref_robust_prune.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, _U32, _U32, _P, _P, _D, _I, _P, _P, _P]
         L.ref_build.restype = _I
@@ -308,6 +313,66 @@ def groundtruth(base, queries, k, metric=0):
     return ids, dd
 
 
+def groundtruth_fast(base, queries, k, metric=0, cand=None, chunk=256, threads=None):
+    """Exact top-k by FP64 distance (ties by id), for float32 points, on the host cores: a float32
+    pass (torch CPU matmul of the |q|^2 + |b|^2 - 2 q.b expansion) keeps the `cand` best candidates
+    per query; their FP64 distances give the answer. The float32 distance of every point is within
+    `bound` of its FP64 distance (a forward error bound of the expansion), so when the cand-th
+    float32 distance exceeds the k-th by more than 2 bound the candidates hold every true top-k
+    point; a query where it does not is recomputed in FP64 over all points. metric 1 = mips
+    (distance -q.b). Returns (ids uint32, dists float64)."""
+    import torch
+
+    base = np.ascontiguousarray(base, dtype=np.float32)
+    queries = np.ascontiguousarray(queries, dtype=np.float32)
+    n, d = base.shape
+    nq = queries.shape[0]
+    cand = min(n, cand or max(4 * k, 64))
+    if threads:
+        torch.set_num_threads(threads)
+    B = torch.from_numpy(base)
+    b64 = base.astype(np.float64)
+    bn = (b64 * b64).sum(1)
+    bn32 = torch.from_numpy(bn.astype(np.float32))
+    bmax = float(np.sqrt(bn.max()))
+    ids = np.zeros((nq, k), np.uint32)
+    dd = np.zeros((nq, k), np.float64)
+    u = 2.0 ** -23
+    for s in range(0, nq, chunk):
+        q = queries[s:s + chunk]
+        Q = torch.from_numpy(q)
+        if metric == 0:
+            D = torch.addmm(bn32[None, :], Q, B.t(), beta=1.0, alpha=-2.0)
+        else:
+            D = -(Q @ B.t())
+        top = torch.topk(D, cand, dim=1, largest=False, sorted=True)
+        tv = top.values.numpy().astype(np.float64)
+        ti = top.indices.numpy()
+        q64 = q.astype(np.float64)
+        qn = np.sqrt((q64 * q64).sum(1))
+        # |error| of a float32 dot of length d is <= d u sum|q_t b_t| <= d u |q||b|; the norms add less
+        bound = (d + 8) * u * (qn * bmax + (qn * qn + bmax * bmax if metric == 0 else 0.0)) * 2.0
+        for j in range(q.shape[0]):
+            if cand < n and not (tv[j, cand - 1] - tv[j, k - 1] > 2.0 * bound[j]):
+                c = np.arange(n)
+            else:
+                c = ti[j]
+            rows = b64[c]
+            dj = ((rows - q64[j]) ** 2).sum(1) if metric == 0 else -(rows @ q64[j])
+            o = np.lexsort((c, dj))[:k]
+            ids[s + j] = c[o]
+            dd[s + j] = dj[o]
+    return ids, dd
+
+
+def write_ibin(path, ids, dists):
+    """groundTruth's .ibin file (types.h:48-73): int32 n, int32 k, int32 ids[n k], float dists[n k]."""
+    with open(path, "wb") as fh:
+        np.array(ids.shape, np.int32).tofile(fh)
+        np.ascontiguousarray(ids, dtype=np.int32).tofile(fh)
+        np.ascontiguousarray(dists, dtype=np.float32).tofile(fh)
+
+
 def permutation(n, seed=0x5EED5EED5EED):
     out = np.zeros(n, np.uint32)
     olib().oracle_permutation(n, seed, _p(out))
@@ -323,7 +388,9 @@ def batch_schedule(n, m=None):
 
 
 def qsearch_time(base, queries, graph, k, L, batch_factor=0.125, metric=0):
-    """The reference's qsearchAll timed as checkRecall times it (check_nn_recall.h:46-59)."""
+    """The reference's qsearchAll timed as checkRecall times it (check_nn_recall.h:46-59). Returns
+    (seconds, ids, visited, comparisons, distances); the distances of the returned ids come from the
+    reference's Point::distance, outside the timed region."""
     base = np.ascontiguousarray(base)
     queries = np.ascontiguousarray(queries, dtype=base.dtype)
     graph = np.ascontiguousarray(graph, dtype=np.uint32)
@@ -331,11 +398,39 @@ def qsearch_time(base, queries, graph, k, L, batch_factor=0.125, metric=0):
     R = graph.shape[1] - 1
     nq = queries.shape[0]
     ids = np.zeros((nq, k), np.uint32)
+    dists = np.zeros((nq, k), np.float32)
     vis = np.zeros(nq, np.uint32)
     cmps = np.zeros(nq, np.uint32)
     secs = rlib().ref_qsearch_time(_DT[base.dtype], metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L,
-                                   batch_factor, _p(ids), _p(vis), _p(cmps))
-    return secs, ids, vis, cmps
+                                   batch_factor, _p(ids), _p(vis), _p(cmps), _p(dists))
+    return secs, ids, vis, cmps, dists
+
+
+def check_recall(base, queries, graph, gt_path, k, L, limit=None, degree_limit=None, batch_factor=0.125, metric=0):
+    """The reference's checkRecall (check_nn_recall.h:17-128) over a groundtruth .ibin file: returns
+    dict(recall, qps, avg_cmps, tail_cmps, avg_visited, tail_visited)."""
+    base = np.ascontiguousarray(base)
+    queries = np.ascontiguousarray(queries, dtype=base.dtype)
+    graph = np.ascontiguousarray(graph, dtype=np.uint32)
+    n, d = base.shape
+    R = graph.shape[1] - 1
+    out = np.zeros(6, np.float64)
+    with _stdout_to_stderr():
+        rc = rlib().ref_check_recall(_DT[base.dtype], metric, n, d, _p(base), queries.shape[0], _p(queries), R,
+                                     _p(graph), os.fsencode(gt_path), k, L, n if limit is None else limit,
+                                     R if degree_limit is None else degree_limit, batch_factor, _p(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_check_recall failed ({rc})")
+    return dict(zip(("recall", "qps", "avg_cmps", "tail_cmps", "avg_visited", "tail_visited"), out.tolist()))
+
+
+def synth_mixture(dtype, n, d, components, seed, stream, lo=32.0, hi=224.0, sigma=20.0, normalize=False):
+    """The seeded Gaussian-mixture rows, generated by the in-place reference library (the same values
+    as the product's pann_synth_mixture; a reference run loads no other library)."""
+    out = np.empty((n, d), dtype=np.uint8 if dtype == 0 else np.float32)
+    if rlib().ref_synth_mixture(dtype, n, d, components, seed, stream, lo, hi, sigma, int(normalize), _p(out)) != 0:
+        raise ValueError("ref_synth_mixture: bad arguments")
+    return out
 
 
 def random_graph(n, R, seed, min_deg=1):

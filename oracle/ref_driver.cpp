@@ -21,10 +21,20 @@
 //                    points with a float re-rank, as GraphIndex::search_dispatch
 //                    calls it for float Euclidian indexes (beamSearch.h:529-597,
 //                    python/graph_index.cpp:140-160, euclidian_point.h:186-240)
+//   ref_check_recall checkRecall() itself on a groundtruth .ibin file
+//                    (check_nn_recall.h:17-128): recall with the groundtruth's
+//                    ties at the k-th distance, QPS, mean visited / comparisons
+//   ref_synth_mixture the seeded Gaussian-mixture generator of the data the
+//                    benchmark and tests use (the same function of (seed,
+//                    stream, row, dim) as the product's pann_synth_mixture), so
+//                    a reference run needs no other library
 //   ref_num_workers  threads used by parallel_for
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <chrono>
+#include <thread>
+#include <vector>
 
 #include "utils/euclidian_point.h"
 #include "utils/mips_point.h"
@@ -35,6 +45,7 @@
 #include "vamana/index.h"
 #include "utils/rangeSearch.h"
 #include "utils/doublingSearch.h"
+#include "utils/check_nn_recall.h"
 
 #define main pann_ref_range_groundtruth_tool_main
 #include "../data_tools/compute_range_groundtruth.cpp"
@@ -131,7 +142,7 @@ template <typename Point>
 double qsearch_time_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries,
                       uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L,
                       double batch_factor, uint32_t* out_ids, uint32_t* out_visited,
-                      uint32_t* out_cmps) {
+                      uint32_t* out_cmps, float* out_dists) {
   using PR = PointRange<Point>;
   auto B = make_points<Point>(base, n, d);
   auto Q = make_points<Point>(queries, nq, d);
@@ -150,7 +161,48 @@ double qsearch_time_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, con
     out_visited[i] = QueryStats.visited[i];
     out_cmps[i] = QueryStats.distances[i];
   }
+  // outside the timed region: the reference's distance of each returned id
+  if (out_dists)
+    parlay::parallel_for(0, (long)nq, [&](long i) {
+      for (uint32_t j = 0; j < k; j++) out_dists[(size_t)i * k + j] = Q[i].distance(B[all[i][j]]);
+    });
   return std::chrono::duration<double>(t1 - t0).count();
+}
+
+template <typename Point>
+int check_recall_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void* queries, uint32_t R,
+                   const uint32_t* graph, const char* gt_path, uint32_t k, uint32_t L, uint64_t limit,
+                   uint32_t degree_limit, double batch_factor, double* out) {
+  using PR = PointRange<Point>;
+  auto B = make_points<Point>(base, n, d);
+  auto Q = make_points<Point>(queries, nq, d);
+  auto G = make_graph(graph, n, R);
+  groundTruth<unsigned int> GT(const_cast<char*>(gt_path));
+  QueryParams QP((long)k, (long)L, (long)limit, (long)degree_limit, 100.0, batch_factor);
+  nn_result r = checkRecall<PR, PR, PR, unsigned int>(G, B, Q, B, Q, B, Q, GT, false, 0, (long)k, QP, false);
+  out[0] = r.recall;
+  out[1] = r.QPS;
+  out[2] = r.avg_cmps;
+  out[3] = r.tail_cmps;
+  out[4] = r.avg_visited;
+  out[5] = r.tail_visited;
+  return 0;
+}
+
+// Data generator (see ref_synth_mixture below).
+inline uint64_t sm_mix(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ULL;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+  return x ^ (x >> 31);
+}
+inline uint64_t sm_key(uint64_t seed, uint64_t stream, uint64_t a, uint64_t b) {
+  return sm_mix(sm_mix(sm_mix(seed ^ (stream << 56)) + a) + b);
+}
+inline double sm_unif(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+inline double sm_normal(uint64_t h1, uint64_t h2) {
+  const double r = std::sqrt(-2.0 * std::log(1.0 - sm_unif(h1)));
+  return r * std::cos(6.283185307179586476925286766559 * sm_unif(h2));
 }
 
 template <typename Point>
@@ -319,10 +371,68 @@ int ref_search(int dtype, int metric, uint32_t n, uint32_t d, const void* base, 
 double ref_qsearch_time(int dtype, int metric, uint32_t n, uint32_t d, const void* base,
                         uint32_t nq, const void* queries, uint32_t R, const uint32_t* graph,
                         uint32_t k, uint32_t L, double batch_factor, uint32_t* out_ids,
-                        uint32_t* out_visited, uint32_t* out_cmps) {
+                        uint32_t* out_visited, uint32_t* out_cmps, float* out_dists) {
   DISPATCH(dtype, metric, qsearch_time_t, n, d, base, nq, queries, R, graph, k, L, batch_factor,
-           out_ids, out_visited, out_cmps);
+           out_ids, out_visited, out_cmps, out_dists);
   return -1.0;
+}
+
+// out: recall, QPS, mean and p99 comparisons, mean and p99 visited (nn_result)
+int ref_check_recall(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,
+                     const void* queries, uint32_t R, const uint32_t* graph, const char* gt_path, uint32_t k,
+                     uint32_t L, uint64_t limit, uint32_t degree_limit, double batch_factor, double* out) {
+  DISPATCH(dtype, metric, check_recall_t, n, d, base, nq, queries, R, graph, gt_path, k, L, limit, degree_limit,
+           batch_factor, out);
+  return -1;
+}
+
+// Seeded Gaussian mixture, every value a function of (seed, stream, row, dim)
+// through a splitmix64 chain: uint8 centres uniform in [lo, hi], float centres
+// N(0,1); the row's component is a hash of (seed, 2 + 2 stream, row) modulo
+// the component count; the noise is N(0,1) (Box-Muller on two hashes of
+// (seed, 3 + 2 stream, row, 2t / 2t+1)) times sigma; uint8 values are
+// rounded half away from zero and clipped to [0, 255]; float rows are
+// optionally L2-normalised in double and rounded to float.
+int ref_synth_mixture(int dtype, uint64_t n, uint32_t d, uint32_t comps, uint64_t seed, uint32_t stream, double lo,
+                      double hi, double sigma, int normalize, void* out) {
+  if (!out || d == 0 || comps == 0 || (dtype != 0 && dtype != 2)) return -1;
+  std::vector<double> cen((size_t)comps * d);
+  for (uint32_t c = 0; c < comps; c++)
+    for (uint32_t t = 0; t < d; t++)
+      cen[(size_t)c * d + t] = dtype == 0 ? lo + (hi - lo) * sm_unif(sm_key(seed, 1, c, t))
+                                          : sm_normal(sm_key(seed, 1, c, 2ull * t), sm_key(seed, 1, c, 2ull * t + 1));
+  const uint64_t s_comp = 2 + 2ull * stream, s_noise = 3 + 2ull * stream;
+  unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  auto rows = [&](unsigned tid) {
+    std::vector<double> v(d);
+    for (uint64_t i = tid; i < n; i += nt) {
+      const double* c = &cen[(size_t)(sm_key(seed, s_comp, i, 0) % comps) * d];
+      for (uint32_t t = 0; t < d; t++)
+        v[t] = c[t] + sigma * sm_normal(sm_key(seed, s_noise, i, 2ull * t), sm_key(seed, s_noise, i, 2ull * t + 1));
+      if (dtype == 0) {
+        uint8_t* o = static_cast<uint8_t*>(out) + i * d;
+        for (uint32_t t = 0; t < d; t++) {
+          const double r = std::round(v[t]);
+          o[t] = (uint8_t)(r < 0.0 ? 0.0 : (r > 255.0 ? 255.0 : r));
+        }
+      } else {
+        double norm = 1.0;
+        if (normalize) {
+          double ss = 0.0;
+          for (uint32_t t = 0; t < d; t++) ss += v[t] * v[t];
+          norm = std::sqrt(ss);
+          if (norm == 0.0) norm = 1.0;
+        }
+        float* o = static_cast<float*>(out) + i * d;
+        for (uint32_t t = 0; t < d; t++) o[t] = (float)(v[t] / norm);
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; t++) th.emplace_back(rows, t);
+  rows(0);
+  for (auto& x : th) x.join();
+  return 0;
 }
 
 int ref_robust_prune(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t R,

@@ -568,14 +568,48 @@ def recall_at_k(ids: np.ndarray, gt_ids: np.ndarray, k: int) -> float:
     return hit / float(k * ids.shape[0])
 
 
-def recall_with_ties(ids: np.ndarray, gt_ids: np.ndarray, gt_d: np.ndarray, k: int) -> float:
-    """checkRecall's recall (check_nn_recall.h:86-112): the groundtruth set is the first k ids plus
-    every later groundtruth id tied with the k-th distance."""
-    hit = 0
-    for i in range(ids.shape[0]):
-        last = gt_d[i, k - 1]
-        extra = [int(x) for x, dd in zip(gt_ids[i, k:], gt_d[i, k:]) if dd == last]
-        truth = [int(x) for x in gt_ids[i, :k]] + extra
-        rep = set(ids[i, :k].tolist())
-        hit += sum(1 for t in truth if t in rep)
-    return hit / float(k * ids.shape[0])
+def point_distances(queries: np.ndarray, base: np.ndarray, ids: np.ndarray, metric: int = L2) -> np.ndarray:
+    """Point::distance of queries[i] to base[ids[i, j]] in the reference's arithmetic, for every
+    (i, j): int32 sums returned as float for 8-bit points, and for float points one sequential sum of
+    separately rounded float products (euclidian_point.h:54-90, mips_point.h:44-66). Returns float32
+    of ids' shape."""
+    ids = np.asarray(ids, dtype=np.int64)
+    rows = base[ids.ravel()].reshape(ids.shape + (base.shape[1],))
+    q = queries[:, None, :]
+    if base.dtype != np.float32:
+        a = q.astype(np.int64)
+        b = rows.astype(np.int64)
+        r = ((a - b) ** 2).sum(-1) if metric == L2 else -(a * b).sum(-1)
+        return r.astype(np.float32)
+    acc = np.zeros(ids.shape, np.float32)
+    for t in range(base.shape[1]):
+        if metric == L2:
+            diff = rows[..., t] - q[..., t]
+            acc = acc + diff * diff
+        else:
+            acc = acc + rows[..., t] * q[..., t]
+    return acc if metric == L2 else -acc
+
+
+def recall_with_ties(ids: np.ndarray, gt_ids: np.ndarray, k: int, queries: np.ndarray, base: np.ndarray,
+                     metric: int = L2) -> float:
+    """checkRecall's recall@k (check_nn_recall.h:86-112): the true set of a query is its first k
+    groundtruth ids plus every later groundtruth id whose distance, recomputed with the reference's
+    own float distance, equals that of the k-th; the hits are the true ids among the first k
+    reported. Returns hits / (k * nq) rounded to float32, as the reference divides."""
+    nq = ids.shape[0]
+    m = gt_ids.shape[1]
+    if m < k:
+        raise ValueError(f"{k}@{k} too large for ground truth data of size {m}")
+    truth = np.ascontiguousarray(gt_ids).astype(np.int64)
+    keep = np.ones(truth.shape, bool)
+    if m > k:
+        d = point_distances(queries, base, truth[:, k - 1:], metric)
+        keep[:, k:] = d[:, 1:] == d[:, :1]
+    rep = np.asarray(ids)[:, :k].astype(np.int64)
+    hits = 0
+    for b in range(0, nq, 4096):
+        t = truth[b:b + 4096]
+        hit = (t[:, :, None] == rep[b:b + 4096, None, :]).any(-1) & keep[b:b + 4096]
+        hits += int(hit.sum())
+    return float(np.float32(hits) / np.float32(k * nq))

@@ -26,7 +26,6 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -45,32 +44,27 @@ int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem);
 uint32_t tier0_slots(const SearchPlan& p, uint32_t R);
 
 constexpr size_t kNoallocScratchBytes = PANN_NOALLOC_SCRATCH_BYTES;
-constexpr int kMaxDevices = 64;
 
 // The scratch itself. Every call on a device shares it and finds in it what
 // the previous call left there.
 static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoallocScratchBytes];
 
-static std::mutex g_noalloc_mu;
-static uint8_t* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the array on `dev`, which must be the current device;
-// looked up on the first call per device (the lookup may load this file's
-// module onto the device). Host code only ever passes this address on: the
-// array's own name is a host-side stand-in, not a device pointer.
+// Device address of the array on `dev`, which must be the current device.
+// Looked up on every call, not cached: the lookup costs little next to the
+// launches, and a process that resets the device (which tears down the
+// context holding the array) gets the new context's address instead of a
+// stale one. The first lookup on a device may load this file's module onto
+// it. Host code only ever passes this address on: the array's own name is a
+// host-side stand-in, not a device pointer.
 static int noalloc_scratch(int dev, uint8_t** out) {
-  if (dev < 0 || dev >= kMaxDevices) return fail(PANN_EINVAL, "device ordinal out of range for the static scratch");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(static search scratch)");
-    }
-    g_noalloc_ptr[dev] = static_cast<uint8_t*>(p);
+  if (dev < 0) return fail(PANN_EINVAL, "no current device for the static scratch");
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(static search scratch)");
   }
-  *out = g_noalloc_ptr[dev];
+  *out = static_cast<uint8_t*>(p);
   return PANN_OK;
 }
 

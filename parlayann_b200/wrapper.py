@@ -38,7 +38,7 @@ from typing import NamedTuple
 
 import numpy as np
 
-from . import L2, MIPS, PREC_F32, PREC_FP8, Index
+from . import L2, MIPS, PREC_F32, PREC_FP8, Index, recall_with_ties
 
 _DTYPE = {"float": np.float32, "uint8": np.uint8, "int8": np.int8}
 _METRIC = {"Euclidian": L2, "mips": MIPS}
@@ -222,16 +222,7 @@ class GraphIndex:
         neighbors = np.asarray(neighbors)
         if (neighbors[:, :k] >= self.points.shape[0]).any():
             raise ValueError("neighbor reported by query out of range")
-        n, m = gt_ids.shape
-        correct = 0
-        for i in range(n):
-            last = _distances(queries[i], self.points[gt_ids[i, k - 1:k]], self.metric)[0]
-            tail = gt_ids[i, k:]
-            ties = tail[_distances(queries[i], self.points[tail], self.metric) == last] if m > k else tail[:0]
-            truth = np.concatenate([gt_ids[i, :k], ties])
-            reported = set(neighbors[i, :k].tolist())
-            correct += sum(1 for t in truth.tolist() if t in reported)
-        recall = correct / float(k * n)
+        recall = recall_with_ties(neighbors, gt_ids, k, queries, self.points, self.metric)
         print(f"Recall: {recall:.6g}")
         return recall
 
