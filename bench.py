@@ -150,6 +150,28 @@ def profiled_traffic():
         return None, None
 
 
+def build_roofline(st, avg_deg, peak, peak_kind):
+    """The GPU build against the HBM roofline. Algorithmic bytes: per insertion search the rows
+    of the nodes it visits (4 (1 + degree) bytes each, the degree taken as the final graph's mean),
+    one point row per distance comparison and the inserted point's own row; one row per robustPrune
+    candidate (insertions and re-prunes); the 4R-byte row written per inserted point; 8 bytes per
+    reverse-edge pair (the sort of (neighbour, point) pairs)."""
+    row = W["d"] * 4
+    deg = min(float(W["R"]), avg_deg)
+    b = (4.0 * st.visited_total * (1.0 + deg) + st.search_cmps * row + st.inserted * row +
+         st.prune_candidates * row + 4.0 * W["R"] * st.inserted + 8.0 * st.edge_pairs)
+    achieved = b / st.seconds / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} (hbm_gbs)",
+            "algorithmic_bytes": round(b), "seconds_device": round(st.seconds, 3),
+            "phase_seconds": {"search": round(st.search_seconds, 3), "prune": round(st.prune_seconds, 3),
+                              "reverse": round(st.reverse_seconds, 3)},
+            "counters": {"inserted": int(st.inserted), "visited": int(st.visited_total),
+                         "search_cmps": int(st.search_cmps), "prune_candidates": int(st.prune_candidates),
+                         "edge_pairs": int(st.edge_pairs), "reprunes": int(st.reprunes),
+                         "batches": int(st.batches)}}
+
+
 def max_over_ranks(seconds: float, device) -> float:
     """The slowest rank's time (all ranks take this collective in the same order)."""
     import torch
@@ -183,11 +205,13 @@ def run_ours(args):
     idx = P.Index(base, W["R"])
     t0 = time.time()
     build_dev = None
+    build_stats = None
     if args.load_graph:
         idx.load_graph(args.load_graph)
     else:
         bst = idx.build(W["Lb"], W["alpha"], num_passes=W["passes"], batch_factor=W["bf"])
         build_dev = round(bst.seconds, 3)
+        build_stats = bst
         if args.save_graph:
             idx.save_graph(args.save_graph)
     build_wall = time.time() - t0
@@ -296,6 +320,7 @@ def run_ours(args):
     per_launch_s = t_dev / args.steps
     achieved = bytes_per_query * nq / per_launch_s / 1e9
     traffic_pq, prof = profiled_traffic()
+    build_roof = build_roofline(build_stats, avg_deg, peak, peak_kind) if build_stats is not None else None
     line = None
     forms = None
     if rank == 0 and not args.no_forms:
@@ -332,6 +357,7 @@ def run_ours(args):
                          "traffic": (round(traffic_pq * nq / 1e9, 4) if traffic_pq else None),
                          "traffic_unit": "GB per launch (ncu dram read+write, scaled from profiles/)"},
             "cpu_baseline": cpu,
+            "build_roofline": build_roof,
         }
         if forms is not None:
             line["forms"] = forms
@@ -366,6 +392,224 @@ def _timed(step, flush, stream, steps, warmup):
     return tot / steps
 
 
+PRECISION_FORMS = (("bf16", 1, 0), ("fp8", 2, 0), ("bf16_tile2", 1, 2), ("fp8_tile2", 2, 2), ("fp8_tile3", 2, 3))
+
+
+def scoring_error(idx, base, q, ids, prec, metric):
+    """Error of the precision's scores (the ones its traversal ranks candidates by, before the
+    exact re-rank) against FP64, on the pairs (query, id): absolute and relative, max and mean."""
+    import parlayann_b200 as P
+
+    sub = min(2000, q.shape[0])
+    ids = np.ascontiguousarray(ids[:sub], dtype=np.uint32)
+    lp = idx.score(q[:sub], ids, prec).astype(np.float64)
+    rows = base[ids.ravel().astype(np.int64)].astype(np.float64).reshape(ids.shape + (base.shape[1],))
+    q64 = q[:sub].astype(np.float64)[:, None, :]
+    d64 = ((rows - q64) ** 2).sum(-1) if metric == P.L2 else -(rows * q64).sum(-1)
+    ab = np.abs(lp - d64)
+    rel = ab / np.maximum(np.abs(d64), 1e-30)
+    return {"pairs": int(ids.size), "abs_max": float(ab.max()), "abs_mean": float(ab.mean()),
+            "rel_max": float(rel.max()), "rel_mean": float(rel.mean())}
+
+
+def precision_forms(idx, base, q, gt, metric, beam, qps_plain, dev, flush, stream, steps, forms=PRECISION_FORMS):
+    """Each precision form at its smallest beam with recall@10 >= 0.95: device QPS through a batch
+    object (CUDA-graph replay), the speed-up over the plain form, the recall loss at the plain
+    form's beam, the error of the precision's own scores against FP64 (before the re-rank, on each
+    query's 20 nearest points) and of the reported (re-ranked) distances."""
+    import torch
+
+    import parlayann_b200 as P
+
+    lib = P.lib()
+    k = W["k"]
+    nq = q.shape[0]
+    dq = torch.from_numpy(q).to(dev)
+    exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, k, q, base, metric)
+    out = {}
+    for name, prec, parents in forms:
+        idx.set_precision(prec)
+        pbeam, prec_rec, pres = None, None, None
+        for L in BEAMS:
+            if L < beam - 10:
+                continue
+            r = idx.search(q, k, L, precision=prec, parents=parents)
+            rec = P.recall_with_ties(r.ids, gt, k, q, base, metric)
+            if rec >= 0.95:
+                pbeam, prec_rec, pres = L, rec, r
+                break
+        if pbeam is None:
+            continue
+        same_beam = idx.search(q, k, beam, precision=prec, parents=parents)
+        loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, k, q, base, metric)
+        b = idx.batch(nq, k, pbeam, precision=prec, parents=parents)
+        d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+        d_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
+        ks = np.full(nq, k, np.uint32)
+        Ls = np.full(nq, pbeam, np.uint32)
+
+        def step_b():
+            rc = lib.pann_batch_run(b.handle, ctypes.c_void_p(dq.data_ptr()), nq, ks.ctypes.data_as(ctypes.c_void_p),
+                                    Ls.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(d_ids.data_ptr()),
+                                    ctypes.c_void_p(d_d.data_ptr()), None, None, None, 1,
+                                    ctypes.c_void_p(stream.cuda_stream))
+            if rc != 0:
+                raise P.PannError(rc, lib.pann_last_error().decode())
+
+        t = _timed(step_b, flush, stream, steps, 3)
+        ids_b = d_ids.cpu().numpy().astype(np.uint32)
+        assert np.array_equal(ids_b, pres.ids), "batched precision form differs from the plain precision form"
+        exact_d = idx.score(q[:2000], pres.ids[:2000])
+        rep_err = np.abs(pres.dists[:2000].astype(np.float64) - exact_d) / np.maximum(np.abs(exact_d), 1e-30)
+        out[name] = {"beam": pbeam, "parents": parents, "recall_at_10": round(prec_rec, 4),
+                     "stopped_early": int(((pres.flags & 2) != 0).sum()), "qps_batched_graph": round(nq / t, 1),
+                     "speedup_vs_plain": round(nq / t / qps_plain, 3),
+                     "recall_loss_at_plain_beam": round(loss, 4),
+                     "scoring_error_vs_fp64": scoring_error(idx, base, q, gt[:, :20], prec, metric),
+                     "reported_distances_equal_exact_f32": bool(rep_err.max() == 0.0)}
+        b.close()
+    idx.set_precision(P.PREC_F32)
+    return out
+
+
+def plain_qps(idx, q, beam, dev, flush, stream, steps):
+    """Device-timed QPS of the plain (exact) search through pann_search_device."""
+    import torch
+
+    import parlayann_b200 as P
+
+    lib = P.lib()
+    k = W["k"]
+    nq = q.shape[0]
+    qp = P.QueryParams(k, beam, idx.n, idx.R, W["bf"])
+    starts = np.zeros(1, np.uint32)
+    dq = torch.from_numpy(q).to(dev)
+    d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
+
+    def step():
+        rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(dq.data_ptr()), nq, ctypes.byref(qp),
+                                    starts.ctypes.data_as(ctypes.c_void_p), 1, ctypes.c_void_p(d_ids.data_ptr()),
+                                    None, None, None, None, ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise P.PannError(rc, lib.pann_last_error().decode())
+
+    return nq / _timed(step, flush, stream, steps, 3)
+
+
+SP_BEAMS = BEAMS + [225, 250, 275, 300, 375, 500, 750, 1000]
+SP_LIMITS = [10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 28, 30, 35]
+SP_BUCKETS = [.1, .2, .3, .4, .5, .6, .7, .75, .8, .85, .9, .93, .95, .97, .98, .99, .995, .999, .9995, .9999, .99995,
+              .99999]
+
+
+def search_and_parse(idx, base, q, gt, dev, flush, stream):
+    """The reference's search_and_parse sweep (check_nn_recall.h:184-265) on the GPU: recall@10 and
+    device-timed QPS for every beam of its list, for the visit limits 10..35 (beam max(limit, k),
+    degree limit min(R, 5 limit)) and for the "best accuracy" point (k = 100, beam 1000, recall of
+    the first 10); then, per recall bucket, the fastest configuration whose recall lies in
+    [bucket, next bucket] (parse_results.h:189-214)."""
+    import torch
+
+    import parlayann_b200 as P
+
+    lib = P.lib()
+    k = W["k"]
+    nq = q.shape[0]
+    starts = np.zeros(1, np.uint32)
+    dq = torch.from_numpy(q).to(dev)
+    d_ids = torch.empty((nq, 100), dtype=torch.int32, device=dev)
+    d_vis = torch.empty(nq, dtype=torch.int32, device=dev)
+    d_cmps = torch.empty(nq, dtype=torch.int32, device=dev)
+
+    def check(kk, L, limit, dl):
+        qp = P.QueryParams(kk, L, limit, dl, W["bf"])
+
+        def step():
+            rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(dq.data_ptr()), nq, ctypes.byref(qp),
+                                        starts.ctypes.data_as(ctypes.c_void_p), 1, ctypes.c_void_p(d_ids.data_ptr()),
+                                        None, ctypes.c_void_p(d_vis.data_ptr()), ctypes.c_void_p(d_cmps.data_ptr()),
+                                        None, ctypes.c_void_p(stream.cuda_stream))
+            if rc != 0:
+                raise P.PannError(rc, lib.pann_last_error().decode())
+
+        t = _timed(step, flush, stream, 2, 1)
+        ids = d_ids.view(-1)[:nq * kk].cpu().numpy().astype(np.uint32).reshape(nq, kk)  # rows of kk ids
+        vis = d_vis.cpu().numpy()
+        cm = d_cmps.cpu().numpy()
+        return {"k": kk, "beam": L, "limit": limit, "degree_limit": dl,
+                "recall": round(P.recall_with_ties(ids, gt, k, q, base), 4), "qps": round(nq / t, 1),
+                "mean_cmps": round(float(cm.mean()), 1), "mean_visited": round(float(vis.mean()), 2)}
+
+    res = [check(k, L, idx.n, idx.R) for L in SP_BEAMS if L >= k]
+    res += [check(k, max(l, k), l, min(idx.R, 5 * l)) for l in SP_LIMITS]
+    res.append(check(100, 1000, idx.n, idx.R))
+    table = []
+    for i, b in enumerate(SP_BUCKETS):
+        cands = [r for r in res if r["recall"] >= b]
+        if i < len(SP_BUCKETS) - 1 and cands:
+            cands = [r for r in cands if r["recall"] <= SP_BUCKETS[i + 1]]
+        if cands:
+            m = max(cands, key=lambda r: r["qps"])
+            table.append({"bucket": b, **m})
+    return {"runs": res, "buckets": table}
+
+
+def run_c2(dev, flush, args):
+    """The precision form at 10M: 10,000,000 base + 10,000 query vectors, 96-d float32, the same
+    generator with 1,024 components, Vamana R=64 L=128 alpha=1.2 two passes built on the GPU with
+    the Euclidean distance; searched as a Euclidean index and as a mips index (on L2-normalised
+    vectors -q.b orders points as |q - b|^2 does, so the one graph serves both). Per metric: the
+    plain form's smallest beam with recall@10 >= 0.95 and its QPS, each precision form next to it."""
+    import torch
+
+    import parlayann_b200 as P
+
+    n, nq, d = 10_000_000, 10_000, 96
+    t0 = time.time()
+    base = P.synth_mixture(P.F32, n, d, 1024, W["seed"], 0, sigma=W["sigma"], normalize=True)
+    q = P.synth_mixture(P.F32, nq, d, 1024, W["seed"], 1, sigma=W["sigma"], normalize=True)
+    gen_s = time.time() - t0
+    stream = torch.cuda.current_stream(dev)
+    steps = max(3, min(args.steps, 10))
+    idx = P.Index(base, W["R"])
+    bst = idx.build(W["Lb"], W["alpha"], num_passes=W["passes"], batch_factor=W["bf"])
+    g = idx.get_graph()
+    out = {"workload": "10M x 96-d f32 (1024-component mixture, L2-normalised, seed 1), 10K queries, Vamana R=64 "
+                       "L=128 alpha=1.2 two passes (GPU build, Euclidean)",
+           "build_seconds_device": round(bst.seconds, 3), "mean_degree": round(float(g[:, 0].mean()), 3),
+           "generate_seconds_host": round(gen_s, 2)}
+    for mname, metric in (("l2", P.L2), ("mips", P.MIPS)):
+        if metric == P.L2:
+            ix = idx
+        else:
+            ix = P.Index(base, W["R"], P.MIPS)
+            ix.set_graph(g)
+        t0 = time.time()
+        gt, _ = ix.groundtruth(q, 20)
+        gt_s = time.time() - t0
+        beam, rec = None, None
+        for L in BEAMS:
+            r = ix.search(q, W["k"], L, batch_factor=W["bf"])
+            rec = P.recall_with_ties(r.ids, gt, W["k"], q, base, metric)
+            if rec >= 0.95:
+                beam = L
+                break
+        if beam is None:
+            out[mname] = {"failed": "no beam of the sweep reached recall 0.95"}
+            continue
+        qps = plain_qps(ix, q, beam, dev, flush, stream, steps)
+        out[mname] = {"groundtruth_seconds": round(gt_s, 3),
+                      "plain": {"beam": beam, "recall_at_10": round(rec, 4), "qps": round(qps, 1)},
+                      "precision": precision_forms(ix, base, q, gt, metric, beam, qps, dev, flush, stream, steps)}
+        best = max(out[mname]["precision"].values(), key=lambda v: v["qps_batched_graph"], default=None)
+        if best:
+            out[mname]["best_speedup_vs_plain"] = best["speedup_vs_plain"]
+        if ix is not idx:
+            ix.close()
+    idx.close()
+    return out
+
+
 def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     """The precision, batched and serving forms and range search on the same
     index, each next to the plain form: QPS at recall@10 >= 0.95 (device
@@ -384,63 +628,11 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     out = {}
     steps = max(3, min(args.steps, 10))
 
-    # FP64 distances of returned ids, for the distance error per precision
-    b64 = None
-
-    def dist_err(ids, dists):
-        nonlocal b64
-        sel = ids[:1000].astype(np.int64)
-        qq = q[:1000].astype(np.float64)
-        bb = base[sel.ravel()].astype(np.float64).reshape(sel.shape[0], sel.shape[1], -1)
-        d64 = ((bb - qq[:, None, :]) ** 2).sum(-1)
-        rel = np.abs(dists[:1000].astype(np.float64) - d64) / np.maximum(d64, 1e-30)
-        return float(rel.max()), float(rel.mean())
-
     want = set(args.forms.split(","))
     # ---- precision form (+ batched): smallest beam with recall >= 0.95, device QPS through a batch object
     prec_out = {}
-    exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, k, q, base)
-    for name, prec, parents in ((("bf16", P.PREC_BF16, 0), ("fp8", P.PREC_FP8, 0), ("bf16_tile2", P.PREC_BF16, 2),
-                                 ("fp8_tile2", P.PREC_FP8, 2), ("fp8_tile3", P.PREC_FP8, 3))
-                                if "precision" in want or "serving" in want else ()):
-        idx.set_precision(prec)
-        pbeam, prec_rec, pres = None, None, None
-        for L in BEAMS:
-            if L < beam - 10:
-                continue
-            r = idx.search(q, k, L, precision=prec, parents=parents)
-            rec = P.recall_with_ties(r.ids, gt, k, q, base)
-            if rec >= 0.95:
-                pbeam, prec_rec, pres = L, rec, r
-                break
-        if pbeam is None:
-            continue
-        same_beam = idx.search(q, k, beam, precision=prec, parents=parents)
-        loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, k, q, base)
-        b = idx.batch(nq, k, pbeam, precision=prec, parents=parents)
-        d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
-        d_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
-        ks = np.full(nq, k, np.uint32)
-        Ls = np.full(nq, pbeam, np.uint32)
-
-        def step_b():
-            rc = lib.pann_batch_run(b.handle, ctypes.c_void_p(dq.data_ptr()), nq, ks.ctypes.data_as(ctypes.c_void_p),
-                                    Ls.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(d_ids.data_ptr()),
-                                    ctypes.c_void_p(d_d.data_ptr()), None, None, None, 1,
-                                    ctypes.c_void_p(stream.cuda_stream))
-            if rc != 0:
-                raise P.PannError(rc, lib.pann_last_error().decode())
-
-        t = _timed(step_b, flush, stream, steps, 3)
-        ids_b = d_ids.cpu().numpy().astype(np.uint32)
-        assert np.array_equal(ids_b, pres.ids), "batched precision form differs from the plain precision form"
-        mx, mean = dist_err(pres.ids, pres.dists)
-        prec_out[name] = {"beam": pbeam, "parents": parents, "recall_at_10": round(prec_rec, 4),
-                          "stopped_early": int(((pres.flags & 2) != 0).sum()), "qps_batched_graph": round(nq / t, 1),
-                          "speedup_vs_plain": round(nq / t / qps_plain, 3),
-                          "recall_loss_at_plain_beam": round(loss, 4),
-                          "reported_distance_rel_error_vs_fp64": {"max": mx, "mean": mean}}
-        b.close()
+    if "precision" in want or "serving" in want:
+        prec_out = precision_forms(idx, base, q, gt, P.L2, beam, qps_plain, dev, flush, stream, steps)
     idx.set_precision(P.PREC_F32)
     if "precision" in want:
         # the reference's own mixed precision: search over one-byte scalar-quantized points, float re-rank of
@@ -533,6 +725,10 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         out["range"]["groundtruth"] = gt
     if "serving" in want:
         out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
+    if "sweep" in want:
+        out["search_and_parse"] = search_and_parse(idx, base, q, gt, dev, flush, stream)
+    if "c2" in want:
+        out["precision_10m"] = run_c2(dev, flush, args)
     return out
 
 
@@ -760,8 +956,10 @@ def main():
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / batched / range / serving forms")
-    ap.add_argument("--forms", default="precision,batched,range,serving",
-                    help="comma list of the forms to run (precision, batched, range, serving)")
+    ap.add_argument("--forms", default="precision,batched,range,serving,sweep,c2",
+                    help="comma list of the forms to run (precision, batched, range, serving, sweep: the "
+                         "reference's search_and_parse sweep, and c2: the precision form on a 10M-point index, "
+                         "Euclidean and mips)")
     ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
     ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
     args = ap.parse_args()

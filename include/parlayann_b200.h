@@ -73,6 +73,12 @@ typedef struct {
   uint64_t visited_total;  /* sum of visited-list sizes */
   uint32_t batches;        /* batch_insert rounds over all passes */
   uint32_t flagged;        /* searches where the reference hashset would have grown */
+  /* work counters (the build's algorithmic bytes are computed from these) */
+  uint64_t search_cmps;      /* distance comparisons of the insertion searches */
+  uint64_t prune_candidates; /* candidates assembled for robustPrune (insertions and re-prunes) */
+  uint64_t edge_pairs;       /* reverse-edge (neighbour, point) pairs grouped */
+  uint64_t reprunes;         /* vertices re-pruned because their reverse edges overflowed R */
+  uint64_t inserted;         /* points inserted over all passes */
 } pann_build_stats;
 
 /* ---------------------------------------------------------------- index */
@@ -195,6 +201,16 @@ typedef struct {
                         shared memory; its own visiting order and recall curve. Status bit 32 marks a
                         query whose seen set filled (it stopped early). */
 } pann_search_options;
+
+/* Distances of given (query, point) pairs: queries nq rows (host), ids nq x m
+ * point ids (host), out nq x m (host). PANN_PREC_F32 gives Point::distance
+ * exactly (euclidian_point.h:54-90, mips_point.h:44-66: integer sums, or the
+ * float32 sequential sum); PANN_PREC_BF16 / PANN_PREC_FP8 give the precision
+ * form's approximate scores, the ones its traversal ranks candidates by
+ * (pann_index_set_precision first). The reference's counterpart is calling
+ * Point::distance on each pair. */
+int pann_score(pann_index* idx, const void* queries, uint32_t nq, const uint32_t* ids, uint32_t m, int precision,
+               float* out);
 
 /* Build the low-precision copy of the points used by `precision` (kept until
  * the next call; PANN_PREC_F32 frees it). No reference counterpart: the

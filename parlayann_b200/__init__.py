@@ -104,6 +104,11 @@ class BuildStats(ctypes.Structure):
         ("visited_total", ctypes.c_uint64),
         ("batches", ctypes.c_uint32),
         ("flagged", ctypes.c_uint32),
+        ("search_cmps", ctypes.c_uint64),
+        ("prune_candidates", ctypes.c_uint64),
+        ("edge_pairs", ctypes.c_uint64),
+        ("reprunes", ctypes.c_uint64),
+        ("inserted", ctypes.c_uint64),
     ]
 
 
@@ -150,6 +155,7 @@ SIGNATURES = {
     "pann_batch_destroy": (_I, [_P]),
     "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
     "pann_groundtruth": (_I, [_P, _P, _U32, _U32, _P, _P]),
+    "pann_score": (_I, [_P, _P, _U32, _P, _U32, _I, _P]),
     "pann_last_error": (ctypes.c_char_p, []),
     "pann_synth_mixture": (_I, [_I, _U64, _U32, _U32, _U64, _U32, ctypes.c_double, ctypes.c_double,
                                 ctypes.c_double, _I, _P]),
@@ -318,6 +324,16 @@ class Index:
     def set_precision(self, precision: int):
         """Build the low-precision copy used by the precision form (float32 indexes)."""
         _check(lib().pann_index_set_precision(self._h, precision))
+
+    def score(self, queries: np.ndarray, ids: np.ndarray, precision: int = PREC_F32) -> np.ndarray:
+        """Distances of queries[i] to the points ids[i, j] (pann_score): Point::distance exactly, or the
+        precision form's approximate score."""
+        queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        out = np.empty(ids.shape, np.float32)
+        _check(lib().pann_score(self._h, _ptr(queries), queries.shape[0], _ptr(ids), ids.shape[1], precision,
+                                _ptr(out)))
+        return out
 
     def search(self, queries: np.ndarray, k: int, L: int, limit: int | None = None, degree_limit: int | None = None,
                batch_factor: float = 0.125, starts=(0,), allow_short: bool = False, precision: int = PREC_F32,

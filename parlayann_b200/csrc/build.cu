@@ -353,6 +353,23 @@ __global__ void count_flag_kernel(const uint32_t* status, uint32_t n, uint32_t f
   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
   if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
 }
+// Sum of end[i] - begin[i] (segment lengths) and of the live degrees of the rows rows[i].
+__global__ void seg_len_sum_kernel(const uint32_t* begin, const uint32_t* end, uint32_t n, unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += end[i] - begin[i];
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+__global__ void degree_sum_kernel(const uint32_t* graph, uint32_t R, const uint32_t* rows, uint32_t n,
+                                  unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < (uint64_t)n * R;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    acc += graph[(uint64_t)rows[e / R] * R + e % R] != PANN_PAD;
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
 __global__ void sum_kernel(const uint32_t* v, uint32_t n, unsigned long long* out) {
   unsigned long long acc = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += v[i];
@@ -427,7 +444,8 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
   BCUDA(cudaMemcpyAsync(bb.start.p, &start0, 4, cudaMemcpyHostToDevice, st));
   BCUDA(bb.counters.ensure(256));
   uint32_t* c32 = bb.counters.as<uint32_t>();  // [0] status or, [1] njobs, [2] flagged count
-  // [0] dist cmps, [1] visited, [2] reverse prune segment cursor
+  // [0] dist cmps, [1] visited, [2] reverse prune segment cursor, [3] search cmps,
+  // [4] insertion prune candidates, [5] reverse-edge pairs
   unsigned long long* c64 = reinterpret_cast<unsigned long long*>(c32 + 8);
   BCUDA(cudaMemsetAsync(bb.counters.p, 0, 256, st));
 
@@ -472,6 +490,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
   const int wpb = 4;
   const size_t warp_smem = stride;
   uint32_t batches = 0;
+  uint64_t reprunes = 0, prune_cands = 0, inserted = 0;
 
   for (int pass = 0; pass < bp->num_passes; pass++) {
     const double alpha = (pass == bp->num_passes - 1) ? bp->alpha : 1.0;  // index.h:173-178
@@ -517,6 +536,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
       }
       count_flag_kernel<<<64, 256, 0, st>>>(bb.status.as<uint32_t>(), B, QS_REF_WOULD_GROW, c32 + 2);
       sum_kernel<<<64, 256, 0, st>>>(bb.cmps.as<uint32_t>(), B, c64);
+      sum_kernel<<<64, 256, 0, st>>>(bb.cmps.as<uint32_t>(), B, c64 + 3);
       sum_kernel<<<64, 256, 0, st>>>(bb.vis_n.as<uint32_t>(), B, c64 + 1);
       // ---- 2. robustPrune of the inserted points
       BCUDA(cudaEventRecord(ea, st));
@@ -546,6 +566,8 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
         return cudaGetLastError();
       }));
       BCUDA(cudaEventRecord(eb, st));
+      seg_len_sum_kernel<<<64, 256, 0, st>>>(bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(), B, c64 + 4);
+      degree_sum_kernel<<<128, 256, 0, st>>>(idx->d_graph, R, pts, B, c64 + 5);
       // ---- 3. reverse edges
       const uint64_t np = (uint64_t)B * R;
       reverse_pairs_kernel<<<(int)std::min<uint64_t>((np + 255) / 256, 65535), 256, 0, st>>>(
@@ -581,6 +603,9 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
       BCUDA(cudaMemcpyAsync(&njobs, c32 + 1, 4, cudaMemcpyDeviceToHost, st));
       BCUDA(cudaMemcpyAsync(&seg_total, c64 + 2, 8, cudaMemcpyDeviceToHost, st));
       BCUDA(cudaStreamSynchronize(st));
+      reprunes += njobs;
+      prune_cands += seg_total;
+      inserted += B;
       if (njobs) {
         if (seg_total >= 0x7FFFFFFFull) {
           cleanup();
@@ -652,14 +677,19 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
     stats->search_seconds = t_search;
     stats->prune_seconds = t_prune;
     stats->reverse_seconds = t_rev;
-    unsigned long long h64[2] = {0, 0};
+    unsigned long long h64[6] = {0, 0, 0, 0, 0, 0};
     uint32_t h32[4] = {0, 0, 0, 0};
-    cudaMemcpy(h64, c64, 16, cudaMemcpyDeviceToHost);
+    cudaMemcpy(h64, c64, 48, cudaMemcpyDeviceToHost);
     cudaMemcpy(h32, c32, 16, cudaMemcpyDeviceToHost);
     stats->dist_cmps = h64[0];
     stats->visited_total = h64[1];
     stats->batches = batches;
     stats->flagged = h32[2];
+    stats->search_cmps = h64[3];
+    stats->prune_candidates = h64[4] + prune_cands;
+    stats->edge_pairs = h64[5];
+    stats->reprunes = reprunes;
+    stats->inserted = inserted;
   }
   cudaEventDestroy(ev0); cudaEventDestroy(ev1);
   cudaEventDestroy(ea); cudaEventDestroy(eb); cudaEventDestroy(ec); cudaEventDestroy(ed);

@@ -150,9 +150,26 @@ static uint32_t pow2_at_least(uint64_t x) {
   return p;
 }
 
+// Tier-0 register budget for float32 Euclidean search: PANN_T0_MINB=4 fits the
+// kernel to four 128-thread blocks per SM (128 registers) instead of three.
+static int t0_minb() {
+  static const int v = [] {
+    const char* e = std::getenv("PANN_T0_MINB");
+    return e && std::atoi(e) == 4 ? 4 : 3;
+  }();
+  return v;
+}
+
+template <int DT, int MT, bool G, int PREC = PREC_F32>
+static auto search_kernel_ptr() {
+  if constexpr (DT == DT_F32 && MT == MT_L2 && !G && PREC == PREC_F32)
+    if (t0_minb() == 4) return search_kernel<DT, MT, G, PREC, 4>;
+  return search_kernel<DT, MT, G, PREC, 3>;
+}
+
 template <int DT, int MT, bool G, int PREC = PREC_F32>
 static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
-  auto k = search_kernel<DT, MT, G, PREC>;
+  auto k = search_kernel_ptr<DT, MT, G, PREC>();
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return e;
   k<<<blocks, threads, smem, st>>>(a);
@@ -212,10 +229,33 @@ cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const Search
   return cudaErrorInvalidValue;
 }
 
+template <int DT, int MT>
+static cudaError_t launch_emulate_block_t(const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem,
+                                          cudaStream_t st) {
+  auto k = search_emulate_block_kernel<DT, MT, EMU_BLOCK_WARPS, 24>;
+  cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
+  if (err != cudaSuccess) return err;
+  k<<<blocks, 32 * EMU_BLOCK_WARPS, smem, st>>>(a, e);
+  return cudaGetLastError();
+}
+cudaError_t launch_emulate_block(int dtype, int metric, const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem,
+                                 cudaStream_t st) {
+#define PANN_EMUB_CASE(DT, MT) \
+  if (dtype == DT && metric == MT) return launch_emulate_block_t<DT, MT>(a, e, blocks, smem, st);
+  PANN_EMUB_CASE(DT_U8, MT_L2)
+  PANN_EMUB_CASE(DT_U8, MT_IP)
+  PANN_EMUB_CASE(DT_I8, MT_L2)
+  PANN_EMUB_CASE(DT_I8, MT_IP)
+  PANN_EMUB_CASE(DT_F32, MT_L2)
+  PANN_EMUB_CASE(DT_F32, MT_IP)
+#undef PANN_EMUB_CASE
+  return cudaErrorInvalidValue;
+}
+
 template <int DT, int MT, bool G, int PREC = PREC_F32>
 static int occupancy_t(int threads, size_t smem) {
   int nb = 0;
-  auto k = search_kernel<DT, MT, G, PREC>;
+  auto k = search_kernel_ptr<DT, MT, G, PREC>();
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
   return nb;
@@ -310,8 +350,9 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
   t.S0 = 1ull << t.bits0;
   t.vs = pow2_at_least(8ull * plan.L + 64);
   t.base = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, 0, true);
-  t.emu_smem_need = emu_smem_bytes(t.base, t.vs, (uint32_t)(4 * t.S0), (uint32_t)(2 * t.S0), true);
-  t.emu_smem = t.emu_smem_need <= smem_cap && 4 * t.S0 < (1ull << 31);
+  t.emu_smem_need = emu_block_layout(idx->stride, plan.L, plan.Ccap, idx->R, t.vs, (uint32_t)(4 * t.S0),
+                                     (uint32_t)(2 * t.S0)).bytes;
+  t.emu_smem = 4 * t.S0 < (1ull << 30) && t.emu_smem_need <= smem_cap;
   t.capA = 16 * t.S0;
   t.capB = 8 * t.S0;
   size_t per_slot = 4ull * (t.capA + t.capB);
@@ -410,7 +451,7 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
       t.job_list = b.emu;
       t.njobs_dev = cnt + 6;
       t.job_counter = cnt + 5;
-      PANN_CUDA(launch_emulate(idx->dtype, idx->metric, true, t, e, 2 * idx->sm_count, z.emu_smem_need, st));
+      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, t, e, idx->sm_count, z.emu_smem_need, st));
       glist = b.ovf;
       grec = b.ovf_rec;
       gcount = cnt + 8;

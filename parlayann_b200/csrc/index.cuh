@@ -76,6 +76,7 @@ struct pann_index {
   float q_slope = 1.0f;
   int32_t q_offset = 0;
   bool graph_borrowed = false;  // d_graph belongs to another index
+  uint32_t gt_fallbacks = 0;  // queries of the last float groundtruth recomputed by the plain kernel
   uint32_t starts_cached_n = 0;
   uint32_t starts_cached[64] = {};
 };

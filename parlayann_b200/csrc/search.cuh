@@ -198,8 +198,10 @@ __device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint
   return 0;
 }
 
-template <int DT, int MT, bool TABLE_GLOBAL, int PREC = PREC_F32>
-__global__ void __launch_bounds__(128, 3) search_kernel(SearchArgs a) {
+// MINB: blocks of 128 threads the register budget is fitted to (3: 168
+// registers a thread; 4: 128).
+template <int DT, int MT, bool TABLE_GLOBAL, int PREC = PREC_F32, int MINB = 3>
+__global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;

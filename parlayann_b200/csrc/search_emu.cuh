@@ -96,57 +96,25 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
   *pos = p;
 }
 
-// Warp: grow the table (hashset.h:25-38): every key of the old table is
-// re-inserted in old-slot order (num_entries counts each re-insertion), then
-// the key that triggered the growth continues from its old-mask slot
-// (:39-47). Returns false if the grown table does not fit this tier.
-//
-// The re-insertion is computed cluster by cluster. With linear probing the
-// set of occupied slots does not depend on the insertion order; only which
-// key sits where inside a cluster (a maximal run of occupied slots) does, and
-// a key only ever lands in the cluster that holds its home. So: (A) the keys'
-// ranks in old-slot order are placed in any order (lanes take ranks far apart,
-// so they seldom share slots), which fixes the clusters; (B) the lane whose
-// key starts a cluster replays that cluster's keys in rank order, each at the
-// first free slot from its home. A cluster longer than 64 sends the
-// re-insertion to a plain sequential pass instead.
-__device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool* a_seen) {
+// Warp: place the keys keys[0..cnt) into the empty table `other` (mask
+// nmask) exactly as inserting them one at a time in rank order would
+// (hashset.h:39-47: probe from the key's slot to its first empty slot; a key
+// already there is not inserted again). With linear probing the set of
+// occupied slots does not depend on the insertion order; only which key sits
+// where inside a cluster (a maximal run of occupied slots) does, and a key
+// only ever lands in the cluster that holds its home. So: (A) the keys'
+// ranks are placed in any order (lanes take ranks far apart, so they seldom
+// share slots), which fixes the clusters; (B) the lane whose key starts a
+// cluster replays that cluster's keys in rank order, each at the first free
+// slot from its home. A cluster longer than 64 sends the placement to a plain
+// sequential pass instead. `tail` (tail_words words after the keys, which may
+// alias the keys' own buffer past cnt) holds the owner bits and the per-lane
+// replay rows.
+__device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, uint32_t* other, uint32_t nmask,
+                                                 uint32_t tail_words, int lane) {
   const unsigned FULL = 0xFFFFFFFFu;
-  const uint32_t size = 1u << h.bits, nsize = size * 2;
-  if (nsize > h.other_cap) return false;
-  uint32_t* other = h.other;
+  const uint32_t nsize = nmask + 1;
   const uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
-  for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
-  __syncwarp();
-  const uint32_t oldmask = size - 1, nmask = nsize - 1;
-  // the old table's keys compacted to its front in slot order (writes never
-  // pass the chunk being read): keys[r] is the key of rank r
-  uint32_t cnt = 0;
-  for (uint32_t base = 0; base < size; base += 128) {  // 4 slots per lane per step
-    uint32_t k4[4];
-    uint32_t c = 0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const uint32_t i = base + 4 * (uint32_t)lane + (uint32_t)j;
-      k4[j] = i < size ? h.cur[i] : PANN_PAD;
-      c += k4[j] != PANN_PAD;
-    }
-    uint32_t pre = c;  // inclusive prefix over lanes
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t t = __shfl_up_sync(FULL, pre, d);
-      if (lane >= d) pre += t;
-    }
-    const uint32_t total = __shfl_sync(FULL, pre, 31);
-    __syncwarp();
-    uint32_t at = cnt + pre - c;
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      if (k4[j] != PANN_PAD) h.cur[at++] = k4[j];
-    cnt += total;
-    __syncwarp();
-  }
-  uint32_t* keys = h.cur;
   // (A) ranks into the new table, lane l taking rank l * nb + b in batch b; a
   // key the old table holds twice keeps the smaller rank (its first copy in
   // old-slot order, the one the reference inserts; the other copy finds it)
@@ -185,7 +153,7 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
   const uint32_t words = nb;
   uint32_t* owner = keys + ((cnt + 3) & ~3u);
   uint32_t* scratch = owner + ((words + 3) & ~3u);
-  const bool scratch_ok = (size_t)(scratch - keys) + 32ull * 64 <= size;
+  const bool scratch_ok = (size_t)(scratch - keys) + 32ull * 64 <= (size_t)tail_words;
   if (!fallback) {
     for (uint32_t b = 0; b < nb; b++) {
       const uint32_t r = b * 32 + lane;
@@ -275,6 +243,50 @@ __device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool*
     }
     __syncwarp();
   }
+}
+
+// Warp: grow the table (hashset.h:25-38): every key of the old table is
+// re-inserted in old-slot order (num_entries counts each re-insertion), then
+// the key that triggered the growth continues from its old-mask slot
+// (:39-47). Returns false if the grown table does not fit this tier. The
+// re-insertion is emu_place_ranked with the keys' ranks in old-slot order.
+__device__ __forceinline__ bool emu_grow(EmuHash& h, uint32_t a, int lane, bool* a_seen) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const uint32_t size = 1u << h.bits, nsize = size * 2;
+  if (nsize > h.other_cap) return false;
+  uint32_t* other = h.other;
+  const uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+  for (uint32_t i = lane; i < (nsize >> 2); i += 32) reinterpret_cast<uint4*>(other)[i] = e4;
+  __syncwarp();
+  const uint32_t oldmask = size - 1, nmask = nsize - 1;
+  // the old table's keys compacted to its front in slot order (writes never
+  // pass the chunk being read): keys[r] is the key of rank r
+  uint32_t cnt = 0;
+  for (uint32_t base = 0; base < size; base += 128) {  // 4 slots per lane per step
+    uint32_t k4[4];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t i = base + 4 * (uint32_t)lane + (uint32_t)j;
+      k4[j] = i < size ? h.cur[i] : PANN_PAD;
+      c += k4[j] != PANN_PAD;
+    }
+    uint32_t pre = c;  // inclusive prefix over lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, pre, d);
+      if (lane >= d) pre += t;
+    }
+    const uint32_t total = __shfl_sync(FULL, pre, 31);
+    __syncwarp();
+    uint32_t at = cnt + pre - c;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k4[j] != PANN_PAD) h.cur[at++] = k4[j];
+    cnt += total;
+    __syncwarp();
+  }
+  emu_place_ranked(h.cur, cnt, other, nmask, size, lane);
   __threadfence_block();
   const long long added = cnt;
   h.num_entries += added;
@@ -459,14 +471,11 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       const uint64_t* rcand = reinterpret_cast<const uint64_t*>(rec + ly.cand);
       for (int i = lane; i < fn; i += 32) fr[i] = rfr[i];
       for (int i = lane; i < cn; i += 32) cand[i] = rcand[i];
-      const uint32_t mask0 = (1u << h.bits) - 1;
-      for (uint32_t b = 0; b < entries; b += 32) {
-        const bool v = b + lane < entries;
-        const uint32_t key = v ? rec[ly.log + b + lane] : PANN_PAD;
-        bool ins;
-        uint32_t pos;
-        emu_probe_rounds(h.cur, mask0, key, v, ref_slot(key, mask0), lane, &ins, &pos);
-      }
+      // the logged ids, inserted in log order (staged in table B, unused until a growth)
+      for (uint32_t i = lane; i < entries; i += 32) h.other[i] = rec[ly.log + i];
+      __syncwarp();
+      emu_place_ranked(h.other, entries, h.cur, (1u << h.bits) - 1, h.other_cap, lane);
+      __syncwarp();
       h.num_entries = entries;
       for (uint32_t i = lane; i < (uint32_t)nvis; i += 32) vset_insert(vset, vmask, rec[ly.vis + i]);
     } else {
@@ -631,6 +640,376 @@ __global__ void __launch_bounds__(32) search_emulate_kernel(SearchArgs a, EmuArg
       if (a.out_status) a.out_status[qi] = status;
     }
     __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same emulation with one block of NW warps per query (shared-memory
+// tables only). The per-visit work that does not touch the reference's table
+// runs beside it: warp 0 makes the hashset calls in order, while warps
+// 1..NW-1 score every neighbour of the visited node (each thread one whole
+// row, all its loads in flight at once), so the rows arrive while the table
+// is probed; the distances of the ids the table reports new are then taken
+// from that set. Sorting, de-duplication and the merge run on all threads.
+// Per query the results, counters and status bits equal the single-warp
+// kernel's (the same calls on the same table in the same order; candidates
+// are a set until sorted, and every order-sensitive step keeps its order).
+//
+// Shared memory: the query, the two frontiers, the two candidate buffers, the
+// new ids with their positions in the adjacency row, the distances of the
+// whole row, control words, the visited-id set and the tables A and B.
+struct EmuBlockLayout {
+  uint32_t fr, cand, nbuf, npos, dall, ctrl, vset, tabA, tabB, bytes;
+};
+__host__ __device__ inline EmuBlockLayout emu_block_layout(uint64_t stride, uint32_t L, uint32_t Ccap, uint32_t R,
+                                                           uint32_t vs, uint32_t capA, uint32_t capB) {
+  EmuBlockLayout y;
+  const uint32_t R4 = (R + 3) & ~3u;
+  uint64_t o = (stride + 15) & ~15ull;
+  y.fr = (uint32_t)o;   o += 16ull * L;
+  y.cand = (uint32_t)o; o += 16ull * Ccap;
+  y.nbuf = (uint32_t)o; o += 4ull * R4;
+  y.npos = (uint32_t)o; o += 4ull * R4;
+  y.dall = (uint32_t)o; o += 4ull * R4;
+  y.ctrl = (uint32_t)o; o += 64;
+  y.vset = (uint32_t)o; o += 4ull * vs;
+  y.tabA = (uint32_t)o; o += 4ull * capA;
+  y.tabB = (uint32_t)o; o += 4ull * capB;
+  y.bytes = (uint32_t)((o + 15) & ~15ull);
+  return y;
+}
+
+// Distance of one whole row, all of its 16-byte chunks loaded before the sum
+// (CH >= the row's chunk count keeps every load of the row in flight at once).
+template <int DT, int MT, int CH>
+__device__ __forceinline__ float row_dist_whole(const uint8_t* __restrict__ row, const uint8_t* qs, int nchunks,
+                                                int32_t qq) {
+  if (DT == DT_F32) {
+    const float4* r = reinterpret_cast<const float4*>(row);
+    const float4* q = reinterpret_cast<const float4*>(qs);
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < nchunks; c0 += CH) {
+      float4 b[CH];
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (c0 + c < nchunks) b[c] = __ldg(r + c0 + c);
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (c0 + c < nchunks) acc = f32_chunk<MT>(acc, b[c], q[c0 + c]);
+    }
+    return MT == MT_L2 ? acc : -acc;
+  } else {
+    const uint4* r = reinterpret_cast<const uint4*>(row);
+    const uint4* q = reinterpret_cast<const uint4*>(qs);
+    int32_t pq = 0, pp = 0;
+    for (int c0 = 0; c0 < nchunks; c0 += CH) {
+      uint4 b[CH];
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (c0 + c < nchunks) b[c] = __ldg(r + c0 + c);
+#pragma unroll
+      for (int c = 0; c < CH; c++)
+        if (c0 + c < nchunks) int_chunk<DT, MT>(b[c], q[c0 + c], pq, pp);
+    }
+    return int_result<MT>(qq, pq, pp);
+  }
+}
+
+// Rank sort of n keys from `in` into `out` over all threads of the block
+// (ties by index, as warp_rank_sort).
+__device__ __forceinline__ void block_rank_sort(const uint64_t* in, uint64_t* out, int n, int tid, int nth) {
+  for (int i = tid; i < n; i += nth) {
+    const uint64_t ki = in[i] & PANN_KEYMASK;
+    int r = 0;
+    for (int j = 0; j < n; j++) {
+      const uint64_t kj = in[j] & PANN_KEYMASK;
+      r += (kj < ki) | ((kj == ki) & (j < i));
+    }
+    out[r] = in[i];
+  }
+}
+
+// set_union + trim (as warp_merge) over all threads of the block.
+__device__ __forceinline__ int block_merge(const uint64_t* fr, int fn, const uint64_t* c, int cn, uint64_t* out,
+                                           int L, int tid, int nth) {
+  for (int i = tid; i < fn; i += nth) {
+    const uint64_t k = fr[i] & PANN_KEYMASK;
+    int lo = 0, hi = cn;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if ((c[mid] & PANN_KEYMASK) < k) lo = mid + 1; else hi = mid; }
+    if (i + lo < L) out[i + lo] = fr[i];
+  }
+  for (int j = tid; j < cn; j += nth) {
+    const uint64_t k = c[j] & PANN_KEYMASK;
+    int lo = 0, hi = fn;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if ((fr[mid] & PANN_KEYMASK) < k) lo = mid + 1; else hi = mid; }
+    if (j + lo < L) out[j + lo] = c[j];
+  }
+  const int t = fn + cn;
+  return t < L ? t : L;
+}
+
+template <int DT, int MT, int NW, int CH>
+__global__ void __launch_bounds__(NW * 32, 1) search_emulate_block_kernel(SearchArgs a, EmuArgs e) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nth = NW * 32;
+  const unsigned FULL = 0xFFFFFFFFu;
+  const EmuBlockLayout y = emu_block_layout(a.stride, a.L, a.Ccap, a.R, e.vs_slots, e.capA, e.capB);
+  uint8_t* qs = smem;
+  uint64_t* frA = reinterpret_cast<uint64_t*>(smem + y.fr);
+  uint64_t* frB = frA + a.L;
+  uint64_t* cand = reinterpret_cast<uint64_t*>(smem + y.cand);
+  uint64_t* cand2 = cand + a.Ccap;
+  uint32_t* nbuf = reinterpret_cast<uint32_t*>(smem + y.nbuf);
+  uint32_t* npos = reinterpret_cast<uint32_t*>(smem + y.npos);
+  float* dall = reinterpret_cast<float*>(smem + y.dall);
+  volatile uint32_t* ctrl = reinterpret_cast<volatile uint32_t*>(smem + y.ctrl);
+  uint32_t* vset = reinterpret_cast<uint32_t*>(smem + y.vset);
+  uint32_t* tabA = reinterpret_cast<uint32_t*>(smem + y.tabA);
+  uint32_t* tabB = reinterpret_cast<uint32_t*>(smem + y.tabB);
+  const uint32_t vmask = e.vs_slots - 1;
+  const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
+  const uint32_t nel = a.dl < a.R ? a.dl : a.R;
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) ctrl[0] = atomicAdd(a.job_counter, 1u);
+    __syncthreads();
+    const uint32_t job = ctrl[0];
+    if (job >= njobs) break;
+    const uint32_t qi = a.job_list ? a.job_list[job] : job;
+    const uint32_t rec_id = e.job_rec ? e.job_rec[job] : PANN_PAD;
+    const uint32_t L = a.qL ? a.qL[qi] : a.L;
+    const uint32_t kq = a.qk ? a.qk[qi] : a.k;
+    const uint32_t bits0 = a.qL ? ref_bits(L, a.dl) : e.bits0;
+    const uint32_t self = a.self_ids ? a.self_ids[qi] : PANN_PAD;
+    const uint8_t* qsrc = a.self_ids ? a.points + (uint64_t)self * a.stride : a.queries + (uint64_t)qi * a.stride;
+    for (int c = tid; c < (int)a.nchunks; c += nth) {
+      uint4 v = __ldg(reinterpret_cast<const uint4*>(qsrc) + c);
+      if (DT == DT_F32 && MT == MT_L2) v = make_uint4(v.x ^ 0x80000000u, v.y ^ 0x80000000u, v.z ^ 0x80000000u, v.w ^ 0x80000000u);
+      reinterpret_cast<uint4*>(qs)[c] = v;
+    }
+    for (uint32_t i = tid; i < (1u << bits0); i += nth) tabA[i] = PANN_PAD;
+    for (uint32_t i = tid; i < e.vs_slots; i += nth) vset[i] = PANN_PAD;
+    __syncthreads();
+    EmuHash h;  // used by warp 0 only
+    h.cur = tabA; h.other = tabB; h.cur_cap = e.capA; h.other_cap = e.capB;
+    h.bits = bits0; h.num_entries = 0;
+    int32_t qq = 0;
+    if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), a.nchunks);
+
+    uint64_t* fr = frA;
+    uint64_t* fr2 = frB;
+    int fn, cn;
+    uint32_t cmps;
+    uint64_t nvis;
+    float u0 = 0.0f;
+    bool u0_fresh = true;
+    bool ok = true;
+    if (rec_id != PANN_PAD) {
+      const ResumeLayout ly = resume_layout(a.L, a.Ccap, a.logcap, a.viscap);
+      const uint32_t* rec = a.rec_pool + (size_t)rec_id * a.rec_words;
+      fn = (int)rec[1];
+      cn = (int)rec[2];
+      nvis = rec[3];
+      cmps = rec[4];
+      const uint32_t entries = rec[5];
+      u0 = __uint_as_float(rec[6]);
+      u0_fresh = false;
+      const uint64_t* rfr = reinterpret_cast<const uint64_t*>(rec + ly.fr);
+      const uint64_t* rcand = reinterpret_cast<const uint64_t*>(rec + ly.cand);
+      for (int i = tid; i < fn; i += nth) fr[i] = rfr[i];
+      for (int i = tid; i < cn; i += nth) cand[i] = rcand[i];
+      if (warp == 0) {
+        // the logged ids, inserted in log order (staged in table B, unused until a growth)
+        for (uint32_t i = lane; i < entries; i += 32) h.other[i] = rec[ly.log + i];
+        __syncwarp();
+        emu_place_ranked(h.other, entries, h.cur, (1u << h.bits) - 1, h.other_cap, lane);
+        __syncwarp();
+        h.num_entries = entries;
+      } else {
+        for (uint32_t i = tid - 32; i < (uint32_t)nvis; i += nth - 32) vset_insert(vset, vmask, rec[ly.vis + i]);
+      }
+    } else {
+      for (uint32_t s = tid; s < a.n_start; s += nth) {
+        const uint32_t id = a.starts[s];
+        frB[s] = make_key(point_dist<DT, MT>(a.points + (uint64_t)id * a.stride, qs, a.d, a.nchunks, qq), id);
+      }
+      if (warp == 0) {
+        bool sdummy;
+        for (uint32_t s0 = 0; s0 < a.n_start && ok; s0 += 32)
+          ok = emu_batch(h, s0 + lane < a.n_start ? a.starts[s0 + lane] : PANN_PAD, s0 + lane < a.n_start, lane,
+                         &sdummy);
+        if (lane == 0) ctrl[1] = ok;
+      }
+      __syncthreads();
+      ok = ctrl[1] != 0;
+      block_rank_sort(frB, fr, (int)a.n_start, tid, nth);
+      fn = (int)a.n_start;
+      cn = 0;
+      cmps = a.n_start;
+      nvis = 0;
+    }
+    __syncthreads();
+    uint32_t status = QS_REF_WOULD_GROW;
+    if (!ok) status |= QS_TABLE_FULL;
+
+    while (ok) {
+      // first and second unvisited frontier entries, the number unvisited (every warp alike)
+      int first = -1, second = -1, cnt = 0;
+      for (int b = 0; b < fn; b += 32) {
+        const int i = b + lane;
+        const bool unv = (i < fn) && !(fr[i] & PANN_VFLAG);
+        unsigned m = __ballot_sync(FULL, unv);
+        cnt += __popc(m);
+        if (first < 0 && m) {
+          first = b + __ffs(m) - 1;
+          m &= m - 1;
+        }
+        if (first >= 0 && second < 0 && m) second = b + __ffs(m) - 1;
+      }
+      if (first < 0 || nvis >= a.limit) break;
+      if (warp == 1 && second >= 0 && (uint32_t)lane * 32 < a.R)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[second]) * a.R + 32 * lane));
+      if (u0_fresh) {
+        u0 = key_dist(fr[first]);
+        u0_fresh = false;
+      }
+      if (a.es_count > 0.0 && (double)nvis >= a.es_count && !((double)key_dist(fr[0]) <= a.es_radius) &&
+          !((double)u0 <= a.es_esr))
+        break;  // early_stopping (earlyStopping.h:19-29)
+      const uint64_t cur_key = fr[first];
+      const bool full = (fn == (int)L);
+      const float cutoff = full ? key_dist(fr[fn - 1]) : 3.40282346638528859812e+38F;
+      __syncthreads();  // every thread has read the frontier before it changes
+      nvis++;
+      if (tid == 0) {
+        fr[first] = cur_key | PANN_VFLAG;
+        if (a.vis_keys && nvis <= a.vis_cap) a.vis_keys[(uint64_t)qi * a.vis_cap + (nvis - 1)] = cur_key & PANN_KEYMASK;
+        vset_insert(vset, vmask, key_id(cur_key));
+      }
+      if (nvis > a.vis_cap && a.vis_keys) status |= QS_VISIT_OVERFLOW;
+      if (nvis > (uint64_t)(vmask / 4 * 3)) { status |= QS_INTERNAL; break; }
+      const uint32_t cid = key_id(cur_key);
+      const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
+      if (warp == 0) {
+        // the hashset calls, in adjacency order (:153-159)
+        int nnew = 0;
+        bool full_tab = false;
+        uint32_t vnext = (uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD;
+        for (uint32_t b = 0; b < nel; b += 32) {
+          const uint32_t v = vnext;
+          vnext = (b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD;
+          bool seen = false;
+          if (!emu_batch(h, v, v != PANN_PAD, lane, &seen)) { full_tab = true; break; }
+          const bool isnew = v != PANN_PAD && !seen && v != self;
+          const unsigned mn = __ballot_sync(FULL, isnew);
+          if (isnew) {
+            const int at = nnew + __popc(mn & ((1u << lane) - 1));
+            nbuf[at] = v;
+            npos[at] = b + lane;
+          }
+          nnew += __popc(mn);
+        }
+        if (lane == 0) {
+          ctrl[2] = (uint32_t)nnew;
+          ctrl[3] = full_tab;
+        }
+      } else {
+        // every neighbour scored while warp 0 probes the table
+        for (uint32_t j = tid - 32; j < nel; j += nth - 32) {
+          const uint32_t v = __ldg(grow + j);
+          if (v != PANN_PAD) dall[j] = row_dist_whole<DT, MT, CH>(a.points + (uint64_t)v * a.stride, qs, a.nchunks, qq);
+        }
+      }
+      __syncthreads();
+      const int nnew = (int)ctrl[2];
+      if (ctrl[3]) {
+        status |= QS_TABLE_FULL;
+        break;
+      }
+      cmps += (uint32_t)nnew;
+      if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
+      if (warp == 0) {
+        for (int b = 0; b < nnew; b += 32) {
+          const int i = b + lane;
+          float dv = 0.0f;
+          uint32_t v = 0;
+          if (i < nnew) {
+            v = nbuf[i];
+            dv = dall[npos[i]];
+          }
+          const bool keep = i < nnew && !(dv >= cutoff);
+          const unsigned m = __ballot_sync(FULL, keep);
+          if (keep) cand[cn + __popc(m & ((1u << lane) - 1))] = make_key(dv, v);
+          cn += __popc(m);
+        }
+        if (lane == 0) ctrl[4] = (uint32_t)cn;
+      }
+      __syncthreads();
+      cn = (int)ctrl[4];
+      if (cn == 0 || (a.limit >= 2ull * L && (double)cn < a.batch_factor * (double)L && cnt - 1 >= 1)) continue;
+      block_rank_sort(cand, cand2, cn, tid, nth);
+      __syncthreads();
+      // unique by id, drop ids already in the frontier, mark ids visited before (order kept)
+      int un = 0;
+      for (int b = 0; b < cn; b += nth) {
+        const int i = b + tid;
+        bool keepc = false;
+        uint64_t k = 0;
+        if (i < cn) {
+          k = cand2[i];
+          keepc = !(i > 0 && key_id(cand2[i - 1]) == key_id(k)) && !frontier_has(fr, fn, k);
+          if (keepc && vset_has(vset, vmask, key_id(k))) k |= PANN_VFLAG;
+        }
+        const unsigned mk = __ballot_sync(FULL, keepc);
+        if (lane == 0) ctrl[8 + warp] = __popc(mk);
+        __syncthreads();
+        int before = 0, tot = 0;
+        for (int w = 0; w < NW; w++) {
+          const int c = (int)ctrl[8 + w];
+          before += w < warp ? c : 0;
+          tot += c;
+        }
+        if (keepc) cand[un + before + __popc(mk & ((1u << lane) - 1))] = k;
+        un += tot;
+        __syncthreads();
+      }
+      fn = block_merge(fr, fn, cand, un, fr2, (int)L, tid, nth);
+      u0_fresh = true;
+      uint64_t* t = fr; fr = fr2; fr2 = t;
+      cn = 0;
+      __syncthreads();
+    }
+    __syncthreads();
+
+    if (status & QS_TABLE_FULL) {
+      if (tid == 0) {
+        if (e.overflow_list) {
+          const uint32_t pos = atomicAdd(e.overflow_count, 1u);
+          e.overflow_list[pos] = qi;
+          e.overflow_rec[pos] = rec_id;
+        }
+        if (a.out_status) a.out_status[qi] = status;
+      }
+      continue;
+    }
+    if (status & QS_INTERNAL) {
+      if (tid == 0 && a.out_status) a.out_status[qi] = status;
+      continue;
+    }
+    if (warp == 0 && h.bits == bits0) status &= ~(uint32_t)QS_REF_WOULD_GROW;
+    if ((uint32_t)fn < kq) status |= QS_SHORT;
+    for (uint32_t j = tid; j < a.kstride; j += nth) {
+      const bool okk = j < (uint32_t)fn && j < kq;
+      a.out_ids[(uint64_t)qi * a.kstride + j] = okk ? key_id(fr[j]) : PANN_PAD;
+      if (a.out_dists) a.out_dists[(uint64_t)qi * a.kstride + j] = okk ? key_dist(fr[j]) : 0.0f;
+    }
+    if (tid == 0) {
+      if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;
+      if (a.out_cmps) a.out_cmps[qi] = cmps;
+      if (a.out_status) a.out_status[qi] = status;
+    }
   }
 }
 

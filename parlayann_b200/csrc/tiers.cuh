@@ -48,6 +48,10 @@ cudaError_t launch_search(int dtype, int metric, bool global_table, const Search
                           size_t smem, cudaStream_t st, int prec);
 cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
                            int blocks, size_t smem, cudaStream_t st);
+// Warps per block of the shared-memory emulation tier (one query per block).
+constexpr int EMU_BLOCK_WARPS = 4;
+cudaError_t launch_emulate_block(int dtype, int metric, const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem,
+                                 cudaStream_t st);
 int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem);
 uint32_t tier0_slots(const SearchPlan& p, uint32_t R);
 

@@ -166,3 +166,24 @@ def test_quantized_search_edge_cases(lib_built):
     with pytest.raises(P.PannError):
         idx.search_quantized(q, 21, 20)                     # k > beam
     idx.close()
+
+
+@pytest.mark.parametrize("metric", [P.L2, P.MIPS], ids=["l2", "mips"])
+def test_score_pairs_exact_and_low_precision(mix_index, metric):
+    """pann_score: the exact scores are Point::distance bit for bit; the bfloat16 / FP8 scores stay
+    within their precision's error of the FP64 distance."""
+    base, q, out = mix_index
+    idx, gt = out[metric]
+    rng = np.random.default_rng(4)
+    ids = np.concatenate([gt, rng.integers(0, base.shape[0], (q.shape[0], 6))], axis=1).astype(np.uint32)
+    ex = idx.score(q, ids)
+    np.testing.assert_array_equal(ex.view(np.uint32), P.point_distances(q, base, ids, metric).view(np.uint32))
+    rows = base[ids.ravel().astype(np.int64)].reshape(ids.shape + (base.shape[1],)).astype(np.float64)
+    q64 = q.astype(np.float64)[:, None, :]
+    d64 = ((rows - q64) ** 2).sum(-1) if metric == P.L2 else -(rows * q64).sum(-1)
+    for prec, tol in ((P.PREC_BF16, 0.02), (P.PREC_FP8, 0.2)):
+        idx.set_precision(prec)
+        lp = idx.score(q, ids, prec).astype(np.float64)
+        # absolute error relative to the scale of the distances (|q||b| = 1 here)
+        assert np.abs(lp - d64).max() < tol, (prec, np.abs(lp - d64).max())
+    idx.set_precision(P.PREC_F32)

@@ -258,3 +258,34 @@ def test_groundtruth_matches_oracle(dtype, metric, lib_built):
     np.testing.assert_array_equal(ids, oi)
     np.testing.assert_array_equal(dd, od)
     idx.close()
+
+
+@pytest.mark.parametrize("metric", [P.L2, P.MIPS])
+@pytest.mark.parametrize("k", [10, 20, 100])
+def test_groundtruth_float_fast_path_equals_plain_kernel(metric, k, lib_built, monkeypatch):
+    """The float32 candidate pass + FP64 re-rank gives the plain FP64 kernel's answers exactly."""
+    base = P.synth_mixture(P.F32, 200_000, 96, 64, 5, 0, sigma=0.3, normalize=True)
+    q = P.synth_mixture(P.F32, 300, 96, 64, 5, 1, sigma=0.3, normalize=True)
+    idx = P.Index(base, 8, metric)
+    ids, dd = idx.groundtruth(q, k)
+    monkeypatch.setenv("PANN_GT_PLAIN", "1")
+    pi, pd = idx.groundtruth(q, k)
+    np.testing.assert_array_equal(ids, pi)
+    np.testing.assert_array_equal(dd, pd)
+    idx.close()
+
+
+def test_groundtruth_float_fast_path_with_duplicates(lib_built):
+    """Thousands of copies of one point: equal distances defeat the margin test for the queries
+    near it, which the plain kernel then answers (ties by id)."""
+    rng = np.random.default_rng(8)
+    base = rng.standard_normal((60_000, 32)).astype(np.float32)
+    base[10_000:14_000] = base[5]
+    q = np.concatenate([base[5:6] + 1e-3 * rng.standard_normal((4, 32)).astype(np.float32),
+                        rng.standard_normal((40, 32)).astype(np.float32)])
+    idx = P.Index(base, 8)
+    ids, dd = idx.groundtruth(q, 20)
+    oi, od = O.groundtruth(base, q, 20)
+    np.testing.assert_array_equal(ids, oi)
+    np.testing.assert_array_equal(dd, od)
+    idx.close()
