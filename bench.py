@@ -392,7 +392,10 @@ def _timed(step, flush, stream, steps, warmup):
     return tot / steps
 
 
-PRECISION_FORMS = (("bf16", 1, 0), ("fp8", 2, 0), ("bf16_tile2", 1, 2), ("fp8_tile2", 2, 2), ("fp8_tile3", 2, 3))
+# (name, precision, parents, scorer): scorer 1 scores the tile search's staged rows on the tensor cores
+PRECISION_FORMS = (("bf16", 1, 0, 0), ("fp8", 2, 0, 0), ("bf16_tile2", 1, 2, 0), ("fp8_tile2", 2, 2, 0),
+                   ("fp8_tile3", 2, 3, 0), ("bf16_tile2_tc", 1, 2, 1), ("fp8_tile2_tc", 2, 2, 1),
+                   ("fp8_tile3_tc", 2, 3, 1))
 
 
 def scoring_error(idx, base, q, ids, prec, metric):
@@ -427,22 +430,22 @@ def precision_forms(idx, base, q, gt, metric, beam, qps_plain, dev, flush, strea
     dq = torch.from_numpy(q).to(dev)
     exact_rec_at_beam = P.recall_with_ties(idx.search(q, k, beam).ids, gt, k, q, base, metric)
     out = {}
-    for name, prec, parents in forms:
+    for name, prec, parents, scorer in forms:
         idx.set_precision(prec)
         pbeam, prec_rec, pres = None, None, None
         for L in BEAMS:
             if L < beam - 10:
                 continue
-            r = idx.search(q, k, L, precision=prec, parents=parents)
+            r = idx.search(q, k, L, precision=prec, parents=parents, scorer=scorer)
             rec = P.recall_with_ties(r.ids, gt, k, q, base, metric)
             if rec >= 0.95:
                 pbeam, prec_rec, pres = L, rec, r
                 break
         if pbeam is None:
             continue
-        same_beam = idx.search(q, k, beam, precision=prec, parents=parents)
+        same_beam = idx.search(q, k, beam, precision=prec, parents=parents, scorer=scorer)
         loss = exact_rec_at_beam - P.recall_with_ties(same_beam.ids, gt, k, q, base, metric)
-        b = idx.batch(nq, k, pbeam, precision=prec, parents=parents)
+        b = idx.batch(nq, k, pbeam, precision=prec, parents=parents, scorer=scorer)
         d_ids = torch.empty((nq, k), dtype=torch.int32, device=dev)
         d_d = torch.empty((nq, k), dtype=torch.float32, device=dev)
         ks = np.full(nq, k, np.uint32)
@@ -461,7 +464,8 @@ def precision_forms(idx, base, q, gt, metric, beam, qps_plain, dev, flush, strea
         assert np.array_equal(ids_b, pres.ids), "batched precision form differs from the plain precision form"
         exact_d = idx.score(q[:2000], pres.ids[:2000])
         rep_err = np.abs(pres.dists[:2000].astype(np.float64) - exact_d) / np.maximum(np.abs(exact_d), 1e-30)
-        out[name] = {"beam": pbeam, "parents": parents, "recall_at_10": round(prec_rec, 4),
+        out[name] = {"beam": pbeam, "parents": parents, "scorer": "tensor cores (tcgen05)" if scorer else "CUDA cores",
+                     "recall_at_10": round(prec_rec, 4),
                      "stopped_early": int(((pres.flags & 2) != 0).sum()), "qps_batched_graph": round(nq / t, 1),
                      "speedup_vs_plain": round(nq / t / qps_plain, 3),
                      "recall_loss_at_plain_beam": round(loss, 4),
@@ -801,17 +805,18 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
 
     rng = np.random.default_rng(7)
     rp = P.RangeParams(20, P.RANGE_GREEDY, radius, 0.0, 0)
-    forms = [("plain", P.PREC_F32, 0, beam)]
+    forms = [("plain", P.PREC_F32, 0, beam, 0)]
     best = max(prec_out.items(), key=lambda kv: kv[1]["qps_batched_graph"]) if prec_out else None
     if best is not None:
         nm, info = best
-        forms.append((nm, P.PREC_BF16 if nm.startswith("bf16") else P.PREC_FP8, info["parents"], info["beam"]))
+        forms.append((nm, P.PREC_BF16 if nm.startswith("bf16") else P.PREC_FP8, info["parents"], info["beam"],
+                      1 if nm.endswith("_tc") else 0))
     serving = {}
-    for fname, prec, parents, kbeam in forms:
+    for fname, prec, parents, kbeam, scorer in forms:
         if prec != P.PREC_F32:
             idx.set_precision(prec)
         srv = P.Server(idx, max_batch_queries=4096, inflight=3, max_k=100, max_beam=max(200, kbeam), precision=prec,
-                       parents=parents)
+                       parents=parents, scorer=scorer)
 
         def schedule(n, rate_qps, range_frac):
             nqs = rng.integers(1, 257, n)

@@ -200,7 +200,15 @@ typedef struct {
                         frontier nodes per step and scoring their new neighbours as one tile staged in
                         shared memory; its own visiting order and recall curve. Status bit 32 marks a
                         query whose seen set filled (it stopped early). */
+  uint32_t scorer;   /* tile search only: PANN_SCORER_CUDA scores each staged row on the CUDA cores (one
+                        row a thread, float32 FMA); PANN_SCORER_TENSOR scores 128 staged rows at a time
+                        on the tensor cores (tcgen05.mma, float32 accumulation in tensor memory; the
+                        query split into bfloat16 hi + lo, or three FP8 terms), with the rows' squared
+                        norms precomputed by pann_index_set_precision. Rows must be a whole number of
+                        32-byte MMA steps (bfloat16: d a multiple of 16; FP8: of 32). */
 } pann_search_options;
+#define PANN_SCORER_CUDA 0
+#define PANN_SCORER_TENSOR 1
 
 /* Distances of given (query, point) pairs: queries nq rows (host), ids nq x m
  * point ids (host), out nq x m (host). PANN_PREC_F32 gives Point::distance
@@ -372,6 +380,7 @@ typedef struct {
   double batch_factor;
   int32_t precision;          /* PANN_PREC_*; low precision needs pann_index_set_precision first */
   uint32_t parents;           /* pann_search_options::parents of every k-NN request */
+  uint32_t scorer;            /* pann_search_options::scorer of every k-NN request */
 } pann_server_options;
 
 int pann_server_create(pann_server** out, pann_index* idx, const pann_server_options* opt, const uint32_t* starts,

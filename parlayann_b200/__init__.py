@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(_HERE, "libparlayann_b200.so")
 
 PANN_OK, PANN_EINVAL, PANN_ENOMEM, PANN_ETIMEOUT, PANN_EDEVICE, PANN_EOVERFLOW, PANN_ESHORT = range(7)
 U8, I8, F32 = 0, 1, 2
+SCORER_CUDA, SCORER_TENSOR = 0, 1  # pann_search_options::scorer (tile search)
 L2, MIPS = 0, 1
 PREC_F32, PREC_BF16, PREC_FP8 = 0, 1, 2
 PANN_NOALLOC_SCRATCH_BYTES = 32 << 20  # static scratch of pann_search_device_noalloc, per device
@@ -52,7 +53,8 @@ class QueryParams(ctypes.Structure):
 class SearchOptions(ctypes.Structure):
     """pann_search_options: precision form and re-rank count."""
 
-    _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32), ("parents", ctypes.c_uint32)]
+    _fields_ = [("precision", ctypes.c_int32), ("rerank", ctypes.c_uint32), ("parents", ctypes.c_uint32),
+                ("scorer", ctypes.c_uint32)]
 
 
 class BatchOptions(ctypes.Structure):
@@ -77,7 +79,8 @@ class ServerOptions(ctypes.Structure):
 
     _fields_ = [("max_batch_queries", ctypes.c_uint32), ("inflight", ctypes.c_uint32), ("max_k", ctypes.c_uint32),
                 ("max_beam", ctypes.c_uint32), ("limit", ctypes.c_uint64), ("degree_limit", ctypes.c_uint32),
-                ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32), ("parents", ctypes.c_uint32)]
+                ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32), ("parents", ctypes.c_uint32),
+                ("scorer", ctypes.c_uint32)]
 
 
 class BuildParams(ctypes.Structure):
@@ -337,7 +340,7 @@ class Index:
 
     def search(self, queries: np.ndarray, k: int, L: int, limit: int | None = None, degree_limit: int | None = None,
                batch_factor: float = 0.125, starts=(0,), allow_short: bool = False, precision: int = PREC_F32,
-               rerank: int = 0, parents: int = 0) -> SearchResult:
+               rerank: int = 0, parents: int = 0, scorer: int = 0) -> SearchResult:
         queries = np.ascontiguousarray(queries, dtype=_NP_OF[self.dtype])
         nq = queries.shape[0]
         qp = QueryParams(k, L, self.n if limit is None else limit, self.R if degree_limit is None else degree_limit,
@@ -352,7 +355,7 @@ class Index:
             rc = lib().pann_search(self._h, _ptr(queries), nq, ctypes.byref(qp), _ptr(st), len(st), _ptr(ids),
                                    _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags))
         else:
-            opt = SearchOptions(precision, rerank, parents)
+            opt = SearchOptions(precision, rerank, parents, scorer)
             rc = lib().pann_search_ex(self._h, _ptr(queries), nq, ctypes.byref(qp), ctypes.byref(opt), _ptr(st),
                                       len(st), _ptr(ids), _ptr(dists), _ptr(vis), _ptr(cmps), _ptr(flags), 0, None)
         if not (allow_short and rc == PANN_ESHORT):
@@ -362,10 +365,10 @@ class Index:
     def batch(self, max_queries: int, max_k: int, max_beam: int, limit: int | None = None,
               degree_limit: int | None = None, batch_factor: float = 0.125, starts=(0,), precision: int = PREC_F32,
               rerank: int = 0, use_graph: bool = True, autotune: bool = False, seen_slots: int = 0,
-              warps_per_block: int = 0, parents: int = 0) -> "Batch":
+              warps_per_block: int = 0, parents: int = 0, scorer: int = 0) -> "Batch":
         """A reusable batch for queries with per-query k and beam (pann_batch_create)."""
         return Batch(self, max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts, precision, rerank,
-                     use_graph, autotune, seen_slots, warps_per_block, parents)
+                     use_graph, autotune, seen_slots, warps_per_block, parents, scorer)
 
     def range_search(self, queries: np.ndarray, beam: int, radius: float, rtype: int = RANGE_GREEDY, start: int = 0,
                      early_stopping_radius: float = 0.0, early_stopping_count: int = 0):
@@ -437,13 +440,13 @@ class Batch:
     graph). Per query the results equal Index.search with that k and beam."""
 
     def __init__(self, index: "Index", max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts,
-                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block, parents=0):
+                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block, parents=0, scorer=0):
         self.index = index
         self.max_k = max_k
         qp = QueryParams(max_k, max_beam, index.n if limit is None else limit,
                          index.R if degree_limit is None else degree_limit, batch_factor)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
-        opt = SearchOptions(precision, rerank, parents)
+        opt = SearchOptions(precision, rerank, parents, scorer)
         bo = BatchOptions(int(use_graph), int(autotune), seen_slots, warps_per_block)
         h = ctypes.c_void_p()
         _check(lib().pann_batch_create(ctypes.byref(h), index.handle, max_queries, ctypes.byref(qp), _ptr(st), len(st),
@@ -494,10 +497,12 @@ class Server:
 
     def __init__(self, index: "Index", max_batch_queries: int = 1024, inflight: int = 3, max_k: int = 100,
                  max_beam: int = 400, limit: int | None = None, degree_limit: int | None = None,
-                 batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,), parents: int = 0):
+                 batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,), parents: int = 0,
+                 scorer: int = 0):
         self.index = index
         o = ServerOptions(max_batch_queries, inflight, max_k, max_beam, index.n if limit is None else limit,
-                          index.R if degree_limit is None else degree_limit, batch_factor, precision, parents)
+                          index.R if degree_limit is None else degree_limit, batch_factor, precision, parents,
+                          scorer)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
         h = ctypes.c_void_p()
         _check(lib().pann_server_create(ctypes.byref(h), index.handle, ctypes.byref(o), _ptr(st), len(st)))

@@ -29,6 +29,7 @@ struct pann_batch {
   int prec = 0;
   uint32_t rerank = 0;
   uint32_t parents = 0;
+  uint32_t scorer = 0;
   pann_batch_options bopt{};
   pann::TierSizes z{};
   // device buffers, allocated at creation
@@ -86,7 +87,8 @@ static int enqueue(pann_batch* b, const TierSizes& z, cudaStream_t st) {
   if (b->parents > 0 && b->prec != PREC_F32) {
     a.job_list = b->order.as<uint32_t>();
     a.njobs_dev = b->counters.as<uint32_t>() + 32;
-    int rc = enqueue_tile(idx, b->plan, a, b->parents, b->counters.as<uint32_t>() + 10, b->prec, b->rerank, st);
+    int rc = enqueue_tile(idx, b->plan, a, b->parents, b->counters.as<uint32_t>() + 10, b->prec, b->rerank, st,
+                          b->scorer);
     if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; the single-parent tiers below
   }
   return enqueue_tiers(idx, b->plan, a, z, tier_bufs(b), st, b->prec, b->rerank);
@@ -171,6 +173,7 @@ int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, c
   b->prec = prec;
   b->rerank = opt ? opt->rerank : 0;
   b->parents = opt ? opt->parents : 0;
+  b->scorer = opt ? opt->scorer : 0;
   if (bopt) b->bopt = *bopt;
   auto bail = [&](int code) {
     pann_batch_destroy(b);

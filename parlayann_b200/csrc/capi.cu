@@ -102,6 +102,30 @@ __global__ void to_fp8_kernel(const float* __restrict__ src, uint64_t src_stride
   }
 }
 
+// Squared norm of every low-precision row as the tensor-core tile scoring
+// uses it: the row dequantized exactly (bfloat16, or E4M3 x the dimension's
+// scale), squared and summed in float32.
+template <int PREC>
+__global__ void lp_norms_kernel(const uint8_t* __restrict__ rows, uint64_t stride, uint64_t n, uint32_t d,
+                                const float* __restrict__ scales, float* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint8_t* r = rows + i * stride;
+    float s = 0.0f;
+    for (uint32_t t = 0; t < d; t++) {
+      float x;
+      if (PREC == PREC_BF16) {
+        x = __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(r)[t]);
+      } else {
+        __nv_fp8_e4m3 f;
+        *reinterpret_cast<uint8_t*>(&f) = r[t];
+        x = float(f) * scales[t];
+      }
+      s = fmaf(x, x, s);
+    }
+    out[i] = s;
+  }
+}
+
 int smem_attr_max() {
   static int cached[64] = {};
   int dev = 0;
@@ -512,7 +536,7 @@ SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
-               int precision, uint32_t rerank, uint32_t parents) {
+               int precision, uint32_t rerank, uint32_t parents, uint32_t scorer) {
   if (nq == 0) return PANN_OK;
   if (precision != PREC_F32 && idx->lp_prec != precision)
     return fail(PANN_EINVAL, "pann_index_set_precision was not called for this precision");
@@ -520,7 +544,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     PANN_CUDA(idx->counters.ensure(64));
     SearchArgs a = base_args(idx, plan, d_queries, nullptr, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
                              nullptr, 0);
-    int rc = enqueue_tile(idx, plan, a, parents, idx->counters.as<uint32_t>() + 10, precision, rerank, st);
+    int rc = enqueue_tile(idx, plan, a, parents, idx->counters.as<uint32_t>() + 10, precision, rerank, st, scorer);
     if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; take the single-parent path
   }
   TierSizes z;
@@ -848,6 +872,7 @@ int pann_index_set_precision(pann_index* idx, int precision) {
   if (precision == PANN_PREC_F32) {
     idx->lp_rows.release();
     idx->lp_scales.release();
+    idx->lp_norms.release();
     idx->lp_prec = 0;
     return PANN_OK;
   }
@@ -893,6 +918,15 @@ int pann_index_set_precision(pann_index* idx, int precision) {
     PANN_CUDA(cudaStreamSynchronize(st));
     dinv.release();
   }
+  PANN_CUDA(idx->lp_norms.ensure(4ull * std::max<uint64_t>(n, 1)));
+  const int nb = (int)std::min<uint64_t>((n + 255) / 256, 65535ull);
+  if (precision == PANN_PREC_BF16)
+    lp_norms_kernel<PREC_BF16><<<nb, 256, 0, st>>>(idx->lp_rows.as<uint8_t>(), idx->lp_stride, n, d,
+                                                   idx->lp_scales.as<float>(), idx->lp_norms.as<float>());
+  else
+    lp_norms_kernel<PREC_FP8><<<nb, 256, 0, st>>>(idx->lp_rows.as<uint8_t>(), idx->lp_stride, n, d,
+                                                  idx->lp_scales.as<float>(), idx->lp_norms.as<float>());
+  PANN_CUDA(cudaGetLastError());
   PANN_CUDA(cudaStreamSynchronize(st));
   idx->lp_prec = precision;
   return PANN_OK;
@@ -908,6 +942,7 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
   const int prec = opt ? opt->precision : PANN_PREC_F32;
   const uint32_t rerank = opt ? opt->rerank : 0;
   const uint32_t parents = opt ? opt->parents : 0;
+  const uint32_t scorer = opt ? opt->scorer : 0;
   SearchPlan plan;
   rc = make_plan(idx, qp, n_start, &plan);
   if (rc) return rc;
@@ -944,7 +979,7 @@ int pann_search_ex(pann_index* idx, const void* queries, uint32_t nq, const pann
     d_status = idx->status.as<uint32_t>();
   }
   rc = run_search(idx, plan, q, nullptr, nq, idx->starts.as<uint32_t>(), d_ids, d_dists, d_vis, d_cmps, d_status,
-                  nullptr, 0, st, prec, rerank, parents);
+                  nullptr, 0, st, prec, rerank, parents, scorer);
   if (rc || on_device) return rc;
   if (k) {
     PANN_CUDA(cudaMemcpyAsync(out_ids, d_ids, 4 * k * nq, cudaMemcpyDeviceToHost, st));

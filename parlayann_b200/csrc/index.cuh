@@ -66,7 +66,7 @@ struct pann_index {
   pann::DevBuf range_meta, range_tabs, range_pool, range_out;
   uint64_t range_held = 0;  // ids in range_out left for pann_range_fetch (0: none)
   // precision form: low-precision copy of float32 points (lowprec.cuh)
-  pann::DevBuf lp_rows, lp_scales;
+  pann::DevBuf lp_rows, lp_scales, lp_norms;
   int lp_prec = 0;
   uint64_t lp_stride = 0;
   uint32_t lp_chunks = 0;
@@ -101,6 +101,6 @@ int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_sta
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
-               int precision = 0, uint32_t rerank = 0, uint32_t parents = 0);
+               int precision = 0, uint32_t rerank = 0, uint32_t parents = 0, uint32_t scorer = 0);
 
 }  // namespace pann

@@ -93,6 +93,7 @@ struct SearchArgs {
   uint64_t lp_stride;
   uint32_t lp_chunks;
   const float* lp_scales;
+  const float* lp_norms;  // squared norm of every low-precision row (tensor-core tile scoring)
   uint32_t rerank;
   // early stopping of range search (earlyStopping.h:19-29); es_count == 0 disables it
   double es_count;   // QP.early_stopping_count

@@ -305,7 +305,7 @@ int pann_server_create(pann_server** out, pann_index* idx, const pann_server_opt
   s->starts.assign(starts, starts + n_start);
   cudaGetDevice(&s->device);
   pann_query_params bounds{opt->max_k, opt->max_beam, opt->limit, opt->degree_limit, opt->batch_factor};
-  pann_search_options so{opt->precision, 0, opt->parents};
+  pann_search_options so{opt->precision, 0, opt->parents, opt->scorer};
   pann_batch_options bo{1, 0, 0, 0};
   s->row_bytes = (size_t)idx->d * idx->esize;
   s->slots.resize(opt->inflight);

@@ -63,7 +63,7 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
                   const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank);
 // The multi-parent tile search of the precision form (tile.cu).
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
-                 int precision, uint32_t rerank, cudaStream_t st);
+                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer = 0);
 // Validates the start points and copies them to idx->starts (cached).
 int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st);
 // The index's own tier buffers for nq queries (grown as needed).

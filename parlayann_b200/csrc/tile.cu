@@ -24,26 +24,34 @@
 #include "index.cuh"
 #include "lowprec.cuh"
 #include "tiers.cuh"
+#include "umma.cuh"
 
 namespace pann {
 
 enum : uint32_t { QS_TRUNCATED = 32u };  // the seen table filled: the search stopped early
 
 struct TileLayout {
-  size_t q, sc, fr, fr2, cand, cid, table, stage, misc, total;
-  uint32_t sstride;  // staged row stride (bytes)
+  size_t q, sc, fr, fr2, cand, cid, table, stage, misc, qb, nrm, tcw, total;
+  uint32_t sstride;  // staged row stride (bytes; CUDA-core scoring)
 };
 
+// Rows a tensor-core scoring round takes: the MMA's M.
+constexpr uint32_t TC_ROWS = 128;
+
 // CW: candidates a step can produce (parents x degree); CWs: rows staged at
-// once (a step with more candidates stages and scores them in rounds).
+// once (a step with more candidates stages and scores them in rounds). With
+// tensor-core scoring (tc) the rows are staged TC_ROWS at a time in the
+// core-matrix layout (umma.cuh), beside the query operand (16 rows: the
+// query's split terms, the rest zero), the staged rows' squared norms and the
+// MMA barrier and tensor-memory address.
 __host__ __device__ inline TileLayout tile_layout(uint32_t d, uint32_t L, uint32_t CW, uint32_t S,
-                                                  uint64_t lp_stride, uint32_t CWs) {
+                                                  uint64_t lp_stride, uint32_t CWs, bool tc = false) {
   TileLayout t{};
   size_t o = 0;
   const size_t dpad = (d + 3) & ~3u;
   // rows at an odd multiple of 16 bytes apart: conflict-free 16-byte reads
   t.sstride = (uint32_t)(((lp_stride / 16) % 2 == 0) ? lp_stride + 16 : lp_stride);
-  // every region starts on a 16-byte boundary (cp.async destinations need it)
+  // every region starts on a 16-byte boundary (cp.async destinations and MMA operands need it)
 #define PANN_TILE_TAKE(field, bytes) \
   t.field = o;                        \
   o += ((size_t)(bytes) + 15) & ~(size_t)15;
@@ -54,7 +62,14 @@ __host__ __device__ inline TileLayout tile_layout(uint32_t d, uint32_t L, uint32
   PANN_TILE_TAKE(cand, 8ull * (CW > L ? CW : L))
   PANN_TILE_TAKE(cid, 4ull * CW)
   PANN_TILE_TAKE(table, 4ull * S)
-  PANN_TILE_TAKE(stage, (size_t)CWs * t.sstride)
+  if (tc) {
+    PANN_TILE_TAKE(stage, (size_t)TC_ROWS * lp_stride)
+    PANN_TILE_TAKE(qb, 16 * lp_stride)
+    PANN_TILE_TAKE(nrm, 4ull * TC_ROWS)
+    PANN_TILE_TAKE(tcw, 16)
+  } else {
+    PANN_TILE_TAKE(stage, (size_t)CWs * t.sstride)
+  }
   PANN_TILE_TAKE(misc, 64)
 #undef PANN_TILE_TAKE
   t.total = o;
@@ -135,7 +150,21 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(gmem_src) : "memory");
 }
 
-template <int MT, int PREC>
+// Time the MMA barrier is waited for before a round is given up (one second,
+// far beyond any MMA's latency; the query is then marked QS_INTERNAL).
+constexpr uint64_t TC_WAIT_LIMIT = 1000000000ull;
+
+// TC: score each staged round on the tensor cores (tcgen05.mma, M = 128 rows,
+// N = 16, float32 accumulator in tensor memory) instead of one row per thread
+// on the CUDA cores. The A operand is the staged rows as stored (bfloat16, or
+// E4M3 of x / s_t); the B operand is the query split into terms that the
+// operand format holds exactly: bfloat16 hi + lo, or for FP8 three E4M3 terms
+// of s_t q_t, each scaled by a power of two into the format's range. The MMA
+// gives each row's dot product with every term; their sum is b.q to about
+// float32 accuracy, and the Euclidean score is |b|^2 - 2 b.q + |q|^2 with the
+// row's squared norm precomputed (SearchArgs::lp_norms). The traversal, the
+// cutoff, the merge and the exact re-rank are those of the CUDA-core scoring.
+template <int MT, int PREC, bool TC>
 __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t W, uint32_t S, uint32_t CW,
                                                           uint32_t CWs) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -143,7 +172,7 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
   const int lane = tid & 31;
   const int warp = tid >> 5;
   const unsigned FULL = 0xFFFFFFFFu;
-  const TileLayout ly = tile_layout(a.d, a.L, CW, S, a.lp_stride, CWs);
+  const TileLayout ly = tile_layout(a.d, a.L, CW, S, a.lp_stride, CWs, TC);
   float* qf = reinterpret_cast<float*>(smem + ly.q);
   float* sc = reinterpret_cast<float*>(smem + ly.sc);
   uint64_t* frA = reinterpret_cast<uint64_t*>(smem + ly.fr);
@@ -160,6 +189,19 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
   if (PREC == PREC_FP8)
     for (uint32_t i = tid; i < a.d; i += blockDim.x) sc[i] = a.lp_scales[i];
   const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
+  // tensor-core state: the MMA barrier, the tensor-memory columns (32, of
+  // which the 16 of N are used), the barrier's phase
+  uint32_t bar = 0, tmem = 0, phase = 0;
+  bool tc_ok = true;
+  if (TC) {
+    bar = smem_u32(smem + ly.tcw);
+    if (warp == 0) tmem_alloc(smem_u32(smem + ly.tcw + 8), 32);
+    if (tid == 0) mbar_init(bar, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    tmem = *reinterpret_cast<volatile uint32_t*>(smem + ly.tcw + 8);
+  }
 
   for (;;) {
     __syncthreads();
@@ -177,6 +219,57 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
     for (uint32_t i = tid; i < Sq; i += blockDim.x) table[i] = PANN_PAD;
     if (tid < 15) misc[1 + tid] = 0;
     __syncthreads();
+    float tc_qn = 0.0f, tc_unscale = 1.0f;
+    if (TC) {
+      // the query operand: 16 rows of lp_chunks chunks, rows past the split terms zero
+      uint8_t* qb = smem + ly.qb;
+      for (uint32_t i = tid; i < 16 * a.lp_chunks * 4; i += blockDim.x) reinterpret_cast<uint32_t*>(qb)[i] = 0u;
+      // |q|^2 (Euclidean) and, for FP8, max |s_t q_t| (float bits; non-negative floats order as integers)
+      float part = 0.0f, mx = 0.0f;
+      for (uint32_t t = tid; t < a.d; t += blockDim.x) {
+        part += qf[t] * qf[t];
+        if (PREC == PREC_FP8) mx = fmaxf(mx, fabsf(sc[t] * qf[t]));
+      }
+      for (int o = 16; o; o >>= 1) {
+        part += __shfl_xor_sync(FULL, part, o);
+        mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+      }
+      if (lane == 0) {
+        atomicAdd(reinterpret_cast<float*>(misc + 10), part);
+        atomicMax(misc + 11, __float_as_uint(mx));
+      }
+      __syncthreads();
+      tc_qn = __uint_as_float(misc[10]);
+      // FP8 terms: v = s_t q_t 2^e0 with max |v| in [128, 256); three E4M3 terms of 4 bits each
+      int e0 = 0;
+      if (PREC == PREC_FP8) {
+        const float m = __uint_as_float(misc[11]);
+        int ex = 0;
+        if (m > 0.0f) frexpf(m, &ex);
+        e0 = 8 - ex;
+        tc_unscale = ldexpf(1.0f, -e0);
+      }
+      for (uint32_t t = tid; t < a.d; t += blockDim.x) {
+        if (PREC == PREC_BF16) {
+          const __nv_bfloat16 hi = __float2bfloat16_rn(qf[t]);
+          const __nv_bfloat16 lo = __float2bfloat16_rn(qf[t] - __bfloat162float(hi));
+          const uint32_t c = (2 * t) / 16, b = (2 * t) % 16;
+          *reinterpret_cast<__nv_bfloat16*>(qb + cm_offset(0, c, a.lp_chunks) + b) = hi;
+          *reinterpret_cast<__nv_bfloat16*>(qb + cm_offset(1, c, a.lp_chunks) + b) = lo;
+        } else {
+          float v = ldexpf(sc[t] * qf[t], e0);
+          const uint32_t c = t / 16, b = t % 16;
+#pragma unroll
+          for (uint32_t j = 0; j < 3; j++) {
+            const __nv_fp8_e4m3 f(v);
+            qb[cm_offset(j, c, a.lp_chunks) + b] = *reinterpret_cast<const uint8_t*>(&f);
+            v = (v - float(f)) * 16.0f;
+          }
+        }
+      }
+      fence_async_smem();
+      __syncthreads();
+    }
     // start points: approximate distances from global rows, all in the seen set
     for (uint32_t s = tid; s < a.n_start; s += blockDim.x) {
       const uint32_t id = a.starts[s];
@@ -262,24 +355,60 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
       __syncthreads();
       const uint32_t ncand = misc[1];
       const float cutoff = fn == L ? key_dist(fr[L - 1]) : 3.40282346638528859812e+38F;
-      for (uint32_t c0 = 0; c0 < ncand; c0 += CWs) {
+      for (uint32_t c0 = 0; c0 < ncand && tc_ok; c0 += CWs) {
         const uint32_t nr = ncand - c0 < CWs ? ncand - c0 : CWs;
         // ---- stage the tile's rows (one round trip per CWs rows)
         for (uint32_t x = tid; x < nr * a.lp_chunks; x += blockDim.x) {
           const uint32_t r = x / a.lp_chunks, c = x - r * a.lp_chunks;
-          cp_async16(stage + (size_t)r * ly.sstride + 16 * c,
-                     a.lp_rows + (uint64_t)cid[c0 + r] * a.lp_stride + 16 * c);
+          const uint32_t off = TC ? cm_offset(r, c, a.lp_chunks) : r * ly.sstride + 16 * c;
+          cp_async16(stage + off, a.lp_rows + (uint64_t)cid[c0 + r] * a.lp_stride + 16 * c);
         }
+        if (TC)
+          for (uint32_t r = tid; r < nr; r += blockDim.x)
+            reinterpret_cast<float*>(smem + ly.nrm)[r] = __ldg(a.lp_norms + cid[c0 + r]);
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 0;" ::: "memory");
-        __syncthreads();
-        // ---- score; keep those below the cutoff of a full frontier (beamSearch.h:173-182)
-        for (uint32_t r = tid; r < nr; r += blockDim.x) {
-          const float dd = tile_row_dist<MT, PREC>(stage + (size_t)r * ly.sstride, qf, sc, a.d, a.lp_chunks);
-          if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[c0 + r]);
+        if (TC) {
+          fence_async_smem();
+          __syncthreads();
+          if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sbo = a.lp_chunks * 128u;
+            const uint32_t sa = smem_u32(stage), sq = smem_u32(smem + ly.qb);
+            for (uint32_t kb = 0; kb < a.lp_chunks / 2; kb++) {
+              const uint64_t ad = umma_desc(sa + kb * 256u, 128u, sbo), bd = umma_desc(sq + kb * 256u, 128u, sbo);
+              if (PREC == PREC_BF16) umma_bf16(tmem, ad, bd, umma_idesc(1, TC_ROWS, 16), kb > 0);
+              else umma_fp8(tmem, ad, bd, umma_idesc(0, TC_ROWS, 16), kb > 0);
+            }
+            umma_commit(bar);
+          }
+          const bool done = mbar_wait(bar, phase, TC_WAIT_LIMIT);
+          phase ^= 1u;
+          if (__syncthreads_or(!done)) {
+            tc_ok = false;  // the query is marked QS_INTERNAL; its MMA may still run: stop using the stage
+            break;
+          }
+          tc_fence_after();
+          float v[4];
+          tmem_ld4(tmem + ((uint32_t)(warp * 32) << 16), v);
+          const uint32_t r = tid;  // TMEM lane = staged row
+          if (r < nr) {
+            const float dot = PREC == PREC_BF16 ? v[0] + v[1] : (v[0] + v[1] * 0.0625f + v[2] * 0.00390625f) * tc_unscale;
+            const float dd = MT == MT_L2 ? reinterpret_cast<const float*>(smem + ly.nrm)[r] + tc_qn - 2.0f * dot : -dot;
+            if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[c0 + r]);
+          }
+          tc_fence_before();
+        } else {
+          __syncthreads();
+          // ---- score; keep those below the cutoff of a full frontier (beamSearch.h:173-182)
+          for (uint32_t r = tid; r < nr; r += blockDim.x) {
+            const float dd = tile_row_dist<MT, PREC>(stage + (size_t)r * ly.sstride, qf, sc, a.d, a.lp_chunks);
+            if (dd < cutoff) cand[atomicAdd(misc + 2, 1u)] = make_key(dd, cid[c0 + r]);
+          }
         }
-        __syncthreads();  // the next round overwrites the staged rows
+        __syncthreads();  // the next round overwrites the staged rows (and the accumulator)
       }
+      if (!tc_ok) break;
       cmps += ncand;
       const uint32_t nc = misc[2];
       if (nc > 0) {
@@ -335,26 +464,35 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
       uint32_t status = 0;
       if (fn < kq) status |= QS_SHORT;
       if (misc[9]) status |= QS_TRUNCATED;
+      if (!tc_ok) status |= QS_INTERNAL;
       if (a.out_visited) a.out_visited[qi] = (uint32_t)nvis;
       if (a.out_cmps) a.out_cmps[qi] = cmps;
       if (a.out_status) a.out_status[qi] = status;
     }
+    if (!tc_ok) break;  // this block takes no more queries (the others do)
+  }
+  if (TC) {
+    if (!tc_ok) mbar_wait(bar, phase ^ 1u, TC_WAIT_LIMIT);  // the round that did not finish in time
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 32);
   }
 }
 
 // Rows staged at once: the most that still gives the best occupancy among
-// CW, 3/4 CW and 1/2 CW (steps with more new candidates stage in rounds).
-template <int MT, int PREC>
+// CW, 3/4 CW and 1/2 CW (steps with more new candidates stage in rounds);
+// with tensor-core scoring, rounds of TC_ROWS rows.
+template <int MT, int PREC, bool TC>
 static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W, uint32_t S, uint32_t CW,
                          cudaStream_t st) {
-  auto k = search_tile_kernel<MT, PREC>;
+  auto k = search_tile_kernel<MT, PREC, TC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return cuda_fail(e, "tile kernel attribute");
-  uint32_t CWs = CW;
-  size_t smem = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, CW).total;
+  uint32_t CWs = TC ? TC_ROWS : CW;
+  size_t smem = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, CWs, TC).total;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem) != cudaSuccess || occ <= 0) occ = 1;
-  for (uint32_t f = 3; f >= 2; f--) {
+  for (uint32_t f = 3; f >= 2 && !TC; f--) {
     const uint32_t cws = std::max<uint32_t>(32, (CW * f / 4 + 15) & ~15u);
     const size_t sm2 = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, cws).total;
     int occ2 = 0;
@@ -364,6 +502,7 @@ static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W,
       smem = sm2;
     }
   }
+  if (TC) occ = std::min(occ, 16);  // 32 tensor-memory columns a block, 512 an SM
   const uint64_t want = a.nq;
   const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count));
   k<<<blocks, 128, smem, st>>>(a, W, S, CW, CWs);
@@ -374,30 +513,41 @@ static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W,
 
 // Sizes and launches the tile kernel; returns PANN_EINVAL (and does nothing)
 // when its state does not fit in shared memory, so the caller can take the
-// single-parent path.
+// single-parent path. scorer 1 scores on the tensor cores (rows of an even
+// number of 16-byte chunks; otherwise a clear error).
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
-                 int precision, uint32_t rerank, cudaStream_t st) {
+                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer) {
+  const bool tc = scorer == PANN_SCORER_TENSOR;
+  if (tc && (idx->lp_chunks % 2 != 0 || !idx->lp_norms.p))
+    return fail(PANN_EDEVICE, "tensor-core scoring needs low-precision rows of an even number of 16-byte chunks "
+                              "(bfloat16: d a multiple of 16; FP8: of 32)");
   const uint32_t nel = std::min(plan.dl, idx->R);
   uint32_t W = std::max<uint32_t>(1, std::min<uint32_t>(parents, 4));
   const uint32_t S = tile_seen_slots(plan.L, nel, idx->R);
-  TileLayout ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, W * nel);
+  TileLayout ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, tc ? TC_ROWS : W * nel, tc);
   while (ly.total > idx->smem_optin && W > 1) {
     W--;
-    ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, W * nel);
+    ly = tile_layout(idx->d, plan.L, W * nel, S, idx->lp_stride, tc ? TC_ROWS : W * nel, tc);
   }
   if (ly.total > idx->smem_optin) return fail(PANN_EINVAL, "tile search state does not fit in shared memory");
   a.lp_rows = idx->lp_rows.as<uint8_t>();
   a.lp_stride = idx->lp_stride;
   a.lp_chunks = idx->lp_chunks;
   a.lp_scales = idx->lp_scales.as<float>();
+  a.lp_norms = idx->lp_norms.as<float>();
   a.rerank = rerank;
   a.job_counter = job_counter;
   PANN_CUDA(cudaMemsetAsync(job_counter, 0, 4, st));
   const int mt = idx->metric;
-  if (mt == MT_L2 && precision == PREC_BF16) return launch_tile_t<MT_L2, PREC_BF16>(idx, a, W, S, W * nel, st);
-  if (mt == MT_IP && precision == PREC_BF16) return launch_tile_t<MT_IP, PREC_BF16>(idx, a, W, S, W * nel, st);
-  if (mt == MT_L2 && precision == PREC_FP8) return launch_tile_t<MT_L2, PREC_FP8>(idx, a, W, S, W * nel, st);
-  if (mt == MT_IP && precision == PREC_FP8) return launch_tile_t<MT_IP, PREC_FP8>(idx, a, W, S, W * nel, st);
+#define PANN_TILE_CASE(MTV, PRV)                                                          \
+  if (mt == MTV && precision == PRV)                                                    \
+    return tc ? launch_tile_t<MTV, PRV, true>(idx, a, W, S, W * nel, st)                \
+              : launch_tile_t<MTV, PRV, false>(idx, a, W, S, W * nel, st);
+  PANN_TILE_CASE(MT_L2, PREC_BF16)
+  PANN_TILE_CASE(MT_IP, PREC_BF16)
+  PANN_TILE_CASE(MT_L2, PREC_FP8)
+  PANN_TILE_CASE(MT_IP, PREC_FP8)
+#undef PANN_TILE_CASE
   return fail(PANN_EINVAL, "the tile search needs a bfloat16 or FP8 precision");
 }
 

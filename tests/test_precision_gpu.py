@@ -187,3 +187,43 @@ def test_score_pairs_exact_and_low_precision(mix_index, metric):
         # absolute error relative to the scale of the distances (|q||b| = 1 here)
         assert np.abs(lp - d64).max() < tol, (prec, np.abs(lp - d64).max())
     idx.set_precision(P.PREC_F32)
+
+
+@pytest.mark.parametrize("metric", [P.L2, P.MIPS], ids=["l2", "mips"])
+@pytest.mark.parametrize("prec", [P.PREC_BF16, P.PREC_FP8], ids=["bf16", "fp8"])
+@pytest.mark.parametrize("parents", [2, 3])
+def test_tile_search_tensor_core_scoring(mix_index, metric, prec, parents):
+    """Tile scoring on the tensor cores (tcgen05.mma, 128 staged rows against the query's split
+    terms): the same recall as scoring on the CUDA cores within 0.02, the bound of the CUDA-core
+    tile search against the exact search, exact float32 distances in the answer, deterministic, and
+    the batched form gives the same answers."""
+    base, q, out = mix_index
+    idx, gt = out[metric]
+    exact = idx.search(q, 10, 40)
+    idx.set_precision(prec)
+    tc = idx.search(q, 10, 40, precision=prec, parents=parents, scorer=P.SCORER_TENSOR)
+    tc2 = idx.search(q, 10, 40, precision=prec, parents=parents, scorer=P.SCORER_TENSOR)
+    cu = idx.search(q, 10, 40, precision=prec, parents=parents)
+    np.testing.assert_array_equal(tc.ids, tc2.ids)
+    assert (tc.flags & 16).sum() == 0
+    rec_tc, rec_cu = P.recall_at_k(tc.ids, gt, 10), P.recall_at_k(cu.ids, gt, 10)
+    rec_exact = P.recall_at_k(exact.ids, gt, 10)
+    assert abs(rec_tc - rec_cu) <= 0.02, (rec_tc, rec_cu)
+    assert rec_tc >= rec_exact - 2 * RECALL_LOSS[prec], (rec_tc, rec_exact)
+    np.testing.assert_array_equal(tc.dists.view(np.uint32), idx.score(q, tc.ids).view(np.uint32))
+    b = idx.batch(len(q), 10, 40, precision=prec, parents=parents, scorer=P.SCORER_TENSOR)
+    br = b.run(q, 10, 40)
+    np.testing.assert_array_equal(br.ids[:, :10], tc.ids)
+    b.close()
+    idx.set_precision(P.PREC_F32)
+
+
+def test_tensor_core_scoring_needs_whole_mma_steps(lib_built):
+    base = P.synth_mixture(P.F32, 2000, 40, 8, 1, 0, sigma=0.3, normalize=True)   # 80-byte bf16 rows
+    idx = P.Index(base, 16)
+    idx.build(32, 1.2)
+    idx.set_precision(P.PREC_BF16)
+    with pytest.raises(P.PannError) as e:
+        idx.search(base[:8], 5, 20, precision=P.PREC_BF16, parents=2, scorer=P.SCORER_TENSOR)
+    assert "tensor-core" in str(e.value)
+    idx.close()
