@@ -711,7 +711,7 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         t_g = time.perf_counter() - t0
         actual = np.diff(gt_offs).astype(np.float64)
         nz = actual > 0
-        gt = {"queries": nr, "seconds": round(t_g, 4), "qps_e2e": round(nr / t_g, 1),
+        rgt = {"queries": nr, "seconds": round(t_g, 4), "qps_e2e": round(nr / t_g, 1),
               "recall_point": round(float(np.mean(sizes[nz] / actual[nz])), 4) if nz.any() else None,
               "recall_cumulative": round(float(sizes.sum() / actual.sum()), 4) if actual.sum() else None}
         try:
@@ -722,11 +722,11 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
                 t0 = time.perf_counter()
                 ro, ri = O.range_groundtruth("ref", base, q[:nc], radius)
                 t_c = time.perf_counter() - t0
-                gt["cpu_reference"] = {"queries": nc, "qps": round(nc / t_c, 2), "tool": "compute_range_groundtruth",
+                rgt["cpu_reference"] = {"queries": nc, "qps": round(nc / t_c, 2), "tool": "compute_range_groundtruth",
                                        "answers_identical": bool(np.array_equal(ri, gt_ids[: int(gt_offs[nc])]))}
         except Exception as ex:  # noqa: BLE001
-            gt["cpu_reference"] = {"failed": str(ex)}
-        out["range"]["groundtruth"] = gt
+            rgt["cpu_reference"] = {"failed": str(ex)}
+        out["range"]["groundtruth"] = rgt
     if "serving" in want:
         out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
     if "sweep" in want:
