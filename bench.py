@@ -558,7 +558,7 @@ def search_and_parse(idx, base, q, gt, dev, flush, stream):
     return {"runs": res, "buckets": table}
 
 
-def run_c2(dev, flush, args):
+def run_c2(dev, flush, args, want):
     """The precision form at 10M: 10,000,000 base + 10,000 query vectors, 96-d float32, the same
     generator with 1,024 components, Vamana R=64 L=128 alpha=1.2 two passes built on the GPU with
     the Euclidean distance; searched as a Euclidean index and as a mips index (on L2-normalised
@@ -608,6 +608,8 @@ def run_c2(dev, flush, args):
         best = max(out[mname]["precision"].values(), key=lambda v: v["qps_batched_graph"], default=None)
         if best:
             out[mname]["best_speedup_vs_plain"] = best["speedup_vs_plain"]
+        if metric == P.L2 and "serving" in want:
+            out["serving"] = run_serving(ix, q, nq, beam, range_radius(base, q), out[mname]["precision"])
         if ix is not idx:
             ix.close()
     idx.close()
@@ -727,12 +729,12 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         except Exception as ex:  # noqa: BLE001
             rgt["cpu_reference"] = {"failed": str(ex)}
         out["range"]["groundtruth"] = rgt
-    if "serving" in want:
+    if "serving" in want and "c2" not in want:
         out["serving"] = run_serving(idx, q, nq, beam, radius, prec_out)
     if "sweep" in want:
         out["search_and_parse"] = search_and_parse(idx, base, q, gt, dev, flush, stream)
     if "c2" in want:
-        out["precision_10m"] = run_c2(dev, flush, args)
+        out["precision_10m"] = run_c2(dev, flush, args, want)
     return out
 
 
@@ -800,7 +802,10 @@ def run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib):
 
 def run_serving(idx, q, nq, beam, radius, prec_out):
     """Open-loop Poisson arrivals at 5 offered rates, for the plain form and
-    for the fastest precision form found above."""
+    for the fastest precision form found above. Each of the 3 slots holds the
+    scratch of 4096 queries at k = 100, beam 200 and admits up to 8192 queries a
+    batch while their scratch fits (requests at k = 10 and the short beam
+    need less per query, so they pack more)."""
     import parlayann_b200 as P
 
     rng = np.random.default_rng(7)
@@ -815,8 +820,12 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
     for fname, prec, parents, kbeam, scorer in forms:
         if prec != P.PREC_F32:
             idx.set_precision(prec)
-        srv = P.Server(idx, max_batch_queries=4096, inflight=3, max_k=100, max_beam=max(200, kbeam), precision=prec,
-                       parents=parents, scorer=scorer)
+        probe = P.Server(idx, max_batch_queries=4096, inflight=1, max_k=100, max_beam=max(200, kbeam),
+                         precision=prec, parents=parents, scorer=scorer)
+        budget = probe.admission()["scratch_bytes"]
+        probe.close()
+        srv = P.Server(idx, max_batch_queries=8192, inflight=3, max_k=100, max_beam=max(200, kbeam), precision=prec,
+                       parents=parents, scorer=scorer, scratch_bytes=budget)
 
         def schedule(n, rate_qps, range_frac):
             nqs = rng.integers(1, 257, n)
@@ -829,8 +838,11 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
             return np.cumsum(gaps), kinds, nqs, kk, bb, rows
 
         a, kd, nqs, kk, bb, rows = schedule(400, 0, 0.0)  # capacity: everything at t = 0
+        srv.admission(reset=True)
         lat, wall = srv.replay(a, kd, nqs, kk, bb, rows, q, rp)
         cap_qps = float(nqs.sum()) / wall
+        adm = srv.admission(reset=True)
+        cap_batch = adm["queries"] / max(adm["batches"], 1)
         rates = []
         for frac in (0.2, 0.4, 0.6, 0.8, 0.95):
             rate = frac * cap_qps
@@ -838,7 +850,10 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
             a, kd, nqs, kk, bb, rows = schedule(n, rate, 0.01)
             lat, wall = srv.replay(a, kd, nqs, kk, bb, rows, q, rp)
             kn, rg = lat[kd == 0], lat[kd == 1]
+            adm = srv.admission(reset=True)
             rates.append({"offered_qps": round(rate, 1), "achieved_qps": round(float(nqs.sum()) / wall, 1),
+                          "batches": adm["batches"],
+                          "queries_per_batch": round(adm["queries"] / max(adm["batches"], 1), 1),
                           "requests": n, "range_requests": int(kd.sum()),
                           "p50_ms": round(1e3 * float(np.percentile(lat, 50)), 3),
                           "p99_ms": round(1e3 * float(np.percentile(lat, 99)), 3),
@@ -847,12 +862,15 @@ def run_serving(idx, q, nq, beam, radius, prec_out):
                           "range_p50_ms": round(1e3 * float(np.percentile(rg, 50)), 3) if len(rg) else None,
                           "range_p99_ms": round(1e3 * float(np.percentile(rg, 99)), 3) if len(rg) else None})
         srv.close()
-        serving[fname] = {"precision": int(prec), "parents": parents, "beam_k10": kbeam,
-                          "capacity_qps_closed": round(cap_qps, 1), "rates": rates}
+        serving[fname] = {"precision": int(prec), "parents": parents, "scorer": scorer, "beam_k10": kbeam,
+                          "scratch_bytes_per_slot": budget, "capacity_qps_closed": round(cap_qps, 1),
+                          "capacity_queries_per_batch": round(cap_batch, 1), "rates": rates}
     idx.set_precision(P.PREC_F32)
     return {"requests": "1-256 queries, k in {10,100} (beam for recall@10 >= 0.95 / 200), 1% range "
                         "requests (1 query, beam 20, greedy, radius at the 1% distance quantile)",
-            "slots": 3, "batch_queries": 4096, "forms": serving}
+            "slots": 3, "admission": "by scratch bytes: each slot's arena holds 4096 queries at k=100, beam 200; "
+                                     "a batch takes up to 8192 queries while its scratch fits",
+            "forms": serving}
 
 
 def cpu_baseline(base, q, graph, beam, res, args):

@@ -361,14 +361,18 @@ int pann_batch_destroy(pann_batch* b);
 /* A request loop over one resident index (no counterpart in the reference,
  * which searches closed batches: qsearchAll, beamSearch.h:599-646). Requests
  * are submitted from any thread and answered asynchronously: a dispatcher
- * thread keeps up to `inflight` batches on the GPU, each a pann_batch whose
- * device scratch holds max_batch_queries queries (the admission unit), and
- * fills every slot that frees up with the waiting k-NN requests in arrival
- * order (continuous batching: requests that arrive while others run join the
- * next slot, and batches overlap on the device). Range requests run on a
- * second worker through pann_range_search. Each request's answer equals the
- * same request run alone (pann_search / pann_range_search). While a server
- * runs it is the only user of its index. */
+ * thread keeps up to `inflight` batches on the GPU, each in a slot with a
+ * device scratch arena of scratch_bytes, and fills every slot that frees up
+ * with the waiting k-NN requests in arrival order while the batch they form
+ * fits the arena (admission by scratch memory: a batch needs its queries and
+ * outputs, per-query work lists and hand-off records sized by its largest
+ * beam, and per-warp seen tables, so requests with small k and beam pack
+ * more queries into a slot) and holds at most max_batch_queries queries
+ * (continuous batching: requests that arrive while others run join the next
+ * slot, and batches overlap on the device). Range requests run on a second
+ * worker through pann_range_search. Each request's answer equals the same
+ * request run alone (pann_search / pann_range_search). While a server runs it
+ * is the only user of its index. */
 typedef struct pann_server pann_server;
 
 typedef struct {
@@ -381,6 +385,8 @@ typedef struct {
   int32_t precision;          /* PANN_PREC_*; low precision needs pann_index_set_precision first */
   uint32_t parents;           /* pann_search_options::parents of every k-NN request */
   uint32_t scorer;            /* pann_search_options::scorer of every k-NN request */
+  uint64_t scratch_bytes;     /* device scratch of each slot; 0: what max_batch_queries queries at max_k and
+                                 max_beam need. A request that alone needs more is refused at submission. */
 } pann_server_options;
 
 int pann_server_create(pann_server** out, pann_index* idx, const pann_server_options* opt, const uint32_t* starts,
@@ -409,6 +415,10 @@ int pann_server_replay(pann_server* s, uint32_t nreq, const double* arrival_s, c
                        const uint32_t* nq, const uint32_t* k, const uint32_t* beam, const uint64_t* q_row,
                        const void* query_pool, const pann_range_params* rp, uint32_t range_start, double* out_latency_s,
                        double* out_wall_s);
+/* Admission since the last reset: batches launched, queries they held, the
+ * largest scratch a batch used and each slot's scratch bytes. */
+int pann_server_admission(pann_server* s, int reset, uint64_t* batches, uint64_t* queries, uint64_t* scratch_peak,
+                          uint64_t* scratch_bytes);
 int pann_server_destroy(pann_server* s);
 
 /* ---------------------------------------------------------------- build */

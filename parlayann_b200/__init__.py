@@ -80,7 +80,7 @@ class ServerOptions(ctypes.Structure):
     _fields_ = [("max_batch_queries", ctypes.c_uint32), ("inflight", ctypes.c_uint32), ("max_k", ctypes.c_uint32),
                 ("max_beam", ctypes.c_uint32), ("limit", ctypes.c_uint64), ("degree_limit", ctypes.c_uint32),
                 ("batch_factor", ctypes.c_double), ("precision", ctypes.c_int32), ("parents", ctypes.c_uint32),
-                ("scorer", ctypes.c_uint32)]
+                ("scorer", ctypes.c_uint32), ("scratch_bytes", ctypes.c_uint64)]
 
 
 class BuildParams(ctypes.Structure):
@@ -148,6 +148,8 @@ SIGNATURES = {
     "pann_server_wait_range": (_I, [_P, _U64, _P, _P, _U64, ctypes.POINTER(ctypes.c_double)]),
     "pann_server_stats": (_I, [_P, _I, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "pann_server_admission": (_I, [_P, _I, ctypes.POINTER(_U64), ctypes.POINTER(_U64), ctypes.POINTER(_U64),
+                                   ctypes.POINTER(_U64)]),
     "pann_server_replay": (_I, [_P, _U32, _P, _P, _P, _P, _P, _P, _P, ctypes.POINTER(RangeParams), _U32, _P,
                                 ctypes.POINTER(ctypes.c_double)]),
     "pann_server_destroy": (_I, [_P]),
@@ -498,11 +500,11 @@ class Server:
     def __init__(self, index: "Index", max_batch_queries: int = 1024, inflight: int = 3, max_k: int = 100,
                  max_beam: int = 400, limit: int | None = None, degree_limit: int | None = None,
                  batch_factor: float = 0.125, precision: int = PREC_F32, starts=(0,), parents: int = 0,
-                 scorer: int = 0):
+                 scorer: int = 0, scratch_bytes: int = 0):
         self.index = index
         o = ServerOptions(max_batch_queries, inflight, max_k, max_beam, index.n if limit is None else limit,
                           index.R if degree_limit is None else degree_limit, batch_factor, precision, parents,
-                          scorer)
+                          scorer, scratch_bytes)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
         h = ctypes.c_void_p()
         _check(lib().pann_server_create(ctypes.byref(h), index.handle, ctypes.byref(o), _ptr(st), len(st)))
@@ -549,6 +551,13 @@ class Server:
         _check(lib().pann_server_stats(self._h, int(reset), ctypes.byref(r), ctypes.byref(q), ctypes.byref(sec),
                                        ctypes.byref(p50), ctypes.byref(p99)))
         return dict(requests=r.value, queries=q.value, seconds=sec.value, p50_s=p50.value, p99_s=p99.value)
+
+    def admission(self, reset: bool = False) -> dict:
+        """Batches launched, queries they held, the largest scratch a batch used and each slot's scratch."""
+        b, q, peak, cap = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        _check(lib().pann_server_admission(self._h, int(reset), ctypes.byref(b), ctypes.byref(q), ctypes.byref(peak),
+                                           ctypes.byref(cap)))
+        return dict(batches=b.value, queries=q.value, scratch_peak=peak.value, scratch_bytes=cap.value)
 
     def replay(self, arrival_s, kind, nq, k, beam, q_row, query_pool, range_params: RangeParams | None = None,
                range_start: int = 0):

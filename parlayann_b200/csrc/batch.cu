@@ -137,6 +137,127 @@ static int autotune(pann_batch* b, cudaStream_t st) {
   return PANN_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batches laid out in an arena (index.cuh: batch_scratch_bytes, run_in_arena).
+
+namespace {
+
+struct ArenaLayout {
+  SearchPlan plan;
+  TierSizes z;
+  size_t cnt, starts, q, qk, qL, order, ids, dists, vis, cmps, status, redo, spill, handoff, gt2, ge2, bytes;
+};
+
+size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int arena_layout(const pann_index* idx, const pann_query_params* bounds, uint32_t n_start, uint32_t nq, int prec,
+                 ArenaLayout* y) {
+  int rc = make_plan(idx, bounds, n_start, &y->plan);
+  if (rc) return rc;
+  // any query may defer candidates (its own beam is at most the bound)
+  y->plan.Ccap = (uint32_t)std::floor(y->plan.bf * (double)y->plan.L) + std::min(y->plan.dl, idx->R) + 1;
+  rc = size_tiers(idx, y->plan, nq, prec, 0, 0, &y->z);
+  if (rc) return rc;
+  const size_t k = y->plan.k;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o += a256(std::max<size_t>(bytes, 16));
+    return at;
+  };
+  y->cnt = take(4 * 64);
+  y->starts = take(4ull * std::max<uint32_t>(n_start, 1));
+  y->q = take(idx->stride * (size_t)nq);
+  y->qk = take(4ull * nq);
+  y->qL = take(4ull * nq);
+  y->order = take(4ull * nq);
+  y->ids = take(4ull * nq * k);
+  y->dists = take(4ull * nq * k);
+  y->vis = take(4ull * nq);
+  y->cmps = take(4ull * nq);
+  y->status = take(4ull * nq);
+  y->redo = take(4ull * 6 * nq);
+  y->spill = take(y->z.spill_bytes);
+  y->handoff = prec == PREC_F32 ? take(y->z.handoff_bytes) : o;
+  y->gt2 = take(y->z.t2_bytes);
+  y->ge2 = prec == PREC_F32 ? take(y->z.e2_bytes) : o;
+  y->bytes = o;
+  return PANN_OK;
+}
+
+}  // namespace
+
+int batch_scratch_bytes(const pann_index* idx, const pann_query_params* bounds, uint32_t n_start, uint32_t nq,
+                        int precision, uint32_t parents, size_t* bytes) {
+  (void)parents;  // the tile search needs no scratch beyond the single-parent tiers' own
+  ArenaLayout y;
+  int rc = arena_layout(idx, bounds, n_start, std::max<uint32_t>(nq, 1), precision, &y);
+  if (rc) return rc;
+  *bytes = y.bytes;
+  return PANN_OK;
+}
+
+int run_in_arena(pann_index* idx, uint8_t* arena, size_t arena_bytes, const pann_query_params* bounds,
+                 const uint32_t* h_starts, uint32_t n_start, const uint8_t* h_queries, uint32_t nq, const uint32_t* h_k,
+                 const uint32_t* h_beam, const uint32_t* h_order, int precision, uint32_t rerank, uint32_t parents,
+                 uint32_t scorer, uint32_t* h_ids, float* h_dists, cudaStream_t st) {
+  if (nq == 0) return PANN_OK;
+  ArenaLayout y;
+  int rc = arena_layout(idx, bounds, n_start, nq, precision, &y);
+  if (rc) return rc;
+  if (y.bytes > arena_bytes)
+    return fail(PANN_EINVAL, "batch needs " + std::to_string(y.bytes) + " bytes of scratch; the arena holds " +
+                                 std::to_string(arena_bytes));
+  auto at = [&](size_t off) { return arena + off; };
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(at(y.cnt));
+  const size_t rb = (size_t)idx->d * idx->esize;
+  // the job count comes from the pinned order array's tail word, so every copy is from pinned memory
+  PANN_CUDA(cudaMemsetAsync(cnt, 0, 4 * 64, st));
+  PANN_CUDA(cudaMemcpyAsync(at(y.starts), h_starts, 4ull * n_start, cudaMemcpyHostToDevice, st));
+  if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(at(y.q), 0, idx->stride * (size_t)nq, st));
+  PANN_CUDA(cudaMemcpy2DAsync(at(y.q), idx->stride, h_queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(at(y.qk), h_k, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(at(y.qL), h_beam, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(at(y.order), h_order, 4ull * nq, cudaMemcpyHostToDevice, st));
+  PANN_CUDA(cudaMemcpyAsync(cnt + 32, h_order + nq, 4, cudaMemcpyHostToDevice, st));
+  SearchArgs a = base_args(idx, y.plan, at(y.q), nullptr, nq, reinterpret_cast<const uint32_t*>(at(y.starts)),
+                           reinterpret_cast<uint32_t*>(at(y.ids)), reinterpret_cast<float*>(at(y.dists)),
+                           reinterpret_cast<uint32_t*>(at(y.vis)), reinterpret_cast<uint32_t*>(at(y.cmps)),
+                           reinterpret_cast<uint32_t*>(at(y.status)), nullptr, 0);
+  a.qk = reinterpret_cast<const uint32_t*>(at(y.qk));
+  a.qL = reinterpret_cast<const uint32_t*>(at(y.qL));
+  a.kstride = y.plan.k;
+  rc = PANN_EINVAL;
+  if (parents > 0 && precision != PREC_F32) {
+    a.job_list = reinterpret_cast<const uint32_t*>(at(y.order));
+    a.njobs_dev = cnt + 32;
+    rc = enqueue_tile(idx, y.plan, a, parents, cnt + 10, precision, rerank, st, scorer);
+    if (rc != PANN_OK && rc != PANN_EINVAL) return rc;
+  }
+  if (rc == PANN_EINVAL) {
+    TierBufs t{};
+    t.cnt = cnt;
+    t.redo0 = reinterpret_cast<uint32_t*>(at(y.redo));
+    t.redo1 = t.redo0 + nq;
+    t.emu = t.redo1 + nq;
+    t.ovf = t.emu + nq;
+    t.emu_rec = t.ovf + nq;
+    t.ovf_rec = t.emu_rec + nq;
+    t.gspill = reinterpret_cast<uint32_t*>(at(y.spill));
+    t.handoff = precision == PREC_F32 ? reinterpret_cast<uint32_t*>(at(y.handoff)) : nullptr;
+    t.gt2 = reinterpret_cast<uint32_t*>(at(y.gt2));
+    t.ge2 = precision == PREC_F32 ? reinterpret_cast<uint32_t*>(at(y.ge2)) : nullptr;
+    t.job_list0 = reinterpret_cast<const uint32_t*>(at(y.order));
+    t.njobs0 = cnt + 32;
+    rc = enqueue_tiers(idx, y.plan, a, y.z, t, st, precision, rerank);
+    if (rc) return rc;
+  }
+  const size_t kb = 4ull * y.plan.k * nq;
+  PANN_CUDA(cudaMemcpyAsync(h_ids, at(y.ids), kb, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(h_dists, at(y.dists), kb, cudaMemcpyDeviceToHost, st));
+  return PANN_OK;
+}
+
 }  // namespace pann
 
 using namespace pann;

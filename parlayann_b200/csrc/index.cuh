@@ -103,4 +103,18 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
                int precision = 0, uint32_t rerank = 0, uint32_t parents = 0, uint32_t scorer = 0);
 
+// A batch laid out in a caller's device arena (the serving form's admission
+// by scratch memory): every buffer of one run of nq queries, whose k and beam
+// are at most bounds->k and bounds->beam, carved from one allocation.
+// batch_scratch_bytes gives the bytes such a run needs; run_in_arena stages
+// the inputs (pinned host arrays: nq query rows of d * element bytes, per-query
+// k and beam, the job order), enqueues the search on `st` and the copies of
+// its ids and distances (nq rows of bounds->k) to pinned host memory.
+int batch_scratch_bytes(const pann_index* idx, const pann_query_params* bounds, uint32_t n_start, uint32_t nq,
+                        int precision, uint32_t parents, size_t* bytes);
+int run_in_arena(pann_index* idx, uint8_t* arena, size_t arena_bytes, const pann_query_params* bounds,
+                 const uint32_t* h_starts, uint32_t n_start, const uint8_t* h_queries, uint32_t nq, const uint32_t* h_k,
+                 const uint32_t* h_beam, const uint32_t* h_order, int precision, uint32_t rerank, uint32_t parents,
+                 uint32_t scorer, uint32_t* h_ids, float* h_dists, cudaStream_t st);
+
 }  // namespace pann

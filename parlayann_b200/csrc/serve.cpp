@@ -1,27 +1,32 @@
 // Serving form (include/parlayann_b200.h, pann_server_*): a request loop over
-// one resident index with continuous batching.
+// one resident index with continuous batching and admission by scratch memory.
 //
 // The reference answers queries in closed batches (qsearchAll,
 // beamSearch.h:599-646; RangeSearch, rangeSearch.h:183-276); it has no request
 // loop. Here requests arrive one by one from any thread. A dispatcher thread
-// owns `inflight` batch slots, each a pann_batch (its device scratch sized for
-// max_batch_queries queries, which is the admission unit) with its own stream,
-// device and pinned host buffers. Whenever a slot is free it takes the waiting
-// k-NN requests in arrival order while their queries fit, launches the batch
-// (CUDA-graph replay of the tiered search) and moves on: requests that arrive
-// while other batches are on the GPU go into the next free slot, so batches
-// overlap on the device. Finished slots are retired by polling their events;
-// each request's latency runs from its submission to the moment its results
-// are in host memory. Range requests run on a second worker through
-// pann_range_search, concurrently with the k-NN batches. Results of a request
-// are the same as that request run alone (same kernels, per-query
-// parameters).
+// owns `inflight` slots, each a device arena of scratch_bytes with its own
+// stream and pinned host buffers. Whenever a slot is free it takes the waiting
+// k-NN requests in arrival order while the batch they form still fits the
+// arena: the bytes a batch needs (its queries, outputs, per-query work lists,
+// the per-warp seen tables and hand-off logs of the first tier, the hand-off
+// records of the queries that may need them, the later tiers' tables) follow
+// from its query count and its largest k and beam (batch_scratch_bytes), so
+// small-k, short-beam requests pack many more queries into a slot than
+// k = 100, beam = 200 ones. The batch is laid out in the arena and run
+// (run_in_arena); requests that arrive while other batches are on the GPU go
+// into the next free slot, so batches overlap on the device. Finished slots
+// are retired by polling their events; each request's latency runs from its
+// submission to the moment its results are in host memory. Range requests run
+// on a second worker through pann_range_search, concurrently with the k-NN
+// batches. Results of a request are the same as that request run alone (same
+// kernels, per-query parameters).
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -54,18 +59,17 @@ struct Request {
 };
 
 struct Slot {
-  pann_batch* b = nullptr;
+  uint8_t* arena = nullptr;  // device scratch of one batch
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
-  uint8_t* d_q = nullptr;
-  uint32_t* d_ids = nullptr;
-  float* d_d = nullptr;
-  uint8_t* h_q = nullptr;  // pinned
+  uint8_t* h_q = nullptr;  // pinned: queries, per-query k / beam / job order, results
+  uint32_t* h_k = nullptr;
+  uint32_t* h_L = nullptr;
+  uint32_t* h_order = nullptr;  // nq job indices, then nq
   uint32_t* h_ids = nullptr;
   float* h_d = nullptr;
-  std::vector<uint32_t> hk, hL;
   std::vector<Request*> reqs;
-  uint32_t nq = 0;
+  uint32_t nq = 0, kmax = 0;
   bool busy = false;
 };
 
@@ -90,6 +94,10 @@ struct pann_server {
   uint64_t done_queries = 0;
   clk::time_point stats_t0;
   std::string fatal;
+  // admission
+  size_t scratch = 0;  // bytes of each slot's arena
+  uint64_t batches = 0, batched_queries = 0;
+  size_t scratch_peak = 0;
 };
 
 namespace {
@@ -106,7 +114,7 @@ void finish(pann_server* s, Request* r, int rc, const std::string& err) {
 // Copies a finished slot's results into its requests (called with s->mu held).
 void retire(pann_server* s, Slot& sl) {
   uint32_t off = 0;
-  const uint32_t K = s->opt.max_k;
+  const uint32_t K = sl.kmax;  // the batch's output rows hold its largest k
   for (Request* r : sl.reqs) {
     r->ids.resize((size_t)r->nq * r->k);
     r->dists.resize((size_t)r->nq * r->k);
@@ -121,39 +129,73 @@ void retire(pann_server* s, Slot& sl) {
   sl.busy = false;
 }
 
+// Bytes a batch of nq queries with largest k and beam needs in an arena.
+size_t batch_bytes(const pann_server* s, uint32_t nq, uint32_t kmax, uint32_t Lmax) {
+  pann_query_params b{kmax, Lmax, s->opt.limit, s->opt.degree_limit, s->opt.batch_factor};
+  size_t bytes = 0;
+  if (pann::batch_scratch_bytes(s->idx, &b, (uint32_t)s->starts.size(), nq, s->opt.precision, s->opt.parents,
+                                &bytes) != PANN_OK)
+    return SIZE_MAX;
+  return bytes;
+}
+
 // Launches the waiting k-NN requests that fit into a free slot (s->mu held on
-// entry; released during the launch). Returns true if something was launched.
+// entry; released during the launch). Requests are taken in arrival order
+// while the batch stays within max_batch_queries and its scratch within the
+// slot's arena. Returns true if something was launched.
 bool launch(pann_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
   if (s->knn_q.empty()) return false;
-  uint32_t nq = 0;
-  while (!s->knn_q.empty() && nq + s->knn_q.front()->nq <= s->opt.max_batch_queries) {
-    Request* r = s->knn_q.front();
+  uint32_t nq = 0, kmax = 0, Lmax = 0;
+  size_t used = 0;
+  while (!s->knn_q.empty()) {
+    const Request* r = s->knn_q.front();
+    const uint32_t n2 = nq + r->nq, k2 = std::max(kmax, r->k), L2 = std::max(Lmax, r->beam);
+    if (n2 > s->opt.max_batch_queries) break;
+    const size_t need = batch_bytes(s, n2, k2, L2);
+    if (need > s->scratch) break;
     s->knn_q.pop_front();
-    sl.reqs.push_back(r);
-    nq += r->nq;
+    sl.reqs.push_back(const_cast<Request*>(r));
+    nq = n2;
+    kmax = k2;
+    Lmax = L2;
+    used = need;
   }
   if (sl.reqs.empty()) return false;
   sl.busy = true;
   sl.nq = nq;
+  sl.kmax = kmax;
+  s->batches++;
+  s->batched_queries += nq;
+  s->scratch_peak = std::max(s->scratch_peak, used);
   lk.unlock();
   uint32_t at = 0;
   for (Request* r : sl.reqs) {
     std::memcpy(sl.h_q + (size_t)at * s->row_bytes, r->queries.data(), (size_t)r->nq * s->row_bytes);
     for (uint32_t i = 0; i < r->nq; i++) {
-      sl.hk[at + i] = r->k;
-      sl.hL[at + i] = r->beam;
+      sl.h_k[at + i] = r->k;
+      sl.h_L[at + i] = r->beam;
     }
     at += r->nq;
   }
-  int rc = PANN_OK;
-  cudaError_t e = cudaMemcpyAsync(sl.d_q, sl.h_q, (size_t)nq * s->row_bytes, cudaMemcpyHostToDevice, sl.st);
-  if (e == cudaSuccess)
-    rc = pann_batch_run(sl.b, sl.d_q, nq, sl.hk.data(), sl.hL.data(), sl.d_ids, sl.d_d, nullptr, nullptr, nullptr, 1,
-                        sl.st);
-  const size_t ob = 4ull * nq * s->opt.max_k;
-  if (e == cudaSuccess && rc == PANN_OK) e = cudaMemcpyAsync(sl.h_ids, sl.d_ids, ob, cudaMemcpyDeviceToHost, sl.st);
-  if (e == cudaSuccess && rc == PANN_OK) e = cudaMemcpyAsync(sl.h_d, sl.d_d, ob, cudaMemcpyDeviceToHost, sl.st);
-  if (e == cudaSuccess && rc == PANN_OK) e = cudaEventRecord(sl.done, sl.st);
+  // longest beam first (counting sort), then the job count
+  {
+    std::vector<uint32_t> count(Lmax + 2, 0);
+    for (uint32_t i = 0; i < nq; i++) count[Lmax - sl.h_L[i]]++;
+    uint32_t acc = 0;
+    for (auto& c : count) {
+      const uint32_t t = c;
+      c = acc;
+      acc += t;
+    }
+    for (uint32_t i = 0; i < nq; i++) sl.h_order[count[Lmax - sl.h_L[i]]++] = i;
+    sl.h_order[nq] = nq;
+  }
+  pann_query_params bounds{kmax, Lmax, s->opt.limit, s->opt.degree_limit, s->opt.batch_factor};
+  int rc = pann::run_in_arena(s->idx, sl.arena, s->scratch, &bounds, s->starts.data(), (uint32_t)s->starts.size(),
+                              sl.h_q, nq, sl.h_k, sl.h_L, sl.h_order, s->opt.precision, 0, s->opt.parents,
+                              s->opt.scorer, sl.h_ids, sl.h_d, sl.st);
+  cudaError_t e = cudaSuccess;
+  if (rc == PANN_OK) e = cudaEventRecord(sl.done, sl.st);
   lk.lock();
   if (e != cudaSuccess || rc != PANN_OK) {
     std::string msg = e != cudaSuccess ? std::string("CUDA error: ") + cudaGetErrorString(e) : pann_last_error();
@@ -304,30 +346,37 @@ int pann_server_create(pann_server** out, pann_index* idx, const pann_server_opt
   s->opt = *opt;
   s->starts.assign(starts, starts + n_start);
   cudaGetDevice(&s->device);
-  pann_query_params bounds{opt->max_k, opt->max_beam, opt->limit, opt->degree_limit, opt->batch_factor};
-  pann_search_options so{opt->precision, 0, opt->parents, opt->scorer};
-  pann_batch_options bo{1, 0, 0, 0};
+  if (opt->precision != PANN_PREC_F32 && idx->lp_prec != opt->precision) {
+    delete s;
+    return pann::fail(PANN_EINVAL, "call pann_index_set_precision for this precision first");
+  }
   s->row_bytes = (size_t)idx->d * idx->esize;
+  // the arena: the option, or what a full batch at the bounds needs
+  s->scratch = opt->scratch_bytes ? (size_t)opt->scratch_bytes
+                                  : batch_bytes(s, opt->max_batch_queries, opt->max_k, opt->max_beam);
+  if (s->scratch == SIZE_MAX || batch_bytes(s, 1, opt->max_k, opt->max_beam) > s->scratch) {
+    const size_t one = batch_bytes(s, 1, opt->max_k, opt->max_beam);
+    delete s;
+    return pann::fail(PANN_EINVAL, "scratch_bytes is below the " + std::to_string(one) +
+                                       " bytes one query at max_k and max_beam needs");
+  }
   s->slots.resize(opt->inflight);
   auto bail = [&](int rc) {
     pann_server_destroy(s);
     return rc;
   };
   for (Slot& sl : s->slots) {
-    int rc = pann_batch_create(&sl.b, idx, opt->max_batch_queries, &bounds, starts, n_start, &so, &bo);
-    if (rc) return bail(rc);
     const size_t m = opt->max_batch_queries;
     cudaError_t e = cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaMalloc(&sl.d_q, m * s->row_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&sl.d_ids, 4 * m * opt->max_k);
-    if (e == cudaSuccess) e = cudaMalloc(&sl.d_d, 4 * m * opt->max_k);
+    if (e == cudaSuccess) e = cudaMalloc(&sl.arena, s->scratch);
     if (e == cudaSuccess) e = cudaMallocHost(&sl.h_q, m * s->row_bytes);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_k, 4 * m);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_L, 4 * m);
+    if (e == cudaSuccess) e = cudaMallocHost(&sl.h_order, 4 * (m + 1));
     if (e == cudaSuccess) e = cudaMallocHost(&sl.h_ids, 4 * m * opt->max_k);
     if (e == cudaSuccess) e = cudaMallocHost(&sl.h_d, 4 * m * opt->max_k);
     if (e != cudaSuccess) return bail(pann::cuda_fail(e, "server slot"));
-    sl.hk.resize(m);
-    sl.hL.resize(m);
   }
   s->stats_t0 = clk::now();
   s->dispatcher = std::thread(dispatcher_main, s);
@@ -343,6 +392,10 @@ int pann_server_submit_knn(pann_server* s, const void* queries, uint32_t nq, uin
     return pann::fail(PANN_EINVAL, "a request needs 1 to max_batch_queries queries");
   if (k == 0 || k > s->opt.max_k || beam < k || beam > s->opt.max_beam || beam < s->starts.size())
     return pann::fail(PANN_EINVAL, "k / beam outside the server's bounds (1 <= k <= beam <= max_beam, k <= max_k)");
+  const size_t need = batch_bytes(s, nq, k, beam);
+  if (need > s->scratch)
+    return pann::fail(PANN_EINVAL, "the request needs " + std::to_string(need) + " bytes of scratch; a slot holds " +
+                                       std::to_string(s->scratch) + " (split it)");
   Request* r = new Request();
   r->kind = 0;
   r->nq = nq;
@@ -429,6 +482,22 @@ int pann_server_stats(pann_server* s, int reset, uint64_t* requests, uint64_t* q
   return PANN_OK;
 }
 
+int pann_server_admission(pann_server* s, int reset, uint64_t* batches, uint64_t* queries, uint64_t* scratch_peak,
+                          uint64_t* scratch_bytes) {
+  if (!s) return pann::fail(PANN_EINVAL, "server is NULL");
+  std::lock_guard<std::mutex> g(s->mu);
+  if (batches) *batches = s->batches;
+  if (queries) *queries = s->batched_queries;
+  if (scratch_peak) *scratch_peak = s->scratch_peak;
+  if (scratch_bytes) *scratch_bytes = s->scratch;
+  if (reset) {
+    s->batches = 0;
+    s->batched_queries = 0;
+    s->scratch_peak = 0;
+  }
+  return PANN_OK;
+}
+
 int pann_server_destroy(pann_server* s) {
   if (!s) return PANN_OK;
   {
@@ -441,15 +510,11 @@ int pann_server_destroy(pann_server* s) {
   for (auto& kv : s->reqs) delete kv.second;
   for (Slot& sl : s->slots) {
     if (sl.st) cudaStreamSynchronize(sl.st);
-    if (sl.b) pann_batch_destroy(sl.b);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.st) cudaStreamDestroy(sl.st);
-    if (sl.d_q) cudaFree(sl.d_q);
-    if (sl.d_ids) cudaFree(sl.d_ids);
-    if (sl.d_d) cudaFree(sl.d_d);
-    if (sl.h_q) cudaFreeHost(sl.h_q);
-    if (sl.h_ids) cudaFreeHost(sl.h_ids);
-    if (sl.h_d) cudaFreeHost(sl.h_d);
+    if (sl.arena) cudaFree(sl.arena);
+    for (void* h : {(void*)sl.h_q, (void*)sl.h_k, (void*)sl.h_L, (void*)sl.h_order, (void*)sl.h_ids, (void*)sl.h_d})
+      if (h) cudaFreeHost(h);
   }
   delete s;
   return PANN_OK;

@@ -111,3 +111,40 @@ def test_server_replay_and_errors(lib_built):
         srv.submit_knn(q[:10], 10, 5)         # beam below k
     srv.close()
     idx.close()
+
+
+def test_server_admission_by_scratch(lib_built):
+    """A slot admits requests while the batch they form fits its scratch arena: with an arena that
+    holds 256 queries at k = 20, beam 80, batches of small-k, short-beam requests hold more queries
+    than batches of large ones; a request that alone needs more than the arena is refused; answers
+    equal the same requests run alone."""
+    base = random_points(np.float32, 20000, 16, 121)
+    g = O.random_graph(20000, 32, 122)
+    q = random_points(np.float32, 4000, 16, 123)
+    idx = P.Index(base, 32)
+    idx.set_graph(g)
+    probe = P.Server(idx, max_batch_queries=256, inflight=1, max_k=20, max_beam=80)
+    budget = probe.admission()["scratch_bytes"]
+    probe.close()
+    srv = P.Server(idx, max_batch_queries=4000, inflight=1, max_k=20, max_beam=80, scratch_bytes=budget)
+
+    def run(k, beam, n_req, per):
+        rows = np.arange(n_req) * per
+        alone = [idx.search(q[r:r + per], k, beam) for r in rows]
+        srv.admission(reset=True)
+        tickets = [srv.submit_knn(q[r:r + per], k, beam) for r in rows]
+        for t, a in zip(tickets, alone):
+            ids, dists, _ = srv.wait(t)
+            np.testing.assert_array_equal(ids, a.ids)
+            np.testing.assert_array_equal(dists.view(np.uint32), a.dists.view(np.uint32))
+        adm = srv.admission()
+        assert adm["scratch_peak"] <= budget
+        return adm["queries"] / adm["batches"]
+
+    small = run(5, 10, 60, 50)
+    large = run(20, 80, 60, 50)
+    assert small > large, (small, large)
+    with pytest.raises(P.PannError):
+        srv.submit_knn(q[:3000], 20, 80)      # alone more than the arena holds
+    srv.close()
+    idx.close()
