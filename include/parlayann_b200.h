@@ -325,9 +325,13 @@ typedef struct pann_batch pann_batch;
 
 typedef struct {
   int32_t use_graph; /* capture the device launch sequence as a CUDA graph on the first run, replay it after */
-  int32_t autotune;  /* time tier-0 seen-table sizes and warps per block on the first run, keep the fastest */
+  int32_t autotune;  /* time the mappings on the first run and keep the fastest (pann_batch_mapping lists the
+                        candidates' knobs: warp per query with the tier-0 seen-table size, warps per block and
+                        register budget, or CTA per query; the tile search's rows per round) */
   uint32_t seen_slots;      /* tier-0 seen-table slots (power of two; 0 = automatic) */
   uint32_t warps_per_block; /* tier-0 warps per block (1, 2 or 4; 0 = automatic) */
+  int32_t cta_per_query;    /* exact search: 1 runs every query on one block of the exact-emulation kernel
+                               (CTA per query) instead of a warp of the first tier; same answers */
 } pann_batch_options;
 
 int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, const pann_query_params* bounds,
@@ -350,6 +354,13 @@ int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32
  * Any pointer may be NULL. */
 int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps_per_block, uint32_t* blocks,
                       int32_t* graph_captured);
+/* The mapping the batch runs with (after autotuning, if any): 1 if every query
+ * runs on one block of the exact-emulation kernel (CTA per query) instead of a
+ * warp of the first tier, the resident blocks per SM the first tier's
+ * registers are fitted to (3 or 4), and the tile search's rows staged per
+ * round (0 = chosen for occupancy). Any pointer may be NULL. No reference
+ * counterpart (the reference runs one thread per query). */
+int pann_batch_mapping(const pann_batch* b, uint32_t* cta_per_query, uint32_t* register_blocks, uint32_t* tile_rows);
 
 /* Frees the batch. Device-buffer runs are asynchronous: call this after the
  * last run's stream work has completed (host-buffer runs are synchronous).

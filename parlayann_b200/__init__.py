@@ -61,7 +61,7 @@ class BatchOptions(ctypes.Structure):
     """pann_batch_options: CUDA-graph replay, autotuning, fixed tier-0 shape."""
 
     _fields_ = [("use_graph", ctypes.c_int32), ("autotune", ctypes.c_int32), ("seen_slots", ctypes.c_uint32),
-                ("warps_per_block", ctypes.c_uint32)]
+                ("warps_per_block", ctypes.c_uint32), ("cta_per_query", ctypes.c_int32)]
 
 
 class RangeParams(ctypes.Structure):
@@ -156,6 +156,7 @@ SIGNATURES = {
     "pann_batch_create": (_I, [ctypes.POINTER(_P), _P, _U32, ctypes.POINTER(QueryParams), _P, _U32,
                                ctypes.POINTER(SearchOptions), ctypes.POINTER(BatchOptions)]),
     "pann_batch_run": (_I, [_P, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _I, _P]),
+    "pann_batch_mapping": (_I, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "pann_batch_config": (_I, [_P, _P, _P, _P, _P]),
     "pann_batch_destroy": (_I, [_P]),
     "pann_build": (_I, [_P, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(BuildStats)]),
@@ -367,10 +368,10 @@ class Index:
     def batch(self, max_queries: int, max_k: int, max_beam: int, limit: int | None = None,
               degree_limit: int | None = None, batch_factor: float = 0.125, starts=(0,), precision: int = PREC_F32,
               rerank: int = 0, use_graph: bool = True, autotune: bool = False, seen_slots: int = 0,
-              warps_per_block: int = 0, parents: int = 0, scorer: int = 0) -> "Batch":
+              warps_per_block: int = 0, parents: int = 0, scorer: int = 0, cta_per_query: bool = False) -> "Batch":
         """A reusable batch for queries with per-query k and beam (pann_batch_create)."""
         return Batch(self, max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts, precision, rerank,
-                     use_graph, autotune, seen_slots, warps_per_block, parents, scorer)
+                     use_graph, autotune, seen_slots, warps_per_block, parents, scorer, cta_per_query)
 
     def range_search(self, queries: np.ndarray, beam: int, radius: float, rtype: int = RANGE_GREEDY, start: int = 0,
                      early_stopping_radius: float = 0.0, early_stopping_count: int = 0):
@@ -442,14 +443,15 @@ class Batch:
     graph). Per query the results equal Index.search with that k and beam."""
 
     def __init__(self, index: "Index", max_queries, max_k, max_beam, limit, degree_limit, batch_factor, starts,
-                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block, parents=0, scorer=0):
+                 precision, rerank, use_graph, autotune, seen_slots, warps_per_block, parents=0, scorer=0,
+                 cta_per_query=False):
         self.index = index
         self.max_k = max_k
         qp = QueryParams(max_k, max_beam, index.n if limit is None else limit,
                          index.R if degree_limit is None else degree_limit, batch_factor)
         st = np.ascontiguousarray(np.asarray(starts, dtype=np.uint32))
         opt = SearchOptions(precision, rerank, parents, scorer)
-        bo = BatchOptions(int(use_graph), int(autotune), seen_slots, warps_per_block)
+        bo = BatchOptions(int(use_graph), int(autotune), seen_slots, warps_per_block, int(cta_per_query))
         h = ctypes.c_void_p()
         _check(lib().pann_batch_create(ctypes.byref(h), index.handle, max_queries, ctypes.byref(qp), _ptr(st), len(st),
                                        ctypes.byref(opt), ctypes.byref(bo)))
@@ -474,7 +476,10 @@ class Batch:
     def config(self) -> dict:
         s, w, b, g = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int32()
         _check(lib().pann_batch_config(self._h, ctypes.byref(s), ctypes.byref(w), ctypes.byref(b), ctypes.byref(g)))
-        return dict(seen_slots=s.value, warps_per_block=w.value, blocks=b.value, graph=bool(g.value))
+        c, m, t = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(lib().pann_batch_mapping(self._h, ctypes.byref(c), ctypes.byref(m), ctypes.byref(t)))
+        return dict(seen_slots=s.value, warps_per_block=w.value, blocks=b.value, graph=bool(g.value),
+                    cta_per_query=bool(c.value), register_blocks=m.value, tile_rows=t.value)
 
     @property
     def handle(self):

@@ -30,6 +30,7 @@ struct pann_batch {
   uint32_t rerank = 0;
   uint32_t parents = 0;
   uint32_t scorer = 0;
+  uint32_t tile_rows = 0;  // tile search: rows staged per round (0 = chosen for occupancy)
   pann_batch_options bopt{};
   pann::TierSizes z{};
   // device buffers, allocated at creation
@@ -88,36 +89,64 @@ static int enqueue(pann_batch* b, const TierSizes& z, cudaStream_t st) {
     a.job_list = b->order.as<uint32_t>();
     a.njobs_dev = b->counters.as<uint32_t>() + 32;
     int rc = enqueue_tile(idx, b->plan, a, b->parents, b->counters.as<uint32_t>() + 10, b->prec, b->rerank, st,
-                          b->scorer);
+                          b->scorer, b->tile_rows);
     if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; the single-parent tiers below
   }
   return enqueue_tiers(idx, b->plan, a, z, tier_bufs(b), st, b->prec, b->rerank);
 }
 
-// Picks the tier-0 seen-table slots and warps per block by timing each
-// candidate on the staged batch (two timed runs each, the faster counts).
+// Picks how the batch maps onto the GPU by timing each candidate on the
+// staged batch (three runs each, the first warming the caches, the faster of
+// the other two counts). Every candidate gives the same answers:
+//  * exact search, warp per query: the first tier's seen-table slots
+//    ({1/2, 1, 2} x the estimate), warps per block ({2, 4}) and register
+//    budget (fitted to 3 or 4 resident blocks);
+//  * exact search, CTA per query: every query on one block of the
+//    exact-emulation kernel (when its tables fit in shared memory);
+//  * tile search (precision form, parents > 0): the rows staged and scored per
+//    round (the tile's height: all the step's candidates, 3/4, 1/2 or 1/4).
 static int autotune(pann_batch* b, cudaStream_t st) {
-  const uint32_t base_S = b->z.S;
-  const uint32_t floor_S = 4 * (b->idx->R + 1);
-  std::vector<std::pair<uint32_t, int>> cands;
-  for (uint32_t S : {base_S / 2, base_S, base_S * 2})
-    for (int w : {2, 4})
-      if (S >= floor_S && S <= 16384) cands.push_back({S, w});
+  struct Cand {
+    TierSizes z;
+    uint32_t tile_rows;
+  };
+  std::vector<Cand> cands;
+  const bool tile = b->parents > 0 && b->prec != PREC_F32;
+  if (tile) {
+    const uint32_t cw = std::max<uint32_t>(1, std::min<uint32_t>(b->parents, 4)) * std::min(b->plan.dl, b->idx->R);
+    for (uint32_t f : {4u, 3u, 2u, 1u}) cands.push_back({b->z, std::max<uint32_t>(16, cw * f / 4)});
+  } else {
+    const uint32_t base_S = b->z.S;
+    const uint32_t floor_S = 4 * (b->idx->R + 1);
+    for (uint32_t S : {base_S / 2, base_S, base_S * 2})
+      for (int w : {2, 4})
+        for (int minb : {3, 4}) {
+          if (S < floor_S || S > 16384) continue;
+          if (minb == 4 && b->prec != PREC_F32) continue;
+          TierSizes z;
+          if (size_tiers(b->idx, b->plan, b->max_q, b->prec, S, w, &z, minb) != PANN_OK) continue;
+          if (z.S != S || z.wpb != w) continue;  // did not fit as asked
+          cands.push_back({z, 0});
+        }
+    if (b->prec == PREC_F32 && b->z.emu_smem) {
+      TierSizes z = b->z;
+      z.cta = true;
+      cands.push_back({z, 0});
+    }
+  }
   cudaEvent_t e0, e1;
   PANN_CUDA(cudaEventCreate(&e0));
   PANN_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  TierSizes best_z = b->z;
+  Cand best_c{b->z, b->tile_rows};
   int rc = PANN_OK;
   for (auto& c : cands) {
-    TierSizes z;
-    if (size_tiers(b->idx, b->plan, b->max_q, b->prec, c.first, c.second, &z) != PANN_OK) continue;
-    if (z.S != c.first || z.wpb != c.second) continue;  // did not fit as asked
-    if ((rc = ensure_tier_buffers(b, z)) != PANN_OK) break;
+    if ((rc = ensure_tier_buffers(b, c.z)) != PANN_OK) break;
+    b->tile_rows = c.tile_rows;
     float t_min = 1e30f;
     for (int rep = 0; rep < 3 && rc == PANN_OK; rep++) {
       cudaEventRecord(e0, st);
-      rc = enqueue(b, z, st);
+      rc = enqueue(b, c.z, st);
       cudaEventRecord(e1, st);
       if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "autotune run");
       float ms = 0;
@@ -127,13 +156,14 @@ static int autotune(pann_batch* b, cudaStream_t st) {
     if (rc) break;
     if (t_min < best) {
       best = t_min;
-      best_z = z;
+      best_c = c;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  b->z = best_z;
+  b->z = best_c.z;
+  b->tile_rows = best_c.tile_rows;
   return PANN_OK;
 }
 
@@ -302,6 +332,12 @@ int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, c
   };
   rc = size_tiers(idx, plan, max_queries, prec, b->bopt.seen_slots, (int)b->bopt.warps_per_block, &b->z);
   if (rc) return bail(rc);
+  if (b->bopt.cta_per_query) {
+    if (prec != PANN_PREC_F32 || !b->z.emu_smem)
+      return bail(fail(PANN_EINVAL, "CTA per query needs the exact search and emulated tables that fit in shared "
+                                    "memory at this beam"));
+    b->z.cta = true;
+  }
   const size_t m = max_queries;
   cudaError_t e = cudaSuccess;
   auto need = [&](DevBuf& d, size_t bytes) {
@@ -381,7 +417,7 @@ int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32
   PANN_CUDA(cudaEventRecord(b->staged, st));
 
   int rc = PANN_OK;
-  if (b->runs == 0 && b->bopt.autotune && !b->bopt.seen_slots && !b->bopt.warps_per_block) {
+  if (b->runs == 0 && b->bopt.autotune && !b->bopt.seen_slots && !b->bopt.warps_per_block && !b->bopt.cta_per_query) {
     rc = autotune(b, st);
     if (rc) return rc;
   }
@@ -445,6 +481,14 @@ int pann_batch_config(const pann_batch* b, uint32_t* seen_slots, uint32_t* warps
   if (warps_per_block) *warps_per_block = (uint32_t)b->z.wpb;
   if (blocks) *blocks = (uint32_t)b->z.blocks;
   if (graph_captured) *graph_captured = b->exec != nullptr;
+  return PANN_OK;
+}
+
+int pann_batch_mapping(const pann_batch* b, uint32_t* cta_per_query, uint32_t* register_blocks, uint32_t* tile_rows) {
+  if (!b) return fail(PANN_EINVAL, "batch is NULL");
+  if (cta_per_query) *cta_per_query = b->z.cta ? 1u : 0u;
+  if (register_blocks) *register_blocks = (uint32_t)b->z.minb;
+  if (tile_rows) *tile_rows = b->tile_rows;
   return PANN_OK;
 }
 

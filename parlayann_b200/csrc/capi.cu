@@ -184,16 +184,18 @@ static int t0_minb() {
   return v;
 }
 
+// The first tier's kernel fitted to `minb` resident 128-thread blocks (3 or 4).
 template <int DT, int MT, bool G, int PREC = PREC_F32>
-static auto search_kernel_ptr() {
-  if constexpr (DT == DT_F32 && MT == MT_L2 && !G && PREC == PREC_F32)
-    if (t0_minb() == 4) return search_kernel<DT, MT, G, PREC, 4>;
+static auto search_kernel_ptr(int minb) {
+  if constexpr (!G && PREC == PREC_F32)
+    if (minb == 4) return search_kernel<DT, MT, G, PREC, 4>;
   return search_kernel<DT, MT, G, PREC, 3>;
 }
 
 template <int DT, int MT, bool G, int PREC = PREC_F32>
-static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st) {
-  auto k = search_kernel_ptr<DT, MT, G, PREC>();
+static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads, size_t smem, cudaStream_t st,
+                                   int minb) {
+  auto k = search_kernel_ptr<DT, MT, G, PREC>(minb);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return e;
   k<<<blocks, threads, smem, st>>>(a);
@@ -201,13 +203,13 @@ static cudaError_t launch_search_t(const SearchArgs& a, int blocks, int threads,
 }
 
 cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks,
-                                 int threads, size_t smem, cudaStream_t st, int prec) {
+                                 int threads, size_t smem, cudaStream_t st, int prec, int minb) {
   if (prec != PREC_F32) {
     if (dtype != DT_F32) return cudaErrorInvalidValue;
 #define PANN_LP_CASE(MT, PR)                                                               \
     if (metric == MT && prec == PR)                                                        \
-      return global_table ? launch_search_t<DT_F32, MT, true, PR>(a, blocks, threads, smem, st) \
-                          : launch_search_t<DT_F32, MT, false, PR>(a, blocks, threads, smem, st);
+      return global_table ? launch_search_t<DT_F32, MT, true, PR>(a, blocks, threads, smem, st, 3) \
+                          : launch_search_t<DT_F32, MT, false, PR>(a, blocks, threads, smem, st, 3);
     PANN_LP_CASE(MT_L2, PREC_BF16)
     PANN_LP_CASE(MT_IP, PREC_BF16)
     PANN_LP_CASE(MT_L2, PREC_FP8)
@@ -217,8 +219,8 @@ cudaError_t launch_search(int dtype, int metric, bool global_table, const Search
   }
 #define PANN_SEARCH_CASE(DT, MT)                                                        \
   if (dtype == DT && metric == MT)                                                      \
-    return global_table ? launch_search_t<DT, MT, true>(a, blocks, threads, smem, st)   \
-                        : launch_search_t<DT, MT, false>(a, blocks, threads, smem, st);
+    return global_table ? launch_search_t<DT, MT, true>(a, blocks, threads, smem, st, 3)   \
+                        : launch_search_t<DT, MT, false>(a, blocks, threads, smem, st, minb);
   PANN_SEARCH_CASE(DT_U8, MT_L2)
   PANN_SEARCH_CASE(DT_U8, MT_IP)
   PANN_SEARCH_CASE(DT_I8, MT_L2)
@@ -277,16 +279,17 @@ cudaError_t launch_emulate_block(int dtype, int metric, const SearchArgs& a, con
 }
 
 template <int DT, int MT, bool G, int PREC = PREC_F32>
-static int occupancy_t(int threads, size_t smem) {
+static int occupancy_t(int threads, size_t smem, int minb = 3) {
   int nb = 0;
-  auto k = search_kernel_ptr<DT, MT, G, PREC>();
+  auto k = search_kernel_ptr<DT, MT, G, PREC>(minb);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, threads, smem) != cudaSuccess) return 0;
   return nb;
 }
-int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem) {
+int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem, int minb) {
 #define PANN_OCC_CASE(DT, MT) \
-  if (dtype == DT && metric == MT) return g ? occupancy_t<DT, MT, true>(threads, smem) : occupancy_t<DT, MT, false>(threads, smem);
+  if (dtype == DT && metric == MT) \
+    return g ? occupancy_t<DT, MT, true>(threads, smem) : occupancy_t<DT, MT, false>(threads, smem, minb);
   PANN_OCC_CASE(DT_U8, MT_L2)
   PANN_OCC_CASE(DT_U8, MT_IP)
   PANN_OCC_CASE(DT_I8, MT_L2)
@@ -329,7 +332,7 @@ uint32_t tier0_slots(const SearchPlan& p, uint32_t R) {
 // global table per warp; (E) queries on which the reference's hashset grows,
 // re-run with that hashset emulated exactly.
 int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int precision, uint32_t S_force,
-               int wpb_force, TierSizes* z) {
+               int wpb_force, TierSizes* z, int minb_force) {
   const size_t smem_cap = idx->smem_optin;
   TierSizes& t = *z;
   t = TierSizes{};
@@ -344,7 +347,8 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
     wb = search_warp_bytes(idx->stride, plan.L, plan.Ccap, idx->R, S, false);
   }
   if ((size_t)wb * wpb > smem_cap) return fail(PANN_EINVAL, "search state for this beam does not fit in shared memory");
-  int occ = precision == PREC_F32 ? search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb)
+  t.minb = precision == PREC_F32 ? (minb_force == 4 || (minb_force == 0 && t0_minb() == 4) ? 4 : 3) : 3;
+  int occ = precision == PREC_F32 ? search_occupancy(idx->dtype, idx->metric, false, 32 * wpb, (size_t)wb * wpb, t.minb)
                                   : lp_occupancy(idx->metric, precision, 32 * wpb, (size_t)wb * wpb);
   if (occ <= 0) occ = 1;
   uint64_t want = (std::max<uint64_t>(nq, 1) + wpb - 1) / wpb;
@@ -431,7 +435,47 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
     }
     t.gspill = b.gspill;
     t.Sg = b.gspill ? z.Sg : 0;
-    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, z.blocks, 32 * z.wpb, (size_t)z.wb * z.wpb, st, precision));
+    if (z.cta && precision == PREC_F32 && z.emu_smem) {
+      // CTA per query: every query on a block of the exact-emulation kernel from its start points
+      // (the same answers: that kernel is the reference's search with its hashset as written);
+      // queries whose emulated table outgrows shared memory continue in the global tier below
+      SearchArgs c = a;
+      c.redo_list = nullptr;
+      c.redo_count = nullptr;
+      c.emu_list = nullptr;
+      c.emu_count = nullptr;
+      c.job_list = b.job_list0;
+      c.njobs_dev = b.njobs0;
+      c.job_counter = cnt + 5;
+      EmuArgs e{};
+      e.bits0 = z.bits0;
+      e.vs_slots = z.vs;
+      e.base_bytes = z.base;
+      e.capA = (uint32_t)(4 * z.S0);
+      e.capB = (uint32_t)(2 * z.S0);
+      e.overflow_list = b.ovf;
+      e.overflow_rec = b.ovf_rec;
+      e.overflow_count = cnt + 8;
+      e.job_rec = nullptr;
+      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, c, e, idx->sm_count, z.emu_smem_need, st));
+      EmuArgs e2 = e;
+      e2.gA = b.ge2;
+      e2.gB = e2.gA + (size_t)z.e2_slots * z.capA;
+      e2.capA = (uint32_t)z.capA;
+      e2.capB = (uint32_t)z.capB;
+      e2.overflow_list = nullptr;
+      e2.overflow_rec = nullptr;
+      e2.overflow_count = nullptr;
+      e2.job_rec = b.ovf_rec;
+      c.job_list = b.ovf;
+      c.njobs_dev = cnt + 8;
+      c.job_counter = cnt + 7;
+      PANN_CUDA(launch_emulate(idx->dtype, idx->metric, false, c, e2, z.e2_slots,
+                               emu_smem_bytes(z.base, z.vs, 0, 0, false), st));
+      return PANN_OK;
+    }
+    PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, z.blocks, 32 * z.wpb, (size_t)z.wb * z.wpb, st, precision,
+                            z.minb));
   }
   // ---- tier 2: queries whose tables still filled up, with one global-memory
   // seen table per warp sized above the reference's own capacity

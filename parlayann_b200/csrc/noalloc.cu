@@ -37,10 +37,10 @@ namespace pann {
 
 // defined in capi.cu
 cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks, int threads,
-                          size_t smem, cudaStream_t st, int prec);
+                          size_t smem, cudaStream_t st, int prec, int minb = 3);
 cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
                            int blocks, size_t smem, cudaStream_t st);
-int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem);
+int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem, int minb = 3);
 uint32_t tier0_slots(const SearchPlan& p, uint32_t R);
 
 constexpr size_t kNoallocScratchBytes = PANN_NOALLOC_SCRATCH_BYTES;

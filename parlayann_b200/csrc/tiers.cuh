@@ -13,6 +13,8 @@ struct TierSizes {
   // tier 0: shared-memory seen tables, per-warp global spill tables
   uint32_t S = 0, wb = 0, Sg = 0;
   int wpb = 0, blocks = 0;
+  int minb = 3;      // resident blocks the first tier's registers are fitted to (3 or 4)
+  bool cta = false;  // every query on one block of the exact-emulation kernel instead of the first tiers
   size_t slots = 0, spill_bytes = 0;
   // hand-off from tier 0 to the emulation tier
   uint32_t logcap = 0, viscap = 0;
@@ -45,25 +47,26 @@ struct TierBufs {
 };
 
 cudaError_t launch_search(int dtype, int metric, bool global_table, const SearchArgs& a, int blocks, int threads,
-                          size_t smem, cudaStream_t st, int prec);
+                          size_t smem, cudaStream_t st, int prec, int minb = 3);
 cudaError_t launch_emulate(int dtype, int metric, bool smem_tables, const SearchArgs& a, const EmuArgs& e,
                            int blocks, size_t smem, cudaStream_t st);
 // Warps per block of the shared-memory emulation tier (one query per block).
 constexpr int EMU_BLOCK_WARPS = 4;
 cudaError_t launch_emulate_block(int dtype, int metric, const SearchArgs& a, const EmuArgs& e, int blocks, size_t smem,
                                  cudaStream_t st);
-int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem);
+int search_occupancy(int dtype, int metric, bool g, int threads, size_t smem, int minb = 3);
 uint32_t tier0_slots(const SearchPlan& p, uint32_t R);
 
 // S_force / wpb_force (0 = automatic) override the tier-0 seen-table slots and
 // warps per block.
 int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int precision, uint32_t S_force,
-               int wpb_force, TierSizes* z);
+               int wpb_force, TierSizes* z, int minb_force = 0);
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a, const TierSizes& z,
                   const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank);
 // The multi-parent tile search of the precision form (tile.cu).
+// tile_rows > 0 fixes the rows staged per round (CUDA-core scoring), else chosen for occupancy.
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
-                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer = 0);
+                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer = 0, uint32_t tile_rows = 0);
 // Validates the start points and copies them to idx->starts (cached).
 int stage_starts(pann_index* idx, const uint32_t* starts, uint32_t n_start, cudaStream_t st);
 // The index's own tier buffers for nq queries (grown as needed).

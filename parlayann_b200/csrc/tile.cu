@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
 // with tensor-core scoring, rounds of TC_ROWS rows.
 template <int MT, int PREC, bool TC>
 static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W, uint32_t S, uint32_t CW,
-                         cudaStream_t st) {
+                         cudaStream_t st, uint32_t tile_rows) {
   auto k = search_tile_kernel<MT, PREC, TC>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
   if (e != cudaSuccess) return cuda_fail(e, "tile kernel attribute");
@@ -492,7 +492,12 @@ static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W,
   size_t smem = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, CWs, TC).total;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem) != cudaSuccess || occ <= 0) occ = 1;
-  for (uint32_t f = 3; f >= 2 && !TC; f--) {
+  if (!TC && tile_rows > 0) {
+    CWs = std::min<uint32_t>(CW, std::max<uint32_t>(16, (tile_rows + 15) & ~15u));
+    smem = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, CWs).total;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem) != cudaSuccess || occ <= 0) occ = 1;
+  }
+  for (uint32_t f = 3; f >= 2 && !TC && tile_rows == 0; f--) {
     const uint32_t cws = std::max<uint32_t>(32, (CW * f / 4 + 15) & ~15u);
     const size_t sm2 = tile_layout(idx->d, a.L, CW, S, idx->lp_stride, cws).total;
     int occ2 = 0;
@@ -516,7 +521,7 @@ static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W,
 // single-parent path. scorer 1 scores on the tensor cores (rows of an even
 // number of 16-byte chunks; otherwise a clear error).
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
-                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer) {
+                 int precision, uint32_t rerank, cudaStream_t st, uint32_t scorer, uint32_t tile_rows) {
   const bool tc = scorer == PANN_SCORER_TENSOR;
   if (tc && (idx->lp_chunks % 2 != 0 || !idx->lp_norms.p))
     return fail(PANN_EDEVICE, "tensor-core scoring needs low-precision rows of an even number of 16-byte chunks "
@@ -541,8 +546,8 @@ int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, ui
   const int mt = idx->metric;
 #define PANN_TILE_CASE(MTV, PRV)                                                          \
   if (mt == MTV && precision == PRV)                                                    \
-    return tc ? launch_tile_t<MTV, PRV, true>(idx, a, W, S, W * nel, st)                \
-              : launch_tile_t<MTV, PRV, false>(idx, a, W, S, W * nel, st);
+    return tc ? launch_tile_t<MTV, PRV, true>(idx, a, W, S, W * nel, st, 0)             \
+              : launch_tile_t<MTV, PRV, false>(idx, a, W, S, W * nel, st, tile_rows);
   PANN_TILE_CASE(MT_L2, PREC_BF16)
   PANN_TILE_CASE(MT_IP, PREC_BF16)
   PANN_TILE_CASE(MT_L2, PREC_FP8)

@@ -104,12 +104,15 @@ def test_batch_autotune_and_fixed_shapes(lib_built):
     q = random_points(np.uint8, 2000, 32, 23)
     k, beam = uneven_shapes(len(q), 24, ks=(1, 10, 40))
     o = per_query_oracle(base, q, g, k, beam)
-    for opts in (dict(autotune=True), dict(seen_slots=512, warps_per_block=2), dict(use_graph=False)):
+    for opts in (dict(autotune=True), dict(seen_slots=512, warps_per_block=2), dict(use_graph=False),
+                 dict(cta_per_query=True)):
         b = idx.batch(len(q), int(k.max()), int(beam.max()), **opts)
         check(b.run(q, k, beam), o, str(opts))
         cfg = b.config()
         if "seen_slots" in opts:
             assert cfg["seen_slots"] == 512 and cfg["warps_per_block"] == 2
+        assert cfg["cta_per_query"] == opts.get("cta_per_query", cfg["cta_per_query"])
+        assert cfg["register_blocks"] in (3, 4)
         assert cfg["graph"] == opts.get("use_graph", True)
         b.close()
     idx.close()
@@ -158,5 +161,43 @@ def test_batch_argument_errors(lib_built):
         b.run(np.concatenate([q, q]), 5, 10)                   # more queries than max_queries
     r = b.run(q[:0], 5, 10)                                    # empty run
     assert r.ids.shape == (0, 5)
+    b.close()
+    idx.close()
+
+
+def test_batch_cta_per_query_with_hashset_growth(lib_built):
+    """CTA per query (every query on one block of the exact-emulation kernel) gives the oracle's
+    answers, the queries whose hashset grows included, and again on graph replay."""
+    base = random_points(np.uint8, 20000, 8, 1)
+    g = O.random_graph(20000, 64, 3, min_deg=60)
+    idx = P.Index(base, 64)
+    idx.set_graph(g)
+    q = random_points(np.uint8, 300, 8, 2)
+    rng = np.random.default_rng(5)
+    beam = rng.choice(np.array([12, 24, 40, 50, 64], np.uint32), len(q)).astype(np.uint32)
+    k = np.minimum(beam, 10).astype(np.uint32)
+    b = idx.batch(len(q), 10, 64, batch_factor=1.0, cta_per_query=True)
+    o = per_query_oracle(base, q, g, k, beam, batch_factor=1.0)
+    assert (o["hash_grew"] > 0).sum() > 0
+    check(b.run(q, k, beam), o, "cta")
+    check(b.run(q, k, beam), o, "cta replay")
+    assert b.config()["cta_per_query"]
+    b.close()
+    idx.close()
+
+
+def test_batch_tile_autotune_keeps_answers(lib_built):
+    """The tile search's rows per round, picked by the autotuner, do not change its answers."""
+    base = P.synth_mixture(P.F32, 20000, 64, 32, 2, 0, sigma=0.3, normalize=True)
+    q = P.synth_mixture(P.F32, 1000, 64, 32, 2, 1, sigma=0.3, normalize=True)
+    idx = P.Index(base, 32)
+    idx.build(48, 1.2)
+    idx.set_precision(P.PREC_FP8)
+    plain = idx.search(q, 10, 40, precision=P.PREC_FP8, parents=3)
+    b = idx.batch(len(q), 10, 40, precision=P.PREC_FP8, parents=3, autotune=True)
+    r = b.run(q, 10, 40)
+    np.testing.assert_array_equal(r.ids[:, :10], plain.ids)
+    np.testing.assert_array_equal(r.dists[:, :10].view(np.uint32), plain.dists.view(np.uint32))
+    assert b.config()["tile_rows"] > 0
     b.close()
     idx.close()
