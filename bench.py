@@ -616,6 +616,50 @@ def run_c2(dev, flush, args, want):
     return out
 
 
+def run_c3(dev, flush, args):
+    """The batched form on a large uint8 index: n base vectors (100,000,000 in the full configuration;
+    --c3-n) x 128-d uint8 from the small configuration's generator with 1,024 components, seed 0,
+    Vamana R=64 L=128 alpha=1.2 two passes built on the GPU; 100,000 queries with per-query k uniform
+    in {1,10,100} and beam uniform in [k, 4k] in one autotuned batch, against one plain launch at the
+    largest k and beam; recall@k per k class on the first 1,000 queries against exact (integer)
+    groundtruth."""
+    import torch
+
+    import parlayann_b200 as P
+
+    n, nq, d = args.c3_n, 100_000, 128
+    t0 = time.time()
+    base = P.synth_mixture(P.U8, n, d, 1024, 0, 0)
+    q = P.synth_mixture(P.U8, nq, d, 1024, 0, 1)
+    gen_s = time.time() - t0
+    stream = torch.cuda.current_stream(dev)
+    idx = P.Index(base, W["R"])
+    bst = idx.build(W["Lb"], W["alpha"], num_passes=W["passes"], batch_factor=W["bf"])
+    dq = torch.from_numpy(q).to(dev)
+    out = {"workload": f"{n:,} x 128-d uint8 (1024-component mixture, seed 0), {nq:,} queries, Vamana R=64 L=128 "
+                       "alpha=1.2 two passes (GPU build)",
+           "n": n, "build_seconds_device": round(bst.seconds, 2), "generate_seconds_host": round(gen_s, 2),
+           "resident_bytes": int(n) * (128 + 4 * W["R"])}
+    out.update(run_batched_uneven(idx, q, dq, dev, flush, stream, max(3, min(args.steps, 5)), P.lib()))
+    sub = 1000
+    gt, _ = idx.groundtruth(q[:sub], 100)
+    rng = np.random.default_rng(5)
+    ks = rng.choice(np.array([1, 10, 100], np.uint32), nq).astype(np.uint32)[:sub]
+    Ls = np.array([rng.integers(max(kk, 1), 4 * kk + 1) for kk in ks], np.uint32)
+    rec = {}
+    for kk in (1, 10, 100):
+        sel = np.where(ks == kk)[0]
+        hits = 0
+        for i in sel:
+            r = idx.search(q[i:i + 1], int(kk), int(Ls[i]))
+            hits += len(set(r.ids[0].tolist()) & set(gt[i, :kk].tolist()))
+        rec[f"recall_at_{kk}"] = round(hits / float(kk * len(sel)), 4) if len(sel) else None
+    out["recall_sample"] = {"queries": sub, **rec, "note": "each query at its own k and beam, ids against exact "
+                                                              "integer groundtruth"}
+    idx.close()
+    return out
+
+
 def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
     """The precision, batched and serving forms and range search on the same
     index, each next to the plain form: QPS at recall@10 >= 0.95 (device
@@ -735,6 +779,8 @@ def run_forms(idx, base, q, gt, gd, beam, qps_plain, dev, flush, args):
         out["search_and_parse"] = search_and_parse(idx, base, q, gt, dev, flush, stream)
     if "c2" in want:
         out["precision_10m"] = run_c2(dev, flush, args, want)
+    if "c3" in want:
+        out["batched_large_u8"] = run_c3(dev, flush, args)
     return out
 
 
@@ -748,21 +794,26 @@ def range_radius(base, q):
     return float(np.quantile(np.concatenate(samp), 0.01))
 
 
-def run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib):
+def run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib, n_index=None):
     """Per-query k in {1,10,100} and beam in [k, 4k] through one batch object
-    (graph replay), against the plain form run per (k, beam) group."""
+    (autotuned mapping, graph replay), against the plain form in one launch at
+    the largest k and beam (what a caller without per-query parameters runs);
+    the batch's answers are checked against the plain form run per (k, beam)
+    group (untimed)."""
     import torch
 
     import parlayann_b200 as P
 
     nq = q.shape[0]
+    n_index = n_index or idx.n
     starts = np.zeros(1, np.uint32)
     rng = np.random.default_rng(5)
     ks = rng.choice(np.array([1, 10, 100], np.uint32), nq).astype(np.uint32)
     Ls = np.array([rng.integers(max(kk, 1), 4 * kk + 1) for kk in ks], np.uint32)
-    b = idx.batch(nq, 100, int(Ls.max()))
-    d_ids = torch.empty((nq, 100), dtype=torch.int32, device=dev)
-    d_d = torch.empty((nq, 100), dtype=torch.float32, device=dev)
+    kmax, Lmax = 100, int(Ls.max())
+    b = idx.batch(nq, kmax, Lmax, autotune=True)
+    d_ids = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
+    d_d = torch.empty((nq, kmax), dtype=torch.float32, device=dev)
 
     def step_u():
         rc = lib.pann_batch_run(b.handle, ctypes.c_void_p(dq.data_ptr()), nq, ks.ctypes.data_as(ctypes.c_void_p),
@@ -774,30 +825,30 @@ def run_batched_uneven(idx, q, dq, dev, flush, stream, steps, lib):
 
     t_b = _timed(step_u, flush, stream, steps, 3)
     ids_u = d_ids.cpu().numpy().astype(np.uint32)
+    mapping = b.config()
     b.close()
-    # the plain form on the same mix: one pann_search_device launch sequence per (k, beam) group
-    groups = {}
-    for i, (kk, LL) in enumerate(zip(ks.tolist(), Ls.tolist())):
-        groups.setdefault((kk, LL), []).append(i)
-    gq = {key: torch.from_numpy(q[np.array(v)]).to(dev) for key, v in groups.items()}
-    gout = {key: torch.empty((len(v), key[0]), dtype=torch.int32, device=dev) for key, v in groups.items()}
+    # the plain form in one launch at the largest k and beam
+    qp = P.QueryParams(kmax, Lmax, n_index, idx.R, W["bf"])
+    d_p = torch.empty((nq, kmax), dtype=torch.int32, device=dev)
 
-    def step_plain_groups():
-        for key, v in groups.items():
-            qp = P.QueryParams(key[0], key[1], W["n"], W["R"], W["bf"])
-            rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(gq[key].data_ptr()), len(v), ctypes.byref(qp),
-                                        starts.ctypes.data_as(ctypes.c_void_p), 1,
-                                        ctypes.c_void_p(gout[key].data_ptr()), None, None, None, None,
-                                        ctypes.c_void_p(stream.cuda_stream))
-            if rc != 0:
-                raise P.PannError(rc, lib.pann_last_error().decode())
+    def step_plain_max():
+        rc = lib.pann_search_device(idx.handle, ctypes.c_void_p(dq.data_ptr()), nq, ctypes.byref(qp),
+                                    starts.ctypes.data_as(ctypes.c_void_p), 1, ctypes.c_void_p(d_p.data_ptr()),
+                                    None, None, None, None, ctypes.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise P.PannError(rc, lib.pann_last_error().decode())
 
-    t_p = _timed(step_plain_groups, flush, stream, steps, 3)
-    exact = all(np.array_equal(ids_u[np.array(v), :key[0]], gout[key].cpu().numpy().astype(np.uint32))
-                for key, v in groups.items())
+    t_p = _timed(step_plain_max, flush, stream, steps, 3)
+    # bit-exact per query with the plain form at the query's own k and beam (untimed)
+    exact = True
+    for kk, LL in sorted(set(zip(ks.tolist(), Ls.tolist()))):
+        sel = np.where((ks == kk) & (Ls == LL))[0]
+        r = idx.search(q[sel], kk, LL, batch_factor=W["bf"])
+        exact &= bool(np.array_equal(ids_u[sel, :kk], r.ids))
     return {"queries": nq, "k": "uniform in {1,10,100}", "beam": "uniform in [k, 4k]",
-            "qps_batched_graph": round(nq / t_b, 1), "qps_plain_per_shape": round(nq / t_p, 1),
-            "shape_groups": len(groups), "speedup": round(t_p / t_b, 3), "bit_exact_with_plain": bool(exact)}
+            "qps_batched_graph": round(nq / t_b, 1), "qps_plain_one_launch_at_max_k_and_beam": round(nq / t_p, 1),
+            "max_k": kmax, "max_beam": Lmax, "speedup_vs_one_launch": round(t_p / t_b, 3),
+            "mapping": mapping, "bit_exact_with_plain": exact}
 
 
 def run_serving(idx, q, nq, beam, radius, prec_out):
@@ -983,6 +1034,8 @@ def main():
                     help="comma list of the forms to run (precision, batched, range, serving, sweep: the "
                          "reference's search_and_parse sweep, and c2: the precision form on a 10M-point index, "
                          "Euclidean and mips)")
+    ap.add_argument("--c3-n", type=int, default=100_000_000,
+                    help="base vectors of the large uint8 batched-form run (forms c3)")
     ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
     ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
     args = ap.parse_args()

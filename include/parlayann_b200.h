@@ -278,24 +278,30 @@ int pann_range_fetch(pann_index* idx, uint32_t* out_ids, uint64_t ids_cap);
 
 /* ---------------------------------------------------------------- quantized search */
 
-/* The reference's own mixed-precision search for float Euclidian indexes: the
- * beam search runs on one-byte scalar-quantized points and the frontier is
+/* The reference's own mixed-precision search for float indexes: the beam
+ * search runs on one-byte scalar-quantized points and the frontier is
  * re-ranked with float distances (beam_search_rerank, beamSearch.h:529-597,
- * as GraphIndex::search_dispatch calls it, python/graph_index.cpp:140-160).
+ * as GraphIndex::search_dispatch calls it, python/graph_index.cpp:140-185).
  *
- * pann_index_set_quantized builds the quantized copy as
+ * pann_index_set_quantized builds the quantized copy. Euclidean indexes: as
  * PointRange<Euclidian_Point<uint8_t>>(Points) does (euclidian_point.h:186-240):
  * slope = 255 / (max - min) over every value with 0 included (all
  * non-negative integers: [0, 255]), offset = round(min * slope), each value
- * round(x * slope) - offset clamped to [0, 255]. Float Euclidean indexes only;
- * call it again after pann_index_set_points. pann_index_quant_params returns
- * the slope and offset. */
+ * round(x * slope) - offset clamped to [0, 255]. Mips indexes: as
+ * PointRange<Quantized_Mips_Point<8, true>>(Points) does (mips_point.h:293-499):
+ * per point the minimum and maximum value (0 included), the minimum of rank
+ * (size_t)(1e-4 n) of the minima and the maximum of rank (size_t)((1 - 1e-4)
+ * (n - 1)) of the maxima, bound = max(max, -min), scale = 127 / bound, each
+ * value round(x * scale) as int8 (+-127 beyond +-bound); the reference
+ * normalises mips points and queries first, which callers of this ABI do
+ * themselves. Call it again after pann_index_set_points.
+ * pann_index_quant_params returns the slope and offset (mips: the scale and 0). */
 int pann_index_set_quantized(pann_index* idx);
 int pann_index_quant_params(const pann_index* idx, float* slope, int32_t* offset);
 
 /* Host buffers, float queries (nq x d). The queries are quantized the same
  * way, the search over the quantized points (QueryParams qp, exact as
- * pann_search on a uint8 index) keeps min(k * rerank_factor, beam) frontier
+ * pann_search on a uint8 Euclidean / int8 mips index) keeps min(k * rerank_factor, beam) frontier
  * entries, these are re-scored with the float distance and ordered by
  * (distance, id), and the first k written (out_ids/out_dists nq x k).
  * out_visited / out_cmps (may be NULL) are the quantized search's counts, as

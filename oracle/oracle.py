@@ -66,8 +66,10 @@ def olib():
         L.oracle_range_groundtruth.restype = _I
         L.oracle_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
         L.oracle_search_quantized.restype = _I
-        L.oracle_search_quantized.argtypes = [_U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _D,
-                                              _U32, _P, _P, _P, _P]
+        L.oracle_search_quantized.argtypes = [_I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D,
+                                              _D, _U32, _P, _P, _P, _P]
+        L.oracle_quant_params_mips.restype = None
+        L.oracle_quant_params_mips.argtypes = [_U32, _U32, _P, _P, _P]
         L.oracle_quant_params.restype = None
         L.oracle_quant_params.argtypes = [_U32, _U32, _P, _P, _P]
         L.oracle_distance.restype = ctypes.c_float
@@ -104,8 +106,8 @@ def rlib():
         L.ref_range_groundtruth.restype = _I
         L.ref_range_groundtruth.argtypes = [_I, _I, _U32, _U32, _P, _U32, _P, ctypes.c_float, _P, _P, _U64]
         L.ref_search_quantized.restype = _I
-        L.ref_search_quantized.argtypes = [_U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _D, _U32,
-                                           _P, _P, _P, _P, _P, _P, _P]
+        L.ref_search_quantized.argtypes = [_I, _U32, _U32, _P, _U32, _P, _U32, _P, _U32, _U32, _U64, _U32, _D, _D,
+                                           _U32, _P, _P, _P, _P, _P, _P, _P]
         L.ref_num_workers.restype = _I
         L.ref_num_workers.argtypes = []
         _rlib = L
@@ -226,10 +228,11 @@ def range_groundtruth(impl, base, queries, radius, metric=0):
 
 
 def search_quantized(impl, base, queries, graph, k, L, rerank_factor=100.0, limit=None, degree_limit=None,
-                     batch_factor=0.125, start=0):
+                     batch_factor=0.125, start=0, metric=0):
     """beam_search_rerank over one-byte scalar-quantized float points with a float re-rank ('oracle':
-    pann_oracle.c; 'ref': the reference compiled in place). Returns dict(ids, dists, visited, cmps, slope,
-    offset[, seconds])."""
+    pann_oracle.c; 'ref': the reference compiled in place); metric 0 Euclidian_Point<uint8_t>, 1
+    Quantized_Mips_Point<8, true>. Returns dict(ids, dists, visited, cmps, slope, offset[, seconds]); for
+    mips slope is the scale and offset 0."""
     base = np.ascontiguousarray(base, dtype=np.float32)
     queries = np.ascontiguousarray(queries, dtype=np.float32)
     graph = np.ascontiguousarray(graph, dtype=np.uint32)
@@ -246,13 +249,18 @@ def search_quantized(impl, base, queries, graph, k, L, rerank_factor=100.0, limi
     offset = np.zeros(1, np.int32)
     out = {}
     if impl == "oracle":
-        rc = olib().oracle_search_quantized(n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit, degree_limit,
-                                            rerank_factor, batch_factor, start, _p(ids), _p(dists), _p(vis), _p(cmps))
-        olib().oracle_quant_params(n, d, _p(base), _p(slope), _p(offset))
+        rc = olib().oracle_search_quantized(metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit,
+                                            degree_limit, rerank_factor, batch_factor, start, _p(ids), _p(dists),
+                                            _p(vis), _p(cmps))
+        if metric == 0:
+            olib().oracle_quant_params(n, d, _p(base), _p(slope), _p(offset))
+        else:
+            bound = np.zeros(1, np.float32)
+            olib().oracle_quant_params_mips(n, d, _p(base), _p(slope), _p(bound))
     else:
         secs = np.zeros(1, np.float64)
         with _stdout_to_stderr():
-            rc = rlib().ref_search_quantized(n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit,
+            rc = rlib().ref_search_quantized(metric, n, d, _p(base), nq, _p(queries), R, _p(graph), k, L, limit,
                                              degree_limit, rerank_factor, batch_factor, start, _p(ids), _p(dists),
                                              _p(vis), _p(cmps), _p(slope), _p(offset), _p(secs))
         out["seconds"] = float(secs[0])

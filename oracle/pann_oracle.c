@@ -491,29 +491,82 @@ static void quant_row(const float* x, uint32_t d, float slope, int32_t offset, u
   }
 }
 
-/* beam_search_rerank (beamSearch.h:529-597) for a float Euclidian index with
- * one-byte quantized points, no filtering: the beam search runs on the
- * quantized points and query; the first min(k * rerank_factor, |frontier|)
- * frontier entries are re-scored with the float distance, sorted by
- * (distance, id), and the first k kept. Returns -2 if the frontier holds
- * fewer than k entries (the reference aborts). */
-int oracle_search_quantized(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
-                            const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
-                            double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids,
-                            float* out_dists, uint32_t* out_visited, uint32_t* out_cmps) {
-  float slope;
-  int32_t offset;
-  oracle_quant_params(n, d, base, &slope, &offset);
+/* Quantized_Mips_Point<8, true>::generate_parameters (mips_point.h:438-499):
+ * per point the minimum and maximum of its values (0.0 the starting point of
+ * both); trimmed: the minimum of rank (size_t)(1e-4 n) among the points'
+ * minima and the maximum of rank (size_t)((1 - 1e-4)(n - 1)) among their
+ * maxima; bound = max(max, -min); parameters(bound, d) (:303-308): scale =
+ * 127 / bound in float. */
+static int cmp_float(const void* a, const void* b) {
+  const float x = *(const float*)a, y = *(const float*)b;
+  return (x > y) - (x < y);
+}
+void oracle_quant_params_mips(uint32_t n, uint32_t d, const float* base, float* scale, float* bound) {
+  float* mins = (float*)malloc(sizeof(float) * (n ? n : 1));
+  float* maxs = (float*)malloc(sizeof(float) * (n ? n : 1));
+  for (uint32_t i = 0; i < n; i++) {
+    float mn = 0.0f, mx = 0.0f;
+    for (uint32_t j = 0; j < d; j++) {
+      const float x = base[(size_t)i * d + j];
+      if (x < mn) mn = x;
+      if (x > mx) mx = x;
+    }
+    mins[i] = mn;
+    maxs[i] = mx;
+  }
+  const double cutoff = .0001;
+  const size_t min_rank = (size_t)(cutoff * n);
+  const size_t max_rank = (size_t)((1.0 - cutoff) * (n - 1));
+  qsort(mins, n, sizeof(float), cmp_float);
+  qsort(maxs, n, sizeof(float), cmp_float);
+  const float mn = mins[min_rank], mx = maxs[max_rank];
+  const float b = mx > -mn ? mx : -mn;
+  *bound = b;
+  *scale = 127 / b;
+  free(mins);
+  free(maxs);
+}
+
+/* translate_point (mips_point.h:421-436): -127 below -bound, 127 above bound,
+ * else round(x * scale), as int8. */
+static void quant_row_mips(const float* x, uint32_t d, float scale, float bound, int8_t* out) {
+  for (uint32_t j = 0; j < d; j++) {
+    const float pj = x[j];
+    if (pj < -bound) out[j] = -127;
+    else if (pj > bound) out[j] = 127;
+    else out[j] = (int8_t)(int32_t)roundf(pj * scale);
+  }
+}
+
+/* beam_search_rerank (beamSearch.h:529-597) for a float index with one-byte
+ * quantized points, no filtering: the beam search runs on the quantized
+ * points and query (uint8 Euclidian for metric 0, int8 mips for metric 1);
+ * the first min(k * rerank_factor, |frontier|) frontier entries are re-scored
+ * with the float distance, sorted by (distance, id), and the first k kept.
+ * Returns -2 if the frontier holds fewer than k entries (the reference
+ * aborts). */
+int oracle_search_quantized(int metric, uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries,
+                            uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit,
+                            uint32_t degree_limit, double rerank_factor, double batch_factor, uint32_t start,
+                            uint32_t* out_ids, float* out_dists, uint32_t* out_visited, uint32_t* out_cmps) {
+  float slope = 1.0f, scale = 1.0f, bound = 1.0f;
+  int32_t offset = 0;
+  if (metric == 0) oracle_quant_params(n, d, base, &slope, &offset);
+  else oracle_quant_params_mips(n, d, base, &scale, &bound);
   uint8_t* qb = (uint8_t*)malloc((size_t)n * d);
-  for (uint32_t i = 0; i < n; i++) quant_row(base + (size_t)i * d, d, slope, offset, qb + (size_t)i * d);
-  pts_t QP8 = {0, 0, d, d, qb};
-  pts_t PF = {2, 0, d, 4 * (size_t)d, (const uint8_t*)base};
+  for (uint32_t i = 0; i < n; i++) {
+    if (metric == 0) quant_row(base + (size_t)i * d, d, slope, offset, qb + (size_t)i * d);
+    else quant_row_mips(base + (size_t)i * d, d, scale, bound, (int8_t*)(qb + (size_t)i * d));
+  }
+  pts_t QP8 = {metric == 0 ? 0 : 1, metric, d, d, qb};
+  pts_t PF = {2, metric, d, 4 * (size_t)d, (const uint8_t*)base};
   qparams_t QP = {k, L, degree_limit, limit, batch_factor, 0.0, 0.0, 0.0};
   uint8_t* qq = (uint8_t*)malloc(d);
   int rc = 0;
   for (uint32_t i = 0; i < nq && rc == 0; i++) {
     const float* q = queries + (size_t)i * d;
-    quant_row(q, d, slope, offset, qq);
+    if (metric == 0) quant_row(q, d, slope, offset, qq);
+    else quant_row_mips(q, d, scale, bound, (int8_t*)qq);
     bs_out_t o;
     if (beam_search_one(&QP8, graph, R, qq, EMPTY32, &start, 1, &QP, &o) != 0) { rc = -1; break; }
     if (o.frontier_n < k) rc = -2;

@@ -19,8 +19,10 @@
 //                    the tool's file is included with its main() renamed)
 //   ref_search_quantized beam_search_rerank() over one-byte scalar-quantized
 //                    points with a float re-rank, as GraphIndex::search_dispatch
-//                    calls it for float Euclidian indexes (beamSearch.h:529-597,
-//                    python/graph_index.cpp:140-160, euclidian_point.h:186-240)
+//                    calls it for float indexes (beamSearch.h:529-597,
+//                    python/graph_index.cpp:140-185): Euclidian_Point<uint8_t>
+//                    (euclidian_point.h:186-240) for Euclidian, and
+//                    Quantized_Mips_Point<8, true> (mips_point.h:293-499) for mips
 //   ref_check_recall checkRecall() itself on a groundtruth .ibin file
 //                    (check_nn_recall.h:17-128): recall with the groundtruth's
 //                    ties at the k-th distance, QPS, mean visited / comparisons
@@ -30,6 +32,7 @@
 //                    a reference run needs no other library
 //   ref_num_workers  threads used by parallel_for
 #include <cmath>
+#include <type_traits>
 #include <cstdint>
 #include <cstring>
 #include <chrono>
@@ -300,25 +303,32 @@ int range_gt_t(uint32_t n, uint32_t d, const void* base, uint32_t nq, const void
   return total > cap ? 1 : 0;
 }
 
+// Euclidian: Euclidian_Point<uint8_t> (slope, offset); mips: Quantized_Mips_Point<8, true>, the
+// quantizer GraphIndex uses for float mips indexes (python/graph_index.cpp:69), whose parameters are
+// reported as (scale, 0).
+template <typename Point, typename QPoint>
 int quantized_t(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
                 const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
                 double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids, float* out_dists,
                 uint32_t* out_visited, uint32_t* out_cmps, float* out_slope, int32_t* out_offset, double* seconds) {
-  using Point = Euclidian_Point<float>;
-  using QPoint = Euclidian_Point<uint8_t>;
   auto B = make_points<Point>(base, n, d);
   auto Q = make_points<Point>(queries, nq, d);
   auto G = make_graph(graph, n, R);
   PointRange<QPoint> QB(B);  // generate_parameters + translate_point per row
-  *out_slope = QB.params.slope;
-  *out_offset = QB.params.offset;
+  if constexpr (std::is_same_v<Point, Euclidian_Point<float>>) {
+    *out_slope = QB.params.slope;
+    *out_offset = QB.params.offset;
+  } else {
+    *out_slope = QB.params.scale;
+    *out_offset = 0;
+  }
   QueryParams QP((long)k, (long)L, (long)limit, (long)degree_limit, rerank_factor, batch_factor);
   stats<unsigned int> QS(nq);
   QS.clear();
   parlay::sequence<unsigned int> starts = {start};
   auto t0 = std::chrono::steady_clock::now();
   parlay::parallel_for(0, nq, [&](size_t i) {
-    std::vector<uint8_t> buf(d);
+    std::vector<uint8_t> buf(QB.params.num_bytes() + 16);
     QPoint::translate_point(buf.data(), Q[i], QB.params);
     QPoint qq(buf.data(), (long)i, QB.params);
     auto res = beam_search_rerank(Q[i], qq, qq, G, B, QB, QB, QS, starts, QP, true);
@@ -461,13 +471,18 @@ int ref_range_search(int dtype, int metric, uint32_t n, uint32_t d, const void* 
   return -1;
 }
 
-int ref_search_quantized(uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries, uint32_t R,
-                         const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit, uint32_t degree_limit,
-                         double rerank_factor, double batch_factor, uint32_t start, uint32_t* out_ids,
-                         float* out_dists, uint32_t* out_visited, uint32_t* out_cmps, float* out_slope,
-                         int32_t* out_offset, double* seconds) {
-  return quantized_t(n, d, base, nq, queries, R, graph, k, L, limit, degree_limit, rerank_factor, batch_factor, start,
-                     out_ids, out_dists, out_visited, out_cmps, out_slope, out_offset, seconds);
+int ref_search_quantized(int metric, uint32_t n, uint32_t d, const float* base, uint32_t nq, const float* queries,
+                         uint32_t R, const uint32_t* graph, uint32_t k, uint32_t L, uint64_t limit,
+                         uint32_t degree_limit, double rerank_factor, double batch_factor, uint32_t start,
+                         uint32_t* out_ids, float* out_dists, uint32_t* out_visited, uint32_t* out_cmps,
+                         float* out_slope, int32_t* out_offset, double* seconds) {
+  if (metric == 0)
+    return quantized_t<Euclidian_Point<float>, Euclidian_Point<uint8_t>>(
+        n, d, base, nq, queries, R, graph, k, L, limit, degree_limit, rerank_factor, batch_factor, start, out_ids,
+        out_dists, out_visited, out_cmps, out_slope, out_offset, seconds);
+  return quantized_t<Mips_Point<float>, Quantized_Mips_Point<8, true>>(
+      n, d, base, nq, queries, R, graph, k, L, limit, degree_limit, rerank_factor, batch_factor, start, out_ids,
+      out_dists, out_visited, out_cmps, out_slope, out_offset, seconds);
 }
 
 int ref_range_groundtruth(int dtype, int metric, uint32_t n, uint32_t d, const void* base, uint32_t nq,

@@ -73,8 +73,9 @@ struct pann_index {
   // quantized search: an internal uint8 Euclidean index over the one-byte
   // quantized points that reads this index's graph (quant.cu)
   pann_index* quant = nullptr;
-  float q_slope = 1.0f;
+  float q_slope = 1.0f;  // mips: the scale
   int32_t q_offset = 0;
+  float q_bound = 1.0f;  // mips: the trimmed bound
   bool graph_borrowed = false;  // d_graph belongs to another index
   uint32_t gt_fallbacks = 0;  // queries of the last float groundtruth recomputed by the plain kernel
   uint32_t starts_cached_n = 0;

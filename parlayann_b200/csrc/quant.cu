@@ -1,7 +1,9 @@
 // Quantized search with a float re-rank: the reference's own mixed-precision
-// search for float Euclidian indexes (GraphIndex::search_dispatch,
-// python/graph_index.cpp:140-160, which calls beam_search_rerank,
-// beamSearch.h:529-597).
+// search for float indexes (GraphIndex::search_dispatch,
+// python/graph_index.cpp:140-185, which calls beam_search_rerank,
+// beamSearch.h:529-597). Euclidian indexes quantize as Euclidian_Point<uint8_t>
+// (below); mips indexes as Quantized_Mips_Point<8, true> into an int8 mips
+// index (set_quantized_mips).
 //
 //   pann_index_set_quantized: one-byte scalar quantization of the points as
 //     PointRange<Euclidian_Point<uint8_t>>(Points) computes it
@@ -81,6 +83,42 @@ __global__ void quant_rows_kernel(const uint8_t* __restrict__ src, uint64_t n, u
   }
 }
 
+// Quantized_Mips_Point<8, true> (mips_point.h:293-499), the quantizer the
+// reference's GraphIndex uses for float mips indexes: per point the minimum
+// and maximum of its values (0.0 the starting point of both), ...
+__global__ void quant_point_minmax_kernel(const uint8_t* __restrict__ points, uint64_t n, uint64_t stride, uint32_t d,
+                                          float* mins, float* maxs) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float* x = reinterpret_cast<const float*>(points + i * stride);
+    float mn = 0.0f, mx = 0.0f;
+    for (uint32_t j = 0; j < d; j++) {
+      mn = fminf(mn, x[j]);
+      mx = fmaxf(mx, x[j]);
+    }
+    mins[i] = mn;
+    maxs[i] = mx;
+  }
+}
+
+// ... and translate_point (:421-436): -127 below -bound, 127 above bound,
+// else round(x * scale), stored as int8 (zero padding past d).
+__global__ void quant_rows_mips_kernel(const uint8_t* __restrict__ src, uint64_t n, uint64_t sstride, uint32_t d,
+                                       float scale, float bound, uint8_t* out, uint64_t ostride) {
+  const uint64_t total = n * ostride;
+  for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = e / ostride;
+    const uint32_t j = (uint32_t)(e % ostride);
+    int8_t v = 0;
+    if (j < d) {
+      const float x = reinterpret_cast<const float*>(src + i * sstride)[j];
+      if (x < -bound) v = -127;
+      else if (x > bound) v = 127;
+      else v = (int8_t)(int32_t)roundf(__fmul_rn(x, scale));
+    }
+    out[e] = (uint8_t)v;
+  }
+}
+
 // One warp per query: float distances of the query's kp candidates (a
 // PAD-terminated frontier prefix), ranked by (distance, id); the first k are
 // written, PAD past the candidates. Shared memory per warp (quant_warp_bytes,
@@ -89,6 +127,7 @@ __global__ void quant_rows_kernel(const uint8_t* __restrict__ src, uint64_t n, u
 __host__ __device__ inline uint64_t quant_warp_bytes(uint64_t stride, uint32_t kp) {
   return stride + ((8ull * kp + 15) & ~15ull);
 }
+template <int MT>
 __global__ void __launch_bounds__(128) quant_rerank_kernel(const uint8_t* __restrict__ points, uint64_t stride,
                                                            uint32_t d, uint32_t nchunks,
                                                            const uint8_t* __restrict__ queries, uint32_t nq,
@@ -101,7 +140,7 @@ __global__ void __launch_bounds__(128) quant_rerank_kernel(const uint8_t* __rest
   uint32_t* ci = reinterpret_cast<uint32_t*>(cd + kp);
   const uint32_t qi = blockIdx.x * (blockDim.x >> 5) + warp;
   if (qi >= nq) return;
-  stage_query<DT_F32, MT_L2>(qs, queries + (uint64_t)qi * stride, (int)nchunks, lane);
+  stage_query<DT_F32, MT>(qs, queries + (uint64_t)qi * stride, (int)nchunks, lane);
   const uint32_t* c = cand + (uint64_t)qi * kp;
   uint32_t nv = 0;  // the valid entries are a prefix
   for (uint32_t b = 0; b < kp; b += 32) {
@@ -112,7 +151,7 @@ __global__ void __launch_bounds__(128) quant_rerank_kernel(const uint8_t* __rest
   for (uint32_t j = lane; j < nv; j += 32) {
     const uint32_t id = c[j];
     ci[j] = id;
-    cd[j] = point_dist<DT_F32, MT_L2>(points + (uint64_t)id * stride, qs, (int)d, (int)nchunks, 0);
+    cd[j] = point_dist<DT_F32, MT>(points + (uint64_t)id * stride, qs, (int)d, (int)nchunks, 0);
   }
   __syncwarp();
   for (uint32_t j = lane; j < nv; j += 32) {
@@ -136,10 +175,58 @@ __global__ void __launch_bounds__(128) quant_rerank_kernel(const uint8_t* __rest
 
 using namespace pann;
 
+// The mips quantization (Quantized_Mips_Point<8, true>): trimmed bound from the
+// points' minima and maxima, scale = 127 / bound, int8 rows in an internal
+// int8 mips index sharing the graph.
+static int set_quantized_mips(pann_index* idx) {
+  cudaStream_t st = idx->stream;
+  const uint64_t n = idx->n;
+  PANN_CUDA(idx->tmp.ensure(8ull * std::max<uint64_t>(n, 1)));
+  float* mins = idx->tmp.as<float>();
+  float* maxs = mins + n;
+  quant_point_minmax_kernel<<<(int)std::min<uint64_t>((n + 255) / 256, 65535ull), 256, 0, st>>>(
+      idx->d_points, n, idx->stride, idx->d, mins, maxs);
+  PANN_CUDA(cudaGetLastError());
+  std::vector<float> hmin(n), hmax(n);
+  PANN_CUDA(cudaMemcpyAsync(hmin.data(), mins, 4ull * n, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaMemcpyAsync(hmax.data(), maxs, 4ull * n, cudaMemcpyDeviceToHost, st));
+  PANN_CUDA(cudaStreamSynchronize(st));
+  // kth_smallest_copy of the minima at rank cutoff n and of the maxima at (1 - cutoff)(n - 1) (:458-465)
+  const double cutoff = .0001;
+  const size_t min_rank = (size_t)(cutoff * (double)n);
+  const size_t max_rank = (size_t)((1.0 - cutoff) * (double)(n - 1));
+  std::nth_element(hmin.begin(), hmin.begin() + min_rank, hmin.end());
+  std::nth_element(hmax.begin(), hmax.begin() + max_rank, hmax.end());
+  const float min_val = hmin[min_rank], max_val = hmax[max_rank];
+  const float bound = std::max(max_val, -min_val);
+  const float scale = 127 / bound;  // parameters(max_val, dims): (range / 2) / max_val, :306-307
+  if (!idx->quant) {
+    pann_index* qi = nullptr;
+    int rc = pann_index_create(&qi, PANN_I8, PANN_MIPS, idx->n, idx->d, idx->R);
+    if (rc) return rc;
+    cudaFree(qi->d_graph);  // the quantized index reads this index's graph
+    qi->d_graph = idx->d_graph;
+    qi->graph_borrowed = true;
+    idx->quant = qi;
+  }
+  pann_index* qi = idx->quant;
+  const uint64_t total = qi->n * qi->stride;
+  const int qb = (int)std::min<uint64_t>((total + 255) / 256, 65535ull * 8);
+  quant_rows_mips_kernel<<<qb, 256, 0, st>>>(idx->d_points, idx->n, idx->stride, idx->d, scale, bound, qi->d_points,
+                                             qi->stride);
+  PANN_CUDA(cudaGetLastError());
+  PANN_CUDA(cudaStreamSynchronize(st));
+  qi->points_set = true;
+  idx->q_slope = scale;
+  idx->q_offset = 0;
+  idx->q_bound = bound;
+  return PANN_OK;
+}
+
 extern "C" int pann_index_set_quantized(pann_index* idx) {
   if (!idx || !idx->points_set) return fail(PANN_EINVAL, "index has no points");
-  if (idx->dtype != PANN_F32 || idx->metric != PANN_L2)
-    return fail(PANN_EINVAL, "the quantized search covers float Euclidian indexes");
+  if (idx->dtype != PANN_F32) return fail(PANN_EINVAL, "the quantized search covers float indexes");
+  if (idx->metric == PANN_MIPS) return set_quantized_mips(idx);
   cudaStream_t st = idx->stream;
   const int blocks = 2 * idx->sm_count;
   PANN_CUDA(idx->tmp.ensure(12ull * blocks));
@@ -236,8 +323,12 @@ extern "C" int pann_search_quantized(pann_index* idx, const void* queries, uint3
   {  // the queries, translated as the points were
     const uint64_t total = (uint64_t)nq * qi->stride;
     const int qb = (int)std::min<uint64_t>((total + 255) / 256, 65535ull * 8);
-    quant_rows_kernel<<<qb, 256, 0, st>>>(idx->q.as<uint8_t>(), nq, idx->stride, idx->d, idx->q_slope, idx->q_offset,
-                                          qi->q.as<uint8_t>(), qi->stride);
+    if (idx->metric == PANN_MIPS)
+      quant_rows_mips_kernel<<<qb, 256, 0, st>>>(idx->q.as<uint8_t>(), nq, idx->stride, idx->d, idx->q_slope,
+                                                 idx->q_bound, qi->q.as<uint8_t>(), qi->stride);
+    else
+      quant_rows_kernel<<<qb, 256, 0, st>>>(idx->q.as<uint8_t>(), nq, idx->stride, idx->d, idx->q_slope,
+                                            idx->q_offset, qi->q.as<uint8_t>(), qi->stride);
     PANN_CUDA(cudaGetLastError());
   }
   rc = run_search(qi, plan, qi->q.as<uint8_t>(), nullptr, nq, qi->starts.as<uint32_t>(), qi->ids.as<uint32_t>(),
@@ -247,7 +338,7 @@ extern "C" int pann_search_quantized(pann_index* idx, const void* queries, uint3
   uint32_t* short_count = idx->counters.as<uint32_t>();
   PANN_CUDA(cudaMemsetAsync(short_count, 0, 4, st));
   {
-    auto kern = quant_rerank_kernel;
+    auto kern = idx->metric == PANN_MIPS ? quant_rerank_kernel<MT_IP> : quant_rerank_kernel<MT_L2>;
     PANN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max()));
     kern<<<(nq + 3) / 4, 128, smem, st>>>(idx->d_points, idx->stride, idx->d, idx->nchunks, idx->q.as<uint8_t>(), nq,
                                           qi->ids.as<uint32_t>(), kp, qp->k, idx->ids.as<uint32_t>(),

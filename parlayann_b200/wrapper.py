@@ -28,9 +28,9 @@ python/graph_index.cpp, python/builder.cpp) over this library.
   graph's, and the start point is 0 as in search_dispatch. `quant=True` on a
   float Euclidian index runs the reference's own quantized search
   (pann_search_quantized: one-byte points, float re-rank of min(100 k, beam)
-  entries, as search_dispatch does); on a float mips index, whose reference
-  quantizer (Quantized_Mips_Point) is not built, it runs the precision form
-  (FP8 tile search with an exact float re-rank) instead.
+  entries, as search_dispatch does); on a float mips index it runs the same
+  search over Quantized_Mips_Point<8, true> rows, with the query normalised
+  first as search_dispatch does.
 """
 from __future__ import annotations
 
@@ -38,7 +38,7 @@ from typing import NamedTuple
 
 import numpy as np
 
-from . import L2, MIPS, PREC_F32, PREC_FP8, Index, recall_with_ties
+from . import L2, MIPS, PREC_F32, Index, recall_with_ties
 
 _DTYPE = {"float": np.float32, "uint8": np.uint8, "int8": np.int8}
 _METRIC = {"Euclidian": L2, "mips": MIPS}
@@ -187,17 +187,11 @@ class GraphIndex:
         if quant and self.metric == MIPS and queries.dtype == np.float32:
             queries = _normalize(queries)   # search_dispatch normalises the query on its quantized path only
         limit = None if visit_limit is None or visit_limit <= 0 else int(visit_limit)
-        if quant and self.points.dtype == np.float32 and self.metric == L2:
+        if quant and self.points.dtype == np.float32:
             if not self._quantized:
                 self.index.set_quantized()
                 self._quantized = True
             r = self.index.search_quantized(queries, int(knn), int(beam_width), limit=limit)
-        elif quant and self.points.dtype == np.float32:
-            if not self._lowprec:
-                self.index.set_precision(PREC_FP8)
-                self._lowprec = True
-            r = self.index.search(queries, int(knn), int(beam_width), limit=limit, precision=PREC_FP8, parents=2,
-                                  allow_short=True)
         else:
             r = self.index.search(queries, int(knn), int(beam_width), limit=limit, precision=PREC_F32,
                                   allow_short=True)

@@ -219,6 +219,27 @@ def test_oracle_quantized_search_matches_golden(path, lib_built):
 
 
 @needs_ref
+@pytest.mark.parametrize("seed,n,d,R,L,k,rf", [(0, 3000, 16, 20, 40, 10, 100.0), (1, 3000, 24, 24, 30, 5, 2.0),
+                                               (2, 20000, 32, 24, 40, 10, 100.0)])
+def test_oracle_mips_quantized_search_matches_reference(seed, n, d, R, L, k, rf, lib_built):
+    """The mips quantizer GraphIndex uses for float mips indexes (Quantized_Mips_Point<8, true>,
+    mips_point.h:293-499; python/graph_index.cpp:69,167-185) on L2-normalised points: trimmed bound,
+    scale, int8 rows, the quantized search and the float re-rank."""
+    rng = np.random.default_rng(170 + seed)
+    base = rng.standard_normal((n, d)).astype(np.float32)
+    base /= np.linalg.norm(base, axis=1, keepdims=True).astype(np.float32)
+    q = rng.standard_normal((40, d)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True).astype(np.float32)
+    g = O.random_graph(n, R, 180 + seed)
+    a = O.search_quantized("oracle", base, q, g, k, L, rerank_factor=rf, metric=1)
+    b = O.search_quantized("ref", base, q, g, k, L, rerank_factor=rf, metric=1)
+    assert a["slope"] == b["slope"] and b["offset"] == 0
+    for key in ("ids", "visited", "cmps"):
+        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+    np.testing.assert_array_equal(a["dists"].view(np.uint32), b["dists"].view(np.uint32))
+
+
+@needs_ref
 def test_oracle_quantized_search_matches_reference(lib_built):
     for seed, (n, d, R, L, k, rf) in enumerate([(3000, 16, 20, 40, 10, 100.0), (3000, 24, 24, 30, 5, 2.0)]):
         base = random_points(np.float32, n, d, 140 + seed)

@@ -123,6 +123,30 @@ def test_quantized_search_matches_oracle(rf, k, L, lib_built):
     idx.close()
 
 
+@pytest.mark.parametrize("rf,k,L", [(100.0, 10, 40), (2.0, 5, 30), (1.0, 8, 8)])
+def test_mips_quantized_search_matches_oracle(rf, k, L, lib_built):
+    """The mips quantized search (Quantized_Mips_Point<8, true> rows in an int8 mips index, float
+    re-rank) against the oracle restatement pinned to the reference: the scale, ids, float distances
+    bit for bit, visited and comparison counts, on L2-normalised points and queries."""
+    rng = np.random.default_rng(321)
+    base = rng.standard_normal((12000, 20)).astype(np.float32)
+    base /= np.linalg.norm(base, axis=1, keepdims=True).astype(np.float32)
+    q = rng.standard_normal((400, 20)).astype(np.float32)
+    q /= np.linalg.norm(q, axis=1, keepdims=True).astype(np.float32)
+    g = O.random_graph(12000, 24, 323)
+    idx = P.Index(base, 24, P.MIPS)
+    idx.set_graph(g)
+    idx.set_quantized()
+    r = idx.search_quantized(q, k, L, rerank_factor=rf)
+    o = O.search_quantized("oracle", base, q, g, k, L, rerank_factor=rf, metric=1)
+    assert idx.quant_params() == (o["slope"], 0)
+    np.testing.assert_array_equal(r.ids, o["ids"])
+    np.testing.assert_array_equal(r.dists.view(np.uint32), o["dists"].view(np.uint32))
+    np.testing.assert_array_equal(r.visited, o["visited"])
+    np.testing.assert_array_equal(r.cmps, o["cmps"])
+    idx.close()
+
+
 def test_quantized_search_integer_valued_points_and_errors(lib_built):
     rng = np.random.default_rng(311)
     base = rng.integers(0, 256, (5000, 16)).astype(np.float32)
@@ -140,9 +164,9 @@ def test_quantized_search_integer_valued_points_and_errors(lib_built):
     with pytest.raises(P.PannError):
         idx.search_quantized(q, 5, 20, rerank_factor=0.5)   # fewer re-ranked entries than k
     idx.close()
-    mips = P.Index(base, 16, P.MIPS)
+    u8 = P.Index(base.astype(np.uint8), 16)
     with pytest.raises(P.PannError):
-        mips.set_quantized()                                # float Euclidean indexes only
+        u8.set_quantized()                                  # float indexes only
     mips.close()
 
 
