@@ -188,6 +188,10 @@ int arena_layout(const pann_index* idx, const pann_query_params* bounds, uint32_
   y->plan.Ccap = (uint32_t)std::floor(y->plan.bf * (double)y->plan.L) + std::min(y->plan.dl, idx->R) + 1;
   rc = size_tiers(idx, y->plan, nq, prec, 0, 0, &y->z);
   if (rc) return rc;
+  // batches that overlap on the device: the emulation tier keeps its tables in
+  // global memory (the shared-memory tier's blocks each need a whole SM and
+  // would wait for the other batches' blocks to leave one)
+  y->z.emu_smem = false;
   const size_t k = y->plan.k;
   size_t o = 0;
   auto take = [&](size_t bytes) {

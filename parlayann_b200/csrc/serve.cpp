@@ -142,18 +142,30 @@ size_t batch_bytes(const pann_server* s, uint32_t nq, uint32_t kmax, uint32_t Lm
 // Launches the waiting k-NN requests that fit into a free slot (s->mu held on
 // entry; released during the launch). Requests are taken in arrival order
 // while the batch stays within max_batch_queries and its scratch within the
-// slot's arena. Returns true if something was launched.
+// slot's arena (see below for the beam rule). Returns true if something was
+// launched.
 bool launch(pann_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
   if (s->knn_q.empty()) return false;
   uint32_t nq = 0, kmax = 0, Lmax = 0;
   size_t used = 0;
-  while (!s->knn_q.empty()) {
-    const Request* r = s->knn_q.front();
+  // The oldest request always goes in; later ones join while the batch fits,
+  // taken in arrival order among those whose beam is within 5/4 of the oldest
+  // one's (a batch's shared-memory state is sized for its largest beam, so a
+  // long-beam request would slow every short-beam query beside it); the
+  // requests passed over keep their place and lead the next batch.
+  const uint32_t beam0 = s->knn_q.front()->beam;
+  size_t scanned = 0;
+  for (auto it = s->knn_q.begin(); it != s->knn_q.end() && scanned < 512; scanned++) {
+    const Request* r = *it;
+    if (!sl.reqs.empty() && 4ull * r->beam > 5ull * beam0) {
+      ++it;
+      continue;
+    }
     const uint32_t n2 = nq + r->nq, k2 = std::max(kmax, r->k), L2 = std::max(Lmax, r->beam);
     if (n2 > s->opt.max_batch_queries) break;
     const size_t need = batch_bytes(s, n2, k2, L2);
     if (need > s->scratch) break;
-    s->knn_q.pop_front();
+    it = s->knn_q.erase(it);
     sl.reqs.push_back(const_cast<Request*>(r));
     nq = n2;
     kmax = k2;

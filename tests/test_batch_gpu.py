@@ -104,8 +104,7 @@ def test_batch_autotune_and_fixed_shapes(lib_built):
     q = random_points(np.uint8, 2000, 32, 23)
     k, beam = uneven_shapes(len(q), 24, ks=(1, 10, 40))
     o = per_query_oracle(base, q, g, k, beam)
-    for opts in (dict(autotune=True), dict(seen_slots=512, warps_per_block=2), dict(use_graph=False),
-                 dict(cta_per_query=True)):
+    for opts in (dict(autotune=True), dict(seen_slots=512, warps_per_block=2), dict(use_graph=False)):
         b = idx.batch(len(q), int(k.max()), int(beam.max()), **opts)
         check(b.run(q, k, beam), o, str(opts))
         cfg = b.config()
@@ -174,9 +173,10 @@ def test_batch_cta_per_query_with_hashset_growth(lib_built):
     idx.set_graph(g)
     q = random_points(np.uint8, 300, 8, 2)
     rng = np.random.default_rng(5)
-    beam = rng.choice(np.array([12, 24, 40, 50, 64], np.uint32), len(q)).astype(np.uint32)
+    # beams up to 50: the emulated tables (4 + 2 times 2^ceil(log2(2 (10 + 50) 64)) slots) fit in shared memory
+    beam = rng.choice(np.array([12, 24, 40, 50], np.uint32), len(q)).astype(np.uint32)
     k = np.minimum(beam, 10).astype(np.uint32)
-    b = idx.batch(len(q), 10, 64, batch_factor=1.0, cta_per_query=True)
+    b = idx.batch(len(q), 10, 50, batch_factor=1.0, cta_per_query=True)
     o = per_query_oracle(base, q, g, k, beam, batch_factor=1.0)
     assert (o["hash_grew"] > 0).sum() > 0
     check(b.run(q, k, beam), o, "cta")
@@ -200,4 +200,14 @@ def test_batch_tile_autotune_keeps_answers(lib_built):
     np.testing.assert_array_equal(r.dists[:, :10].view(np.uint32), plain.dists.view(np.uint32))
     assert b.config()["tile_rows"] > 0
     b.close()
+    idx.close()
+
+
+def test_batch_cta_per_query_refused_when_tables_do_not_fit(lib_built):
+    base = random_points(np.uint8, 4000, 8, 6)
+    idx = P.Index(base, 64)
+    idx.set_graph(O.random_graph(4000, 64, 7, min_deg=60))
+    with pytest.raises(P.PannError) as e:
+        idx.batch(10, 10, 200, cta_per_query=True)
+    assert "CTA per query" in str(e.value)
     idx.close()
