@@ -178,6 +178,118 @@ __global__ void __launch_bounds__(128) greedy_prune_kernel(const uint8_t* __rest
   }
 }
 
+// Distance of the row at `row` (shared or global memory: generic loads) to the
+// point staged at qs, with point_dist's arithmetic (common.cuh).
+template <int DT, int MT>
+__device__ __forceinline__ float row_dist_generic(const uint8_t* row, const uint8_t* qs, int nchunks, int32_t qq) {
+  if (DT == DT_F32) {
+    const float4* r = reinterpret_cast<const float4*>(row);
+    const float4* q = reinterpret_cast<const float4*>(qs);
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < nchunks; c0 += ROW_CHUNKS) {
+      float4 b[ROW_CHUNKS];
+#pragma unroll
+      for (int c = 0; c < ROW_CHUNKS; c++)
+        if (c0 + c < nchunks) b[c] = r[c0 + c];
+#pragma unroll
+      for (int c = 0; c < ROW_CHUNKS; c++)
+        if (c0 + c < nchunks) acc = f32_chunk<MT>(acc, b[c], q[c0 + c]);
+    }
+    return MT == MT_L2 ? acc : -acc;
+  } else {
+    const uint4* r = reinterpret_cast<const uint4*>(row);
+    const uint4* q = reinterpret_cast<const uint4*>(qs);
+    int32_t pq = 0, pp = 0;
+    for (int c = 0; c < nchunks; c++) int_chunk<DT, MT>(r[c], q[c], pq, pp);
+    return int_result<MT>(qq, pq, pp);
+  }
+}
+
+// The greedy part of robustPrune as greedy_prune_kernel computes it, with one
+// block of 128 threads per job and the candidates' rows staged in shared
+// memory (the first `cap_rows` of the segment; later ones are read from
+// global memory): each selection is one pass of the block over the live
+// candidates after it, every distance from shared memory, instead of a
+// warp's dependent global loads. Same answers: the same candidates, the same
+// order of selections, the same float / integer distance and the alpha test
+// in double.
+template <int DT, int MT>
+__global__ void __launch_bounds__(128) greedy_prune_block_kernel(const uint8_t* __restrict__ points, uint64_t stride,
+                                                                 int nchunks, uint32_t* graph, uint32_t R,
+                                                                 uint32_t njobs, const uint32_t* __restrict__ pts,
+                                                                 const uint32_t* __restrict__ seg_begin,
+                                                                 const uint32_t* __restrict__ seg_end, uint64_t* keys,
+                                                                 double alpha, uint32_t cap_rows,
+                                                                 unsigned long long* dist_cmps) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint8_t* qs = smem;                     // p*
+  uint8_t* rows = smem + stride;          // cap_rows staged candidate rows
+  __shared__ int s_found;
+  __shared__ unsigned long long s_cmps;
+  for (uint32_t job = blockIdx.x; job < njobs; job += gridDim.x) {
+    const uint32_t p = pts[job];
+    uint64_t* K = keys + seg_begin[job];
+    const uint32_t m = seg_end[job] - seg_begin[job];
+    const uint32_t staged = m < cap_rows ? m : cap_rows;
+    // unique by id (index.h:86-88), and the rows of the first `staged` candidates
+    for (uint32_t i = tid; i < m; i += 128)
+      if (i > 0 && key_id(K[i]) == key_id(K[i - 1])) K[i] |= PANN_VFLAG;
+    for (uint32_t x = tid; x < staged * (uint32_t)nchunks; x += 128) {
+      const uint32_t r = x / nchunks, c = x - r * nchunks;
+      reinterpret_cast<uint4*>(rows + (size_t)r * stride)[c] =
+          __ldg(reinterpret_cast<const uint4*>(points + (uint64_t)key_id(K[r]) * stride) + c);
+    }
+    if (tid == 0) s_cmps = 0;
+    __syncthreads();
+    uint32_t nsel = 0, idx = 0;
+    uint32_t* row = graph + (uint64_t)p * R;
+    while (nsel < R && idx < m) {
+      if (warp == 0) {
+        int found = -1;
+        for (uint32_t b = idx; b < m && found < 0; b += 32) {
+          const uint32_t i = b + lane;
+          const bool live = i < m && !(K[i] & PANN_VFLAG);
+          const unsigned msk = __ballot_sync(0xFFFFFFFFu, live);
+          if (msk) found = (int)(b + __ffs(msk) - 1);
+        }
+        if (lane == 0) s_found = found;
+      }
+      __syncthreads();
+      const int found = s_found;
+      if (found < 0) break;
+      const uint32_t pstar = key_id(K[found]);
+      idx = (uint32_t)found + 1;
+      if (pstar == p) {  // :99-101
+        __syncthreads();
+        continue;
+      }
+      if (tid == 0) row[nsel] = pstar;
+      nsel++;
+      const uint8_t* src = (uint32_t)found < staged ? rows + (size_t)found * stride : points + (uint64_t)pstar * stride;
+      for (int c = tid; c < nchunks; c += 128) reinterpret_cast<uint4*>(qs)[c] = reinterpret_cast<const uint4*>(src)[c];
+      __syncthreads();
+      int32_t qq = 0;
+      if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);
+      uint32_t my_cmps = 0;
+      for (uint32_t i = idx + tid; i < m; i += 128) {
+        const uint64_t k = K[i];
+        if (k & PANN_VFLAG) continue;
+        my_cmps++;
+        const uint8_t* r = i < staged ? rows + (size_t)i * stride : points + (uint64_t)key_id(k) * stride;
+        const float dsp = row_dist_generic<DT, MT>(r, qs, nchunks, qq);
+        if (__dmul_rn(alpha, (double)dsp) <= (double)key_dist(k)) K[i] = k | PANN_VFLAG;
+      }
+      for (int o = 16; o; o >>= 1) my_cmps += __shfl_xor_sync(0xFFFFFFFFu, my_cmps, o);
+      if (lane == 0 && my_cmps) atomicAdd(&s_cmps, (unsigned long long)my_cmps);
+      __syncthreads();
+    }
+    for (uint32_t j = nsel + tid; j < R; j += 128) row[j] = PANN_PAD;
+    __syncthreads();
+    if (tid == 0) atomicAdd(dist_cmps, s_cmps);
+  }
+}
+
 // Reverse-edge pairs: key = new neighbour (PAD for empty slots), value = inserted point.
 __global__ void reverse_pairs_kernel(const uint32_t* __restrict__ graph, uint32_t R, const uint32_t* __restrict__ pts,
                                      uint32_t B, uint32_t* kout, uint32_t* vout) {
@@ -312,6 +424,34 @@ static void batch_schedule(uint64_t n, uint64_t m, std::vector<uint64_t>& fl, st
     ce.push_back(c);
     inc++;
   }
+}
+
+// robustPrune's greedy part for njobs segments: the block kernel with up to
+// 64 KB of staged candidate rows per block (PANN_PRUNE_WARP=1 selects the
+// warp-per-job kernel instead).
+template <int DT, int MT>
+static cudaError_t launch_greedy(const pann_index* idx, uint32_t njobs, const uint32_t* pts, const uint32_t* sb,
+                                 const uint32_t* se, uint64_t* keys, double alpha, unsigned long long* cmps,
+                                 cudaStream_t st) {
+  if (njobs == 0) return cudaSuccess;
+  static const bool warp_kernel = std::getenv("PANN_PRUNE_WARP") != nullptr;
+  if (warp_kernel) {
+    const int wpb = 4;
+    const int blocks = (int)std::min<uint32_t>((njobs + wpb - 1) / wpb, 65535);
+    greedy_prune_kernel<DT, MT><<<blocks, 32 * wpb, wpb * idx->stride, st>>>(
+        idx->d_points, idx->stride, (int)idx->d, (int)idx->nchunks, idx->d_graph, idx->R, njobs, pts, sb, se, keys,
+        alpha, cmps);
+    return cudaGetLastError();
+  }
+  const uint32_t cap_rows = (uint32_t)std::max<uint64_t>(1, (64ull << 10) / idx->stride);
+  const size_t smem = idx->stride * (1 + (size_t)cap_rows);
+  auto k = greedy_prune_block_kernel<DT, MT>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
+  if (e != cudaSuccess) return e;
+  const int blocks = (int)std::min<uint32_t>(njobs, 2u * 65535u);
+  k<<<blocks, 128, smem, st>>>(idx->d_points, idx->stride, (int)idx->nchunks, idx->d_graph, idx->R, njobs, pts, sb, se,
+                               keys, alpha, cap_rows, cmps);
+  return cudaGetLastError();
 }
 
 template <typename F>
@@ -559,11 +699,8 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
       }
       BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
         constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
-        int blocks = (int)std::min<uint32_t>((B + wpb - 1) / wpb, 65535);
-        greedy_prune_kernel<DT, MT><<<blocks, 32 * wpb, wpb * warp_smem, st>>>(
-            idx->d_points, stride, d, nch, idx->d_graph, R, B, pts, bb.seg_begin.as<uint32_t>(),
-            bb.seg_end.as<uint32_t>(), bb.seg_b.as<uint64_t>(), alpha, c64);
-        return cudaGetLastError();
+        return launch_greedy<DT, MT>(idx, B, pts, bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(),
+                                     bb.seg_b.as<uint64_t>(), alpha, c64, st);
       }));
       BCUDA(cudaEventRecord(eb, st));
       seg_len_sum_kernel<<<64, 256, 0, st>>>(bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(), B, c64 + 4);
@@ -638,11 +775,8 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
         }
         BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
           constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
-          int blocks = (int)std::min<uint32_t>((njobs + wpb - 1) / wpb, 65535);
-          greedy_prune_kernel<DT, MT><<<blocks, 32 * wpb, wpb * warp_smem, st>>>(
-              idx->d_points, stride, d, nch, idx->d_graph, R, njobs, bb.jobs.as<uint32_t>(),
-              bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(), bb.seg_b.as<uint64_t>(), alpha, c64);
-          return cudaGetLastError();
+          return launch_greedy<DT, MT>(idx, njobs, bb.jobs.as<uint32_t>(), bb.seg_begin.as<uint32_t>(),
+                                       bb.seg_end.as<uint32_t>(), bb.seg_b.as<uint64_t>(), alpha, c64, st);
         }));
       }
       BCUDA(cudaEventRecord(ec, st));
