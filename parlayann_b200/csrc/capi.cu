@@ -457,7 +457,8 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
       e.overflow_rec = b.ovf_rec;
       e.overflow_count = cnt + 8;
       e.job_rec = nullptr;
-      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, c, e, idx->sm_count, z.emu_smem_need, st));
+      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, c, e, (int)std::min<uint64_t>(idx->sm_count, a.nq),
+                                     z.emu_smem_need, st));
       EmuArgs e2 = e;
       e2.gA = b.ge2;
       e2.gB = e2.gA + (size_t)z.e2_slots * z.capA;
@@ -519,7 +520,10 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
       t.job_list = b.emu;
       t.njobs_dev = cnt + 6;
       t.job_counter = cnt + 5;
-      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, t, e, idx->sm_count, z.emu_smem_need, st));
+      // no more blocks than queries: each needs most of an SM's shared memory,
+      // so a small search beside other work on the device asks for few SMs
+      PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, t, e, (int)std::min<uint64_t>(idx->sm_count, a.nq),
+                                     z.emu_smem_need, st));
       glist = b.ovf;
       grec = b.ovf_rec;
       gcount = cnt + 8;

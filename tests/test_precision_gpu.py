@@ -167,7 +167,7 @@ def test_quantized_search_integer_valued_points_and_errors(lib_built):
     u8 = P.Index(base.astype(np.uint8), 16)
     with pytest.raises(P.PannError):
         u8.set_quantized()                                  # float indexes only
-    mips.close()
+    u8.close()
 
 
 def test_quantized_search_edge_cases(lib_built):
