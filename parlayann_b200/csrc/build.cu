@@ -443,10 +443,18 @@ static cudaError_t launch_greedy(const pann_index* idx, uint32_t njobs, const ui
         alpha, cmps);
     return cudaGetLastError();
   }
-  const uint32_t cap_rows = (uint32_t)std::max<uint64_t>(1, (64ull << 10) / idx->stride);
-  const size_t smem = idx->stride * (1 + (size_t)cap_rows);
   auto k = greedy_prune_block_kernel<DT, MT>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr_max());
+  // dynamic + static shared memory must stay within the opt-in limit; rows
+  // past the staged ones are read from global memory (cap_rows may be 0)
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, k);
+  if (e != cudaSuccess) return e;
+  const uint64_t limit = (uint64_t)smem_attr_max() - fa.sharedSizeBytes;
+  if (idx->stride > limit) return cudaErrorInvalidValue;
+  const uint32_t cap_rows =
+      (uint32_t)std::min<uint64_t>((64ull << 10) / idx->stride, (limit - idx->stride) / idx->stride);
+  const size_t smem = idx->stride * (1 + (size_t)cap_rows);
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int blocks = (int)std::min<uint32_t>(njobs, 2u * 65535u);
   k<<<blocks, 128, smem, st>>>(idx->d_points, idx->stride, (int)idx->nchunks, idx->d_graph, idx->R, njobs, pts, sb, se,
