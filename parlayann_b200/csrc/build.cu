@@ -267,7 +267,12 @@ __global__ void __launch_bounds__(128) greedy_prune_block_kernel(const uint8_t* 
       if (tid == 0) row[nsel] = pstar;
       nsel++;
       const uint8_t* src = (uint32_t)found < staged ? rows + (size_t)found * stride : points + (uint64_t)pstar * stride;
-      for (int c = tid; c < nchunks; c += 128) reinterpret_cast<uint4*>(qs)[c] = reinterpret_cast<const uint4*>(src)[c];
+      for (int c = tid; c < nchunks; c += 128) {
+        uint4 v = reinterpret_cast<const uint4*>(src)[c];
+        // staged as stage_query stages it: float32 Euclidean rows negated (f32_chunk forms x + (-q))
+        if (DT == DT_F32 && MT == MT_L2) v = make_uint4(v.x ^ 0x80000000u, v.y ^ 0x80000000u, v.z ^ 0x80000000u, v.w ^ 0x80000000u);
+        reinterpret_cast<uint4*>(qs)[c] = v;
+      }
       __syncthreads();
       int32_t qq = 0;
       if (DT != DT_F32 && MT == MT_L2) qq = sq_norm_int<DT>(reinterpret_cast<const uint4*>(qs), nchunks);
