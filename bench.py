@@ -638,7 +638,9 @@ def run_c3(dev, flush, args):
     gen_s = time.time() - t0
     stream = torch.cuda.current_stream(dev)
     idx = P.Index(base, W["R"])
+    print(f"c3: generated {n:,} x {d} uint8 in {gen_s:.1f} s; building", file=sys.stderr, flush=True)
     bst = idx.build(W["Lb"], W["alpha"], num_passes=W["passes"], batch_factor=W["bf"])
+    print(f"c3: built in {bst.seconds:.1f} s (device)", file=sys.stderr, flush=True)
     dq = torch.from_numpy(q).to(dev)
     out = {"workload": f"{n:,} x 128-d uint8 (1024-component mixture, seed 0), {nq:,} queries, Vamana R=64 L=128 "
                        "alpha=1.2 two passes (GPU build)",
