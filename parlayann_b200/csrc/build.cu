@@ -20,6 +20,7 @@
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -431,16 +432,33 @@ static void batch_schedule(uint64_t n, uint64_t m, std::vector<uint64_t>& fl, st
   }
 }
 
+// Which greedy kernel a prune step runs. The block kernel stages a job's
+// candidate rows in shared memory and pays off on the insertion prune's long
+// candidate lists; a re-prune's list (a full row plus its new reverse edges)
+// is short, and one warp per job keeps many more jobs resident. Selectable
+// with PANN_PRUNE_KERNEL=warp|block|auto (auto: block for insertions, warp
+// for re-prunes); every choice gives the same graph.
+static bool prune_block_kernel(bool reprune) {
+  static const int mode = [] {
+    const char* e = std::getenv("PANN_PRUNE_KERNEL");
+    if (!e) return 0;
+    if (!std::strcmp(e, "warp")) return 1;
+    if (!std::strcmp(e, "block")) return 2;
+    return 0;
+  }();
+  if (mode == 1) return false;
+  if (mode == 2) return true;
+  return !reprune;
+}
+
 // robustPrune's greedy part for njobs segments: the block kernel with up to
-// 64 KB of staged candidate rows per block (PANN_PRUNE_WARP=1 selects the
-// warp-per-job kernel instead).
+// 64 KB of staged candidate rows per block, or the warp-per-job kernel.
 template <int DT, int MT>
 static cudaError_t launch_greedy(const pann_index* idx, uint32_t njobs, const uint32_t* pts, const uint32_t* sb,
                                  const uint32_t* se, uint64_t* keys, double alpha, unsigned long long* cmps,
-                                 cudaStream_t st) {
+                                 bool reprune, cudaStream_t st) {
   if (njobs == 0) return cudaSuccess;
-  static const bool warp_kernel = std::getenv("PANN_PRUNE_WARP") != nullptr;
-  if (warp_kernel) {
+  if (!prune_block_kernel(reprune)) {
     const int wpb = 4;
     const int blocks = (int)std::min<uint32_t>((njobs + wpb - 1) / wpb, 65535);
     greedy_prune_kernel<DT, MT><<<blocks, 32 * wpb, wpb * idx->stride, st>>>(
@@ -713,7 +731,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
       BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
         constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
         return launch_greedy<DT, MT>(idx, B, pts, bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(),
-                                     bb.seg_b.as<uint64_t>(), alpha, c64, st);
+                                     bb.seg_b.as<uint64_t>(), alpha, c64, false, st);
       }));
       BCUDA(cudaEventRecord(eb, st));
       seg_len_sum_kernel<<<64, 256, 0, st>>>(bb.seg_begin.as<uint32_t>(), bb.seg_end.as<uint32_t>(), B, c64 + 4);
@@ -789,7 +807,7 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
         BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
           constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;
           return launch_greedy<DT, MT>(idx, njobs, bb.jobs.as<uint32_t>(), bb.seg_begin.as<uint32_t>(),
-                                       bb.seg_end.as<uint32_t>(), bb.seg_b.as<uint64_t>(), alpha, c64, st);
+                                       bb.seg_end.as<uint32_t>(), bb.seg_b.as<uint64_t>(), alpha, c64, true, st);
         }));
       }
       BCUDA(cudaEventRecord(ec, st));
