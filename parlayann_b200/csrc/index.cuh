@@ -1,6 +1,7 @@
 // Internal definition of the index handle behind the C ABI.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include "../../include/parlayann_b200.h"
@@ -35,6 +36,13 @@ struct DevBuf {
     cudaError_t e = cudaMalloc(&p, want);
     if (e == cudaSuccess) bytes = want;
     return e;
+  }
+  // as ensure, with room for growth (a buffer whose size follows the
+  // request mix is not reallocated, and the device not drained, each time
+  // a slightly larger request arrives)
+  cudaError_t ensure_grow(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    return ensure(std::max(want, bytes + bytes / 2));
   }
   void release() {
     if (p) cudaFree(p);

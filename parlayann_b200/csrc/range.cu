@@ -384,6 +384,18 @@ static cudaError_t launch_expand(int dtype, int metric, const RangeArgs& a, int 
   return cudaErrorInvalidValue;
 }
 
+// A small device-to-host read of a result the stream is still producing.
+// The stream is waited on first, so the copy into pageable memory (which
+// the driver completes synchronously) never waits on a long kernel itself:
+// other threads' launches on other streams (the serving loop's batches)
+// are not held up meanwhile.
+static cudaError_t to_host(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
+}
+
 static uint32_t ceil_log2(uint64_t x) {
   uint32_t b = 0;
   while ((1ull << b) < x) b++;
@@ -451,7 +463,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
   // ---- 2. classify; per-query metadata in one buffer
   // words: jobs nq | res_n nq | src nq | extra nq | rstatus nq | res_cmps nq | retry nq | res_off 2nq | offsets 2(nq+1) | counters 8
   const size_t meta_words = 11ull * nq + 2 + 8 + 8;
-  PANN_CUDA(idx->range_meta.ensure(4 * meta_words));
+  PANN_CUDA(idx->range_meta.ensure_grow(4 * meta_words));
   uint32_t* jobs = idx->range_meta.as<uint32_t>();
   uint32_t* res_n = jobs + nq;
   uint32_t* src = res_n + nq;
@@ -474,8 +486,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     PANN_CUDA(cudaGetLastError());
   }
   uint32_t h_njobs = 0;
-  PANN_CUDA(cudaMemcpyAsync(&h_njobs, cnt, 4, cudaMemcpyDeviceToHost, st));
-  PANN_CUDA(cudaStreamSynchronize(st));
+  PANN_CUDA(to_host(&h_njobs, cnt, 4, st));
 
   // ---- 3. expansions, in tiers of growing per-query room; the answers go to
   // a pool sized up front and grown (with a re-run) if they do not fit
@@ -496,7 +507,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     const size_t smem = idx->stride + 12ull * keybuf + 4ull * (CTL_WORDS + keybuf / 32 + 2);
     unsigned long long pool_cap = std::max<unsigned long long>(1ull << 22, 256ull * h_njobs);
     for (int attempt = 0; attempt < 3; attempt++) {
-      PANN_CUDA(idx->range_pool.ensure(4 * pool_cap));
+      PANN_CUDA(idx->range_pool.ensure_grow(4 * pool_cap));
       PANN_CUDA(cudaMemsetAsync(pool_count, 0, 8, st));
       const uint32_t* tier_jobs = jobs;
       const uint32_t* tier_n = cnt;
@@ -506,7 +517,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
         const size_t per_slot = 4ull * (2ull * cap + qcap);
         int slots = (int)std::max<uint64_t>(1, std::min<uint64_t>({(uint64_t)pending, (uint64_t)tiers[t].max_slots,
                                                                    (4ull << 30) / per_slot}));
-        PANN_CUDA(idx->range_tabs.ensure(per_slot * slots));
+        PANN_CUDA(idx->range_tabs.ensure_grow(per_slot * slots));
         PANN_CUDA(cudaMemsetAsync(cnt + 1, 0, 8, st));  // job counter, retry count
         RangeArgs ra{};
         ra.points = idx->d_points;
@@ -542,8 +553,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
         PANN_CUDA(launch_expand(idx->dtype, idx->metric, ra, slots, smem, st));
         if (t == 0) {
           uint32_t h_retry = 0;
-          PANN_CUDA(cudaMemcpyAsync(&h_retry, cnt + 2, 4, cudaMemcpyDeviceToHost, st));
-          PANN_CUDA(cudaStreamSynchronize(st));
+          PANN_CUDA(to_host(&h_retry, cnt + 2, 4, st));
           pending = h_retry;
           if (pending) {
             // the retry list becomes the next tier's job list
@@ -554,8 +564,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
         }
       }
       unsigned long long used = 0;
-      PANN_CUDA(cudaMemcpyAsync(&used, pool_count, 8, cudaMemcpyDeviceToHost, st));
-      PANN_CUDA(cudaStreamSynchronize(st));
+      PANN_CUDA(to_host(&used, pool_count, 8, st));
       if (used <= pool_cap) break;
       pool_cap = used;  // the answers did not fit: size the pool for them and run again
       PANN_CUDA(cudaMemsetAsync(rstat, 0, 4ull * nq, st));
@@ -564,6 +573,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
 
   // ---- 4. counts, offsets, the CSR gather
   std::vector<uint32_t> h_n(nq), h_src(nq), h_extra(nq), h_rst(nq), h_rcmps(nq), h_vis(nq), h_cmps(nq), h_st(nq);
+  PANN_CUDA(cudaStreamSynchronize(st));
   PANN_CUDA(cudaMemcpyAsync(h_n.data(), res_n, 4ull * nq, cudaMemcpyDeviceToHost, st));
   PANN_CUDA(cudaMemcpyAsync(h_src.data(), src, 4ull * nq, cudaMemcpyDeviceToHost, st));
   PANN_CUDA(cudaMemcpyAsync(h_extra.data(), extra, 4ull * nq, cudaMemcpyDeviceToHost, st));
@@ -589,7 +599,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
   out_offsets[nq] = total;
   if (total == 0) return PANN_OK;
   if (total <= ids_cap && !out_ids) return fail(PANN_EINVAL, "out_ids is NULL");
-  PANN_CUDA(idx->range_out.ensure(4 * total));
+  PANN_CUDA(idx->range_out.ensure_grow(4 * total));
   PANN_CUDA(cudaMemcpyAsync(d_offsets, out_offsets, 8ull * (nq + 1), cudaMemcpyHostToDevice, st));
   {
     int blocks = (int)std::min<uint64_t>((nq + 7) / 8, 8192);
@@ -604,6 +614,7 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
     return fail(PANN_EOVERFLOW, "range answers need " + std::to_string(total) + " ids; out_ids holds " +
                                     std::to_string(ids_cap) + " (pann_range_fetch copies them)");
   }
+  PANN_CUDA(cudaStreamSynchronize(st));
   PANN_CUDA(cudaMemcpyAsync(out_ids, idx->range_out.p, 4 * total, cudaMemcpyDeviceToHost, st));
   PANN_CUDA(cudaStreamSynchronize(st));
   return PANN_OK;

@@ -479,6 +479,27 @@ __global__ void __launch_bounds__(128) search_tile_kernel(SearchArgs a, uint32_t
   }
 }
 
+// Blocks of `threads` threads with `smem` bytes of dynamic shared memory that
+// one multiprocessor holds, from the kernel's registers and static shared
+// memory and the device's per-multiprocessor limits.
+static int resident_blocks(const void* k, int threads, size_t smem) {
+  cudaFuncAttributes fa{};
+  int dev = 0, smem_sm = 0, regs_sm = 0, thr_sm = 0, reserved = 0;
+  if (cudaFuncGetAttributes(&fa, k) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+    return 1;
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  const size_t per_block_smem = smem + fa.sharedSizeBytes + (size_t)reserved;
+  const int warps = (threads + 31) / 32;
+  const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocated per warp in units of 256
+  int by_smem = per_block_smem ? (int)((size_t)smem_sm / per_block_smem) : 32;
+  int by_regs = regs_warp ? regs_sm / (warps * regs_warp) : 32;
+  int by_thr = thr_sm / threads;
+  return std::max(1, std::min({by_smem, by_regs, by_thr}));
+}
+
 // Rows staged at once: the most that still gives the best occupancy among
 // CW, 3/4 CW and 1/2 CW (steps with more new candidates stage in rounds);
 // with tensor-core scoring, rounds of TC_ROWS rows.
@@ -507,7 +528,13 @@ static int launch_tile_t(const pann_index* idx, const SearchArgs& a, uint32_t W,
       smem = sm2;
     }
   }
-  if (TC) occ = std::min(occ, 16);  // 32 tensor-memory columns a block, 512 an SM
+  if (TC) {
+    // the occupancy query has answered 1 block per SM for this kernel even
+    // where 5 fit (measured); the blocks a multiprocessor holds by its shared
+    // memory, registers and threads, capped by tensor memory: 32 columns a
+    // block, 512 an SM
+    occ = std::min(std::max(occ, resident_blocks(reinterpret_cast<const void*>(k), 128, smem)), 16);
+  }
   const uint64_t want = a.nq;
   const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)occ * idx->sm_count));
   k<<<blocks, 128, smem, st>>>(a, W, S, CW, CWs);

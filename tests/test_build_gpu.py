@@ -77,3 +77,37 @@ def test_build_then_search_recall(lib_built):
     r = idx.search(q, 10, 64)
     assert P.recall_at_k(r.ids, gt, 10) > 0.9
     idx.close()
+
+
+_BLOCK_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r})
+sys.path.insert(0, {tests!r})
+import parlayann_b200 as P
+from conftest import random_points
+from oracle import oracle as O
+for dtype, metric in [(np.uint8, P.L2), (np.float32, P.L2), (np.float32, P.MIPS), (np.int8, P.MIPS)]:
+    base = random_points(dtype, 2500, 24, 71)
+    idx = P.Index(base, 12, metric)
+    st = idx.build(24, 1.2, num_passes=2)
+    g = idx.get_graph()
+    o, tot = O.build_graph("oracle", base, 12, 24, 1.2, 2, metric=metric)
+    live = lambda g: [tuple(r[1:1 + r[0]].tolist()) for r in g]
+    assert live(g) == live(o), (dtype, metric)
+    assert st.dist_cmps == tot, (dtype, metric)
+    idx.close()
+print("BLOCK_OK")
+"""
+
+
+def test_build_block_prune_kernel_matches_oracle(lib_built):
+    """The block-per-job greedy prune kernel (PANN_PRUNE_KERNEL=block, read once per process, so
+    run in a child process) gives the oracle's graph and distance-comparison count."""
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = _BLOCK_SCRIPT.format(root=os.path.dirname(here), tests=here)
+    env = dict(os.environ, PANN_PRUNE_KERNEL="block")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and "BLOCK_OK" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
