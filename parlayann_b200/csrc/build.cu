@@ -778,14 +778,14 @@ extern "C" int pann_build(pann_index* idx, const pann_build_params* bp, const ui
           return fail(PANN_ENOMEM, "reverse-edge prune segments exceed 2^31 keys");
         }
         // scratch for exactly seg_total keys (grown if this batch needs more)
-        BCUDA(bb.seg_a.ensure(8 * seg_total + 8));
-        BCUDA(bb.seg_b.ensure(8 * seg_total + 8));
+        BCUDA(bb.seg_a.ensure_grow(8 * seg_total + 8));
+        BCUDA(bb.seg_b.ensure_grow(8 * seg_total + 8));
         {
           size_t need = 0;
           cub::DeviceSegmentedSort::SortKeys(nullptr, need, bb.seg_a.as<uint64_t>(), bb.seg_b.as<uint64_t>(),
                                              (int)seg_total, (int)njobs, bb.seg_begin.as<uint32_t>(),
                                              bb.seg_end.as<uint32_t>(), st);
-          BCUDA(bb.cub_tmp.ensure(need + 256));
+          BCUDA(bb.cub_tmp.ensure_grow(need + 256));
         }
         BCUDA(dispatch_dm(dtype, metric, [&](auto DTc, auto MTc) {
           constexpr int DT = decltype(DTc)::value, MT = decltype(MTc)::value;

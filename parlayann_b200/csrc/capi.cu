@@ -612,7 +612,7 @@ int index_tier_buffers(pann_index* idx, const TierSizes& z, uint32_t nq, int pre
   // [7] global emulation job counter, [8] emulation overflow count,
   // [9] resume records taken
   PANN_CUDA(idx->counters.ensure(64));
-  PANN_CUDA(idx->redo.ensure(sizeof(uint32_t) * 6 * (size_t)std::max<uint32_t>(nq, 1)));
+  PANN_CUDA(idx->redo.ensure_grow(sizeof(uint32_t) * 6 * (size_t)std::max<uint32_t>(nq, 1)));
   TierBufs& b = *out;
   b = TierBufs{};
   b.cnt = idx->counters.as<uint32_t>();
@@ -625,15 +625,15 @@ int index_tier_buffers(pann_index* idx, const TierSizes& z, uint32_t nq, int pre
   // the spill table and the hand-off buffers are optional: without them
   // queries re-run in the later tiers
   if (precision == PREC_F32) {
-    if (idx->handoff.ensure(z.handoff_bytes) == cudaSuccess) b.handoff = idx->handoff.as<uint32_t>();
+    if (idx->handoff.ensure_grow(z.handoff_bytes) == cudaSuccess) b.handoff = idx->handoff.as<uint32_t>();
     else cudaGetLastError();
   }
-  if (idx->gtables.ensure(z.spill_bytes) == cudaSuccess) b.gspill = idx->gtables.as<uint32_t>();
+  if (idx->gtables.ensure_grow(z.spill_bytes) == cudaSuccess) b.gspill = idx->gtables.as<uint32_t>();
   else cudaGetLastError();
-  PANN_CUDA(idx->gtables2.ensure(z.t2_bytes));
+  PANN_CUDA(idx->gtables2.ensure_grow(z.t2_bytes));
   b.gt2 = idx->gtables2.as<uint32_t>();
   if (precision == PREC_F32) {
-    PANN_CUDA(idx->emu.ensure(z.e2_bytes));
+    PANN_CUDA(idx->emu.ensure_grow(z.e2_bytes));
     b.ge2 = idx->emu.as<uint32_t>();
   }
   return PANN_OK;

@@ -42,7 +42,10 @@ struct DevBuf {
   // a slightly larger request arrives)
   cudaError_t ensure_grow(size_t want) {
     if (want <= bytes) return cudaSuccess;
-    return ensure(std::max(want, bytes + bytes / 2));
+    const size_t grown = std::max(want, bytes + bytes / 2);
+    if (grown > want && ensure(grown) == cudaSuccess) return cudaSuccess;
+    cudaGetLastError();  // no room to spare: exactly what is asked
+    return ensure(want);
   }
   void release() {
     if (p) cudaFree(p);
