@@ -193,6 +193,27 @@ def replica_qps(queries_per_rank: int, steps: int, world: int, slowest_seconds: 
     return world * queries_per_rank * steps / slowest_seconds
 
 
+def profile_case(idx, q, beam, args):
+    """--case tile:PREC:PARENTS:SCORER (PREC bf16|fp8, SCORER cuda|tc): the tile search alone over the
+    1M workload, --warmup + --steps calls at the plain form's beam, for a profiler's launch selection
+    (the kernel's own launches only; no JSON metric line)."""
+    import parlayann_b200 as P
+
+    kind, prec, parents, scorer = args.case.split(":")
+    if kind != "tile":
+        raise SystemExit(f"unknown --case {args.case}")
+    pr = {"bf16": P.PREC_BF16, "fp8": P.PREC_FP8}[prec]
+    sc = {"cuda": P.SCORER_CUDA, "tc": P.SCORER_TENSOR}[scorer]
+    idx.set_precision(pr)
+    secs = []
+    for _ in range(args.warmup + args.steps):
+        t = time.time()
+        idx.search(q, W["k"], beam, precision=pr, parents=int(parents), scorer=sc)
+        secs.append(round(time.time() - t, 5))
+    idx.set_precision(P.PREC_F32)
+    return {"case": args.case, "beam": beam, "host_seconds_per_call": secs}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -237,6 +258,8 @@ def run_ours(args):
         res = idx.search(q, k, beam, batch_factor=W["bf"])
         recall = P.recall_with_ties(res.ids, gt, k, q, base)
     nq = q.shape[0]
+    if args.case:
+        return profile_case(idx, q, beam, args)
     mean_vis = float(res.visited.mean())
     mean_cmps = float(res.cmps.mean())
     row_bytes = W["d"] * 4
@@ -1042,6 +1065,8 @@ def main():
                          "Euclidean and mips)")
     ap.add_argument("--c3-n", type=int, default=100_000_000,
                     help="base vectors of the large uint8 batched-form run (forms c3)")
+    ap.add_argument("--case", default="", help="profiling case instead of the benchmark: tile:PREC:PARENTS:SCORER "
+                                                "(PREC bf16|fp8, SCORER cuda|tc)")
     ap.add_argument("--save-graph", default="", help="write the built graph (reference file format)")
     ap.add_argument("--load-graph", default="", help="load a graph file instead of building")
     args = ap.parse_args()
