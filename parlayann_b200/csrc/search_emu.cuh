@@ -96,6 +96,10 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
   *pos = p;
 }
 
+// Longest cluster the ranked placement replays; a longer one (or more long
+// clusters than the scratch lists) sends it to the plain sequential pass.
+constexpr uint32_t EMU_LONG_CLUSTER = 256;
+
 // Warp: place the keys keys[0..cnt) into the empty table `other` (mask
 // nmask) exactly as inserting them one at a time in rank order would
 // (hashset.h:39-47: probe from the key's slot to its first empty slot; a key
@@ -105,11 +109,12 @@ __device__ __forceinline__ void emu_probe_rounds(uint32_t* tab, uint32_t mask, u
 // only ever lands in the cluster that holds its home. So: (A) the keys'
 // ranks are placed in any order (lanes take ranks far apart, so they seldom
 // share slots), which fixes the clusters; (B) the lane whose key starts a
-// cluster replays that cluster's keys in rank order, each at the first free
-// slot from its home. A cluster longer than 64 sends the placement to a plain
-// sequential pass instead. `tail` (tail_words words after the keys, which may
-// alias the keys' own buffer past cnt) holds the owner bits and the per-lane
-// replay rows.
+// cluster of up to 8 keys replays it in rank order, each key at the first
+// free slot from its home, and the warp replays each longer cluster
+// together. A cluster longer than EMU_LONG_CLUSTER sends the placement to a
+// plain sequential pass instead. `tail` (tail_words words after the keys,
+// which may alias the keys' own buffer past cnt) holds the owner bits and
+// the list of long clusters.
 __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, uint32_t* other, uint32_t nmask,
                                                  uint32_t tail_words, int lane) {
   const unsigned FULL = 0xFFFFFFFFu;
@@ -169,14 +174,23 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
       if (lane == 0) owner[b] = om;
     }
     __syncwarp();
-    bool long_run = false;
+    // clusters of up to 8 keys are replayed by their owner lane in registers;
+    // longer ones are listed (start, length) in the scratch rows and replayed
+    // by the whole warp afterwards, so one long cluster does not hold 31 idle
+    // lanes for the square of its length
+    uint32_t* longs = scratch;
+    const uint32_t long_cap = scratch_ok ? 1024u : 0u;  // pairs in the 32 x 64-word scratch
+    uint32_t nlong = 0;
+    bool too_long = false;
     for (uint32_t b = 0; b < nb; b++) {
       const uint32_t r = b * 32 + lane;
+      bool is_long = false;
+      uint32_t s0 = 0, m = 0;
       if (r < cnt && ((owner[b] >> lane) & 1u)) {
-        uint32_t s0 = ref_slot(keys[r], nmask);
+        s0 = ref_slot(keys[r], nmask);
         while (other[s0] != r) s0 = (s0 + 1) & nmask;
-        uint32_t m = 1;
-        while (m <= 64 && other[(s0 + m) & nmask] != PANN_PAD) m++;
+        m = 1;
+        while (m <= EMU_LONG_CLUSTER && other[(s0 + m) & nmask] != PANN_PAD) m++;
         if (m == 1) {
           other[s0] = keys[r];
         } else if (m <= 8) {
@@ -203,31 +217,62 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
             taken |= 1u << pos;
             other[(s0 + pos) & nmask] = key;
           }
-        } else if (m <= 64 && scratch_ok) {
-          uint32_t* row = scratch + (size_t)lane * 64;
-          uint64_t taken = 0;
-          uint32_t last = 0xFFFFFFFFu;  // no rank taken yet
-          for (uint32_t t = 0; t < m; t++) {
-            uint32_t best = 0xFFFFFFFFu;
-            for (uint32_t j = 0; j < m; j++) {
-              const uint32_t w = other[(s0 + j) & nmask];
-              if ((last == 0xFFFFFFFFu || w > last) && w < best) best = w;
-            }
-            last = best;
-            const uint32_t key = keys[best];
-            const uint32_t o = (ref_slot(key, nmask) - s0) & nmask;
-            const uint32_t pos = (uint32_t)(__ffsll((long long)(~taken & (~0ull << o))) - 1);
-            taken |= 1ull << pos;
-            row[pos] = key;
-          }
-          for (uint32_t j = 0; j < m; j++) other[(s0 + j) & nmask] = row[j];
+        } else if (m <= EMU_LONG_CLUSTER) {
+          is_long = true;
         } else {
-          long_run = true;
+          too_long = true;
+        }
+      }
+      const unsigned lm = __ballot_sync(FULL, is_long);
+      if (is_long) {
+        const uint32_t at = nlong + __popc(lm & ((1u << lane) - 1));
+        if (at < long_cap) {
+          longs[2 * at] = s0;
+          longs[2 * at + 1] = m;
+        }
+      }
+      nlong += __popc(lm);
+      __syncwarp();
+    }
+    fallback = __any_sync(FULL, too_long) || nlong > long_cap;
+    // Long clusters, one at a time over the warp. Inserting a cluster's keys
+    // in rank order with linear probing leaves at each slot, left to right,
+    // the smallest-rank key whose home is at or before that slot among those
+    // not yet placed (a key of smaller rank that could reach the slot was
+    // inserted first and found every slot before it taken by smaller ranks),
+    // so each slot is one warp minimum over the eligible ranks.
+    for (uint32_t c = 0; c < nlong && !fallback; c++) {
+      const uint32_t s0 = longs[2 * c], m = longs[2 * c + 1];
+      uint32_t rk[EMU_LONG_CLUSTER / 32], ky[EMU_LONG_CLUSTER / 32], of[EMU_LONG_CLUSTER / 32];
+#pragma unroll
+      for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++) {
+        const uint32_t i = (uint32_t)j * 32 + (uint32_t)lane;
+        rk[j] = 0xFFFFFFFFu;
+        of[j] = 0xFFFFFFFFu;
+        ky[j] = 0;
+        if (i < m) {
+          rk[j] = other[(s0 + i) & nmask];
+          ky[j] = keys[rk[j]];
+          of[j] = (ref_slot(ky[j], nmask) - s0) & nmask;
+        }
+      }
+      __syncwarp();
+      for (uint32_t t = 0; t < m; t++) {
+        uint32_t best = 0xFFFFFFFFu, bkey = 0;
+        int bj = -1;
+#pragma unroll
+        for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++)
+          if (of[j] <= t && rk[j] < best) { best = rk[j]; bkey = ky[j]; bj = j; }
+        const uint32_t wmin = __reduce_min_sync(FULL, best);
+        if (bj >= 0 && best == wmin) {
+#pragma unroll
+          for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++)
+            if (j == bj) { rk[j] = 0xFFFFFFFFu; of[j] = 0xFFFFFFFFu; }
+          other[(s0 + t) & nmask] = bkey;
         }
       }
       __syncwarp();
     }
-    fallback = __any_sync(FULL, long_run);
   }
   if (fallback) {
     // the plain sequential re-insertion
@@ -820,10 +865,10 @@ __global__ void __launch_bounds__(NW * 32, 1) search_emulate_block_kernel(Search
       const uint64_t* rcand = reinterpret_cast<const uint64_t*>(rec + ly.cand);
       for (int i = tid; i < fn; i += nth) fr[i] = rfr[i];
       for (int i = tid; i < cn; i += nth) cand[i] = rcand[i];
+      // the logged ids, inserted in log order (staged in table B, unused until a growth)
+      for (uint32_t i = tid; i < entries; i += nth) tabB[i] = rec[ly.log + i];
+      __syncthreads();
       if (warp == 0) {
-        // the logged ids, inserted in log order (staged in table B, unused until a growth)
-        for (uint32_t i = lane; i < entries; i += 32) h.other[i] = rec[ly.log + i];
-        __syncwarp();
         emu_place_ranked(h.other, entries, h.cur, (1u << h.bits) - 1, h.other_cap, lane);
         __syncwarp();
         h.num_entries = entries;
