@@ -153,35 +153,31 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
   __threadfence_block();
   bool fallback = false;
   // (B) owners: keys that start a cluster, one bit per rank in the old table's
-  // free tail; then each owner replays its cluster (up to 8 keys in registers,
-  // up to 64 through a per-lane scratch row also in the free tail)
+  // free tail; then each owner replays its cluster of up to 8 keys in
+  // registers, and the warp each longer one (listed in the free tail)
   const uint32_t words = nb;
   uint32_t* owner = keys + ((cnt + 3) & ~3u);
   uint32_t* scratch = owner + ((words + 3) & ~3u);
   const bool scratch_ok = (size_t)(scratch - keys) + 32ull * 64 <= (size_t)tail_words;
   if (!fallback) {
-    for (uint32_t b = 0; b < nb; b++) {
-      const uint32_t r = b * 32 + lane;
-      bool own = false;
-      if (r < cnt) {
-        const uint32_t k = keys[r];
-        uint32_t p = ref_slot(k, nmask);
-        uint32_t w = other[p];
-        while (w != r && keys[w] != k) { p = (p + 1) & nmask; w = other[p]; }
-        own = w == r && other[(p - 1) & nmask] == PANN_PAD;  // a second copy of a key owns nothing
-      }
-      const unsigned om = __ballot_sync(FULL, own);
-      if (lane == 0) owner[b] = om;
+    // the rank at each cluster's first slot (occupied, the slot before it
+    // empty), found by one pass over the slots
+    for (uint32_t b = lane; b < nb; b += 32) owner[b] = 0;
+    __syncwarp();
+    for (uint32_t base = 0; base < nsize; base += 32) {
+      const uint32_t p = base + (uint32_t)lane;
+      const uint32_t w = p < nsize ? other[p] : PANN_PAD;
+      if (w != PANN_PAD && other[(p - 1) & nmask] == PANN_PAD) atomicOr(owner + (w >> 5), 1u << (w & 31));
     }
     __syncwarp();
+    __threadfence_block();
     // clusters of up to 8 keys are replayed by their owner lane in registers;
     // longer ones are listed (start, length) in the scratch rows and replayed
     // by the whole warp afterwards, so one long cluster does not hold 31 idle
     // lanes for the square of its length
     uint32_t* longs = scratch;
-    const uint32_t long_cap = scratch_ok ? 1024u : 0u;  // pairs in the 32 x 64-word scratch
+    const uint32_t long_cap = scratch_ok ? 1024u : 0u;  // (start, length) pairs in 2048 words
     uint32_t nlong = 0;
-    bool too_long = false;
     for (uint32_t b = 0; b < nb; b++) {
       const uint32_t r = b * 32 + lane;
       bool is_long = false;
@@ -190,7 +186,7 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
         s0 = ref_slot(keys[r], nmask);
         while (other[s0] != r) s0 = (s0 + 1) & nmask;
         m = 1;
-        while (m <= EMU_LONG_CLUSTER && other[(s0 + m) & nmask] != PANN_PAD) m++;
+        while (m <= 8 && other[(s0 + m) & nmask] != PANN_PAD) m++;
         if (m == 1) {
           other[s0] = keys[r];
         } else if (m <= 8) {
@@ -217,10 +213,8 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
             taken |= 1u << pos;
             other[(s0 + pos) & nmask] = key;
           }
-        } else if (m <= EMU_LONG_CLUSTER) {
-          is_long = true;
         } else {
-          too_long = true;
+          is_long = true;  // its length is measured by the warp below
         }
       }
       const unsigned lm = __ballot_sync(FULL, is_long);
@@ -234,7 +228,7 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
       nlong += __popc(lm);
       __syncwarp();
     }
-    fallback = __any_sync(FULL, too_long) || nlong > long_cap;
+    fallback = nlong > long_cap;
     // Long clusters, one at a time over the warp. Inserting a cluster's keys
     // in rank order with linear probing leaves at each slot, left to right,
     // the smallest-rank key whose home is at or before that slot among those
@@ -242,7 +236,21 @@ __device__ __forceinline__ void emu_place_ranked(uint32_t* keys, uint32_t cnt, u
     // inserted first and found every slot before it taken by smaller ranks),
     // so each slot is one warp minimum over the eligible ranks.
     for (uint32_t c = 0; c < nlong && !fallback; c++) {
-      const uint32_t s0 = longs[2 * c], m = longs[2 * c + 1];
+      const uint32_t s0 = longs[2 * c];
+      uint32_t m = 9;  // longer than 8: count 32 slots at a time up to its first empty slot
+      for (;;) {
+        const unsigned emp = __ballot_sync(FULL, other[(s0 + m + (uint32_t)lane) & nmask] == PANN_PAD);
+        if (emp) {
+          m += (uint32_t)(__ffs(emp) - 1);
+          break;
+        }
+        m += 32;
+        if (m > EMU_LONG_CLUSTER) break;
+      }
+      if (m > EMU_LONG_CLUSTER) {
+        fallback = true;
+        break;
+      }
       uint32_t rk[EMU_LONG_CLUSTER / 32], ky[EMU_LONG_CLUSTER / 32], of[EMU_LONG_CLUSTER / 32];
 #pragma unroll
       for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++) {
