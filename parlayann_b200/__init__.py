@@ -20,7 +20,8 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libparlayann_b200.so")
+# PANN_LIB_PATH loads another build of the same library (a debug or variant build)
+LIB_PATH = os.environ.get("PANN_LIB_PATH") or os.path.join(_HERE, "libparlayann_b200.so")
 
 PANN_OK, PANN_EINVAL, PANN_ENOMEM, PANN_ETIMEOUT, PANN_EDEVICE, PANN_EOVERFLOW, PANN_ESHORT = range(7)
 U8, I8, F32 = 0, 1, 2

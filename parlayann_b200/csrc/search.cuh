@@ -335,7 +335,12 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
           spec1 = (uint32_t)lane + 32 < nel ? __ldg(srow + 32 + lane) : PANN_PAD;
         }
       } else if (second >= 0 && lane == 0) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[second]) * a.R));
+        const uint32_t* srow = a.graph + (uint64_t)key_id(fr[second]) * a.R;
+#ifndef PANN_LINE_PREFETCH
+        if ((a.R & 3u) == 0) prefetch_l2_bulk(srow, 4u * a.R);
+        else
+#endif
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(srow));
       }
       __syncwarp();
       if (lane == 0) fr[first] = cur | PANN_VFLAG;
@@ -390,13 +395,10 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       // the expected next node's neighbours not seen so far: their rows on
       // their way to L2 while this node's rows are scored
       if (a.speculate && PREC == PREC_F32 && !TABLE_GLOBAL) {
-        const uint32_t lines = (uint32_t)((a.stride + 127) >> 7);
         if (spec0 != PANN_PAD && !table_has(table, mask, spec0))
-          for (uint32_t l = 0; l < lines; l++)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.points + (uint64_t)spec0 * a.stride + 128 * l));
+          prefetch_l2_bulk(a.points + (uint64_t)spec0 * a.stride, (uint32_t)a.stride);
         if (spec1 != PANN_PAD && !table_has(table, mask, spec1))
-          for (uint32_t l = 0; l < lines; l++)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.points + (uint64_t)spec1 * a.stride + 128 * l));
+          prefetch_l2_bulk(a.points + (uint64_t)spec1 * a.stride, (uint32_t)a.stride);
       }
       // distances; keep those below the cutoff (:176-182)
       cmps += (uint32_t)nnew;
