@@ -138,16 +138,6 @@ int smem_attr_max() {
   return cached[dev];
 }
 
-// Tier 0 loads the expected next node's adjacency during the visit before
-// and prefetches its unseen neighbours' rows (PANN_T0_SPECULATE=1).
-static bool t0_speculate() {
-  static const bool on = [] {
-    const char* e = std::getenv("PANN_T0_SPECULATE");
-    return e && e[0] == '1';
-  }();
-  return on;
-}
-
 int make_plan(const pann_index* idx, const pann_query_params* qp, uint32_t n_start, SearchPlan* plan) {
   if (!qp) return fail(PANN_EINVAL, "query params are NULL");
   if (qp->beam == 0) return fail(PANN_EINVAL, "beam (L) must be positive");
@@ -588,7 +578,6 @@ SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_
   a.vis_keys = d_vis_keys;
   a.vis_cap = vis_cap;
   a.opaque_zero = 0;
-  a.speculate = t0_speculate() ? 1u : 0u;
   return a;
 }
 

@@ -86,22 +86,9 @@ __device__ __forceinline__ int32_t dp4s(uint32_t a, uint32_t b, int32_t c) { ret
 // instead of one per line.
 constexpr int ROW_CHUNKS = 8;
 
-// One bulk prefetch of bytes (a multiple of 16) from a 16-byte aligned
-// global address into L2: the whole range, where a prefetch instruction per
-// line may bring in only the sector it names.
-__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// The part of a row past its first ROW_CHUNKS chunks (which the caller loads
-// at once) on its way to L2.
 __device__ __forceinline__ void prefetch_row_l2(const void* row, int nchunks) {
   const char* p = static_cast<const char*>(row);
-#ifdef PANN_LINE_PREFETCH
   for (int c = ROW_CHUNKS; c < nchunks; c += ROW_CHUNKS) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 16 * c));
-#else
-  if (nchunks > ROW_CHUNKS) prefetch_l2_bulk(p + 16 * ROW_CHUNKS, 16u * (uint32_t)(nchunks - ROW_CHUNKS));
-#endif
 }
 
 // uint8/int8 rows; q (16-byte chunks) staged in shared memory.

@@ -75,7 +75,6 @@ struct SearchArgs {
   uint32_t* emu_rec;    // per emu_list entry: resume record index, or PAD to re-run from scratch
   uint32_t* emu_count;
   uint64_t opaque_zero;  // always 0; see f32_chunk2
-  uint32_t speculate;    // 1: load the expected next node's adjacency early and prefetch its new rows
   // Hand-off to the emulation tier. Before the visit in which a query could
   // push the reference's seen-set past its growth threshold, tier 0 stops the
   // query and saves its exact state in a resume record; the emulation tier
@@ -286,9 +285,6 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
     // refreshed only at a merge: its distance, taken at the first scan after one
     float u0 = 0.0f;
     bool u0_fresh = true;
-    // the adjacency of the node expected to be expanded next, loaded during
-    // the visit before (its first 64 ids, one or two per lane)
-    uint32_t spec_id = PANN_PAD, spec0 = PANN_PAD, spec1 = PANN_PAD;
 
     for (;;) {
       __syncwarp();
@@ -322,26 +318,9 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       }
       const uint64_t cur = fr[first];
       // the next node to expand is most often the following unvisited entry:
-      // start its adjacency row on its way (into registers, or to L2)
-      const bool spec_hit = a.speculate && key_id(cur) == spec_id;
-      const uint32_t hit0 = spec0, hit1 = spec1;
-      if (a.speculate) {
-        spec_id = PANN_PAD;
-        spec0 = spec1 = PANN_PAD;
-        if (second >= 0 && nel <= 64) {
-          spec_id = key_id(fr[second]);
-          const uint32_t* srow = a.graph + (uint64_t)spec_id * a.R;
-          spec0 = (uint32_t)lane < nel ? __ldg(srow + lane) : PANN_PAD;
-          spec1 = (uint32_t)lane + 32 < nel ? __ldg(srow + 32 + lane) : PANN_PAD;
-        }
-      } else if (second >= 0 && lane == 0) {
-        const uint32_t* srow = a.graph + (uint64_t)key_id(fr[second]) * a.R;
-#ifndef PANN_LINE_PREFETCH
-        if ((a.R & 3u) == 0) prefetch_l2_bulk(srow, 4u * a.R);
-        else
-#endif
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(srow));
-      }
+      // start its adjacency row on its way to L2
+      if (second >= 0 && lane == 0)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a.graph + (uint64_t)key_id(fr[second]) * a.R));
       __syncwarp();
       if (lane == 0) fr[first] = cur | PANN_VFLAG;
       nvis++;
@@ -370,10 +349,10 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       uint32_t ins = 0;
       // the next 32 ids are loaded before this chunk's seen-set work, so a
       // row longer than one warp costs one round trip, not one per chunk
-      uint32_t vnext = spec_hit ? hit0 : ((uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD);
+      uint32_t vnext = (uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD;
       for (uint32_t b = 0; b < nel; b += 32) {
         const uint32_t v = vnext;
-        vnext = (spec_hit && b == 0) ? hit1 : ((b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD);
+        vnext = (b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD;
         int inserted = 0;
         if (v != PANN_PAD) {
           if (!spilled) inserted = table_insert(table, mask, v);
@@ -392,14 +371,6 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       if (entries > ref_half) status |= QS_REF_WOULD_GROW;
       __syncwarp();
 
-      // the expected next node's neighbours not seen so far: their rows on
-      // their way to L2 while this node's rows are scored
-      if (a.speculate && PREC == PREC_F32 && !TABLE_GLOBAL) {
-        if (spec0 != PANN_PAD && !table_has(table, mask, spec0))
-          prefetch_l2_bulk(a.points + (uint64_t)spec0 * a.stride, (uint32_t)a.stride);
-        if (spec1 != PANN_PAD && !table_has(table, mask, spec1))
-          prefetch_l2_bulk(a.points + (uint64_t)spec1 * a.stride, (uint32_t)a.stride);
-      }
       // distances; keep those below the cutoff (:176-182)
       cmps += (uint32_t)nnew;
       if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }

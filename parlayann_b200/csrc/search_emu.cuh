@@ -414,6 +414,255 @@ __device__ __forceinline__ bool emu_batch(EmuHash& h, uint32_t key, bool valid, 
   return true;
 }
 
+// As emu_batch, but stops at the first call that grows the table: the calls
+// before it take effect (their results in *seen) and *grow_lane gets the
+// growing call's lane, -1 if none. The caller grows the table for that key
+// (emu_grow_block) and continues with the lanes after it.
+__device__ __forceinline__ void emu_batch_part(EmuHash& h, uint32_t key, bool act, int lane, bool* seen,
+                                               int* grow_lane) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const unsigned todo = __ballot_sync(FULL, act);
+  const uint32_t size = 1u << h.bits, mask = size - 1;
+  const uint32_t home = ref_slot(key, mask);
+  const bool home_hit0 = act && h.cur[home] == key;
+  __syncwarp();
+  bool ins;
+  uint32_t pos;
+  emu_probe_rounds(h.cur, mask, key, act, home, lane, &ins, &pos);
+  const unsigned kgrp = __match_any_sync(FULL, act ? key : (0x80000000u | (uint32_t)lane));
+  const int first = __ffs(kgrp & todo) - 1;
+  const bool f_ins = __shfl_sync(FULL, ins, first < 0 ? lane : first);
+  const uint32_t f_pos = __shfl_sync(FULL, pos, first < 0 ? lane : first);
+  const bool home_hit = home_hit0 || (act && first >= 0 && first < lane && f_ins && f_pos == home);
+  const unsigned insm = __ballot_sync(FULL, act && ins);
+  const long long before = h.num_entries + __popc(insm & ((1u << lane) - 1));
+  const bool grows = act && !home_hit && before > (long long)(size / 2);
+  const unsigned gm = __ballot_sync(FULL, grows);
+  if (!gm) {
+    if (act) *seen = !ins;
+    h.num_entries += __popc(insm);
+    *grow_lane = -1;
+    return;
+  }
+  const int g = __ffs(gm) - 1;
+  if (act && ins && lane >= g) h.cur[pos] = PANN_PAD;  // undo the calls at and after g
+  __syncwarp();
+  __threadfence_block();
+  if (act && lane < g) *seen = !ins;
+  h.num_entries += __popc(insm & ((1u << g) - 1));
+  *grow_lane = g;
+}
+
+// Block: emu_place_ranked with every thread of the block (nth threads, NW
+// warps). (A) ranks claim slots with compare-and-swap in any order (the set
+// of occupied slots does not depend on it; a repeated key keeps its smaller
+// rank); (B) cluster owners from one pass over the slots, clusters of up to
+// 8 keys replayed by their owner thread, longer ones by one warp each;
+// beyond EMU_LONG_CLUSTER keys, or more long clusters than the free tail
+// lists, a sequential pass by thread 0. ctl: 4 words of shared scratch.
+__device__ __forceinline__ void emu_place_ranked_block(uint32_t* keys, uint32_t cnt, uint32_t* other, uint32_t nmask,
+                                                       uint32_t tail_words, int tid, int nth, volatile uint32_t* ctl) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const int lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+  const uint32_t nsize = nmask + 1;
+  volatile uint32_t* vo = other;
+  for (uint32_t r = (uint32_t)tid; r < cnt; r += (uint32_t)nth) {
+    const uint32_t k = keys[r];
+    uint32_t p = ref_slot(k, nmask);
+    for (;;) {
+      uint32_t w = vo[p];
+      if (w == PANN_PAD) {
+        w = atomicCAS(other + p, PANN_PAD, r);
+        if (w == PANN_PAD) break;
+      }
+      if (keys[w] == k) {
+        atomicMin(other + p, r);
+        break;
+      }
+      p = (p + 1) & nmask;
+    }
+  }
+  const uint32_t nb = (cnt + 31) / 32;
+  uint32_t* owner = keys + ((cnt + 3) & ~3u);
+  uint32_t* longs = owner + ((nb + 3) & ~3u);
+  const uint32_t room = (size_t)(longs - keys) < (size_t)tail_words ? tail_words - (uint32_t)(longs - keys) : 0u;
+  const uint32_t long_cap = room < 1024u ? room : 1024u;
+  if (tid == 0) { ctl[0] = 0; ctl[1] = 0; }
+  for (uint32_t b = (uint32_t)tid; b < nb; b += (uint32_t)nth) owner[b] = 0;
+  __syncthreads();
+  for (uint32_t p = (uint32_t)tid; p < nsize; p += (uint32_t)nth) {
+    const uint32_t w = vo[p];
+    if (w != PANN_PAD && vo[(p - 1) & nmask] == PANN_PAD) atomicOr(owner + (w >> 5), 1u << (w & 31));
+  }
+  __syncthreads();
+  for (uint32_t r = (uint32_t)tid; r < cnt; r += (uint32_t)nth) {
+    if (!((owner[r >> 5] >> (r & 31)) & 1u)) continue;
+    const uint32_t s0 = ref_slot(keys[r], nmask);  // an owner sits at its home
+    uint32_t m = 1;
+    while (m <= 8 && vo[(s0 + m) & nmask] != PANN_PAD) m++;
+    if (m == 1) {
+      other[s0] = keys[r];
+    } else if (m <= 8) {
+      uint32_t ix[8], kx[8], ox[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) ix[j] = (uint32_t)j < m ? vo[(s0 + j) & nmask] : 0xFFFFFFFFu;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        kx[j] = (uint32_t)j < m ? keys[ix[j]] : 0u;
+        ox[j] = (ref_slot(kx[j], nmask) - s0) & nmask;
+      }
+      uint32_t taken = 0, used = 0;
+      for (uint32_t t = 0; t < m; t++) {
+        uint32_t best = 0xFFFFFFFFu, bj = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          if (!((used >> j) & 1u) && ix[j] < best) { best = ix[j]; bj = (uint32_t)j; }
+        used |= 1u << bj;
+        uint32_t key = 0, o = 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          if ((uint32_t)j == bj) { key = kx[j]; o = ox[j]; }
+        const uint32_t pos = (uint32_t)(__ffs(~taken & (~0u << o)) - 1);
+        taken |= 1u << pos;
+        other[(s0 + pos) & nmask] = key;
+      }
+    } else {
+      const uint32_t at = atomicAdd((uint32_t*)ctl, 1u);
+      if (at < long_cap) longs[at] = s0;
+    }
+  }
+  __syncthreads();
+  const uint32_t nlong = ctl[0];
+  bool fallback = nlong > long_cap;
+  for (uint32_t c = (uint32_t)warp; c < nlong && !fallback; c += (uint32_t)nw) {
+    const uint32_t s0 = longs[c];
+    uint32_t m = 9;
+    for (;;) {
+      const unsigned emp = __ballot_sync(FULL, vo[(s0 + m + (uint32_t)lane) & nmask] == PANN_PAD);
+      if (emp) {
+        m += (uint32_t)(__ffs(emp) - 1);
+        break;
+      }
+      m += 32;
+      if (m > EMU_LONG_CLUSTER) break;
+    }
+    if (m > EMU_LONG_CLUSTER) {
+      if (lane == 0) ctl[1] = 1;
+      break;
+    }
+    uint32_t rk[EMU_LONG_CLUSTER / 32], ky[EMU_LONG_CLUSTER / 32], of[EMU_LONG_CLUSTER / 32];
+#pragma unroll
+    for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++) {
+      const uint32_t i = (uint32_t)j * 32 + (uint32_t)lane;
+      rk[j] = 0xFFFFFFFFu;
+      of[j] = 0xFFFFFFFFu;
+      ky[j] = 0;
+      if (i < m) {
+        rk[j] = vo[(s0 + i) & nmask];
+        ky[j] = keys[rk[j]];
+        of[j] = (ref_slot(ky[j], nmask) - s0) & nmask;
+      }
+    }
+    __syncwarp();
+    for (uint32_t t = 0; t < m; t++) {
+      uint32_t best = 0xFFFFFFFFu, bkey = 0;
+      int bj = -1;
+#pragma unroll
+      for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++)
+        if (of[j] <= t && rk[j] < best) { best = rk[j]; bkey = ky[j]; bj = j; }
+      const uint32_t wmin = __reduce_min_sync(FULL, best);
+      if (bj >= 0 && best == wmin) {
+#pragma unroll
+        for (int j = 0; j < EMU_LONG_CLUSTER / 32; j++)
+          if (j == bj) { rk[j] = 0xFFFFFFFFu; of[j] = 0xFFFFFFFFu; }
+        other[(s0 + t) & nmask] = bkey;
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  if (fallback || ctl[1]) {
+    const uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+    for (uint32_t i = (uint32_t)tid; i < (nsize >> 2); i += (uint32_t)nth) reinterpret_cast<uint4*>(other)[i] = e4;
+    __syncthreads();
+    if (tid == 0) {
+      for (uint32_t i = 0; i < cnt; i++) {
+        const uint32_t k = keys[i];
+        uint32_t p = ref_slot(k, nmask);
+        while (vo[p] != PANN_PAD && vo[p] != k) p = (p + 1) & nmask;
+        vo[p] = k;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Block: emu_grow with every thread (the table state passed in, the
+// triggering key a). Returns false (every thread alike) if the grown table
+// does not fit `other_cap`; else *added = re-inserted keys and *a_seen =
+// whether a was found. ctl: 8 words of shared scratch.
+__device__ __forceinline__ bool emu_grow_block(uint32_t* cur, uint32_t* other, uint32_t bits, uint32_t other_cap,
+                                               uint32_t a, int tid, int nth, volatile uint32_t* ctl, uint32_t* added,
+                                               bool* a_seen) {
+  const unsigned FULL = 0xFFFFFFFFu;
+  const int lane = tid & 31, warp = tid >> 5, nw = nth >> 5;
+  const uint32_t size = 1u << bits, nsize = size * 2;
+  if (nsize > other_cap) return false;
+  const uint4 e4 = make_uint4(PANN_PAD, PANN_PAD, PANN_PAD, PANN_PAD);
+  for (uint32_t i = (uint32_t)tid; i < (nsize >> 2); i += (uint32_t)nth) reinterpret_cast<uint4*>(other)[i] = e4;
+  // the old table's keys compacted to its front in slot order
+  uint32_t cnt = 0;
+  for (uint32_t base = 0; base < size; base += 4u * (uint32_t)nth) {
+    uint32_t k4[4];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uint32_t i = base + 4 * (uint32_t)tid + (uint32_t)j;
+      k4[j] = i < size ? cur[i] : PANN_PAD;
+      c += k4[j] != PANN_PAD;
+    }
+    uint32_t pre = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, pre, d);
+      if (lane >= d) pre += t;
+    }
+    if (lane == 31) ctl[4 + warp] = pre;
+    __syncthreads();
+    uint32_t woff = 0, total = 0;
+    for (int w = 0; w < nw; w++) {
+      const uint32_t t = ctl[4 + w];
+      woff += w < warp ? t : 0u;
+      total += t;
+    }
+    __syncthreads();
+    uint32_t at = cnt + woff + pre - c;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (k4[j] != PANN_PAD) cur[at++] = k4[j];
+    cnt += total;
+    __syncthreads();
+  }
+  emu_place_ranked_block(cur, cnt, other, nsize - 1, size, tid, nth, ctl);
+  // the call that grew the table: probe from the old-mask slot in the new table
+  if (tid == 0) {
+    uint32_t loc = ref_slot(a, size - 1);
+    uint32_t hit = 0;
+    if (other[loc] != PANN_PAD) {
+      loc = (loc + 1) & (nsize - 1);
+      while (other[loc] != PANN_PAD && other[loc] != a) loc = (loc + 1) & (nsize - 1);
+      hit = other[loc] == a;
+    }
+    if (!hit) other[loc] = a;
+    ctl[0] = hit;
+  }
+  __syncthreads();
+  *added = cnt;
+  *a_seen = ctl[0] != 0;
+  __syncthreads();
+  return true;
+}
+
 __device__ __forceinline__ void vset_insert(uint32_t* t, uint32_t mask, uint32_t id) {
   uint32_t h = hash_slot(id, mask);
   for (uint32_t p = 0; p <= mask; p++) {
@@ -724,7 +973,7 @@ __host__ __device__ inline EmuBlockLayout emu_block_layout(uint64_t stride, uint
   y.nbuf = (uint32_t)o; o += 4ull * R4;
   y.npos = (uint32_t)o; o += 4ull * R4;
   y.dall = (uint32_t)o; o += 4ull * R4;
-  y.ctrl = (uint32_t)o; o += 64;
+  y.ctrl = (uint32_t)o; o += 128;
   y.vset = (uint32_t)o; o += 4ull * vs;
   y.tabA = (uint32_t)o; o += 4ull * capA;
   y.tabB = (uint32_t)o; o += 4ull * capB;
@@ -876,13 +1125,9 @@ __global__ void __launch_bounds__(NW * 32, 1) search_emulate_block_kernel(Search
       // the logged ids, inserted in log order (staged in table B, unused until a growth)
       for (uint32_t i = tid; i < entries; i += nth) tabB[i] = rec[ly.log + i];
       __syncthreads();
-      if (warp == 0) {
-        emu_place_ranked(h.other, entries, h.cur, (1u << h.bits) - 1, h.other_cap, lane);
-        __syncwarp();
-        h.num_entries = entries;
-      } else {
-        for (uint32_t i = tid - 32; i < (uint32_t)nvis; i += nth - 32) vset_insert(vset, vmask, rec[ly.vis + i]);
-      }
+      emu_place_ranked_block(tabB, entries, tabA, (1u << bits0) - 1, e.capB, tid, nth, ctrl + 20);
+      h.num_entries = entries;
+      for (uint32_t i = tid; i < (uint32_t)nvis; i += nth) vset_insert(vset, vmask, rec[ly.vis + i]);
     } else {
       for (uint32_t s = tid; s < a.n_start; s += nth) {
         const uint32_t id = a.starts[s];
@@ -945,37 +1190,89 @@ __global__ void __launch_bounds__(NW * 32, 1) search_emulate_block_kernel(Search
       if (nvis > (uint64_t)(vmask / 4 * 3)) { status |= QS_INTERNAL; break; }
       const uint32_t cid = key_id(cur_key);
       const uint32_t* grow = a.graph + (uint64_t)cid * a.R;
-      if (warp == 0) {
-        // the hashset calls, in adjacency order (:153-159)
-        int nnew = 0;
+      {
+        // warp 0 makes the hashset calls in adjacency order (:153-159) while
+        // warps 1..NW-1 score every neighbour; a call that grows the table
+        // stops the calls, the whole block grows it (emu_grow_block), and
+        // warp 0 goes on with the calls after it
+        int nnew = 0;            // warp 0's state from here on
         bool full_tab = false;
-        uint32_t vnext = (uint32_t)lane < nel ? __ldg(grow + lane) : PANN_PAD;
-        for (uint32_t b = 0; b < nel; b += 32) {
-          const uint32_t v = vnext;
-          vnext = (b + 32 + lane < nel) ? __ldg(grow + b + 32 + lane) : PANN_PAD;
-          bool seen = false;
-          if (!emu_batch(h, v, v != PANN_PAD, lane, &seen)) { full_tab = true; break; }
-          const bool isnew = v != PANN_PAD && !seen && v != self;
-          const unsigned mn = __ballot_sync(FULL, isnew);
-          if (isnew) {
-            const int at = nnew + __popc(mn & ((1u << lane) - 1));
-            nbuf[at] = v;
-            npos[at] = b + lane;
+        uint32_t b = 0, v = PANN_PAD;
+        unsigned pend = 0;
+        bool open = false, seen = false;
+        int g = -1;
+        bool first_round = true;
+        for (;;) {
+          if (warp == 0) {
+            g = -1;
+            while (!full_tab) {
+              if (!open) {
+                if (b >= nel) break;
+                v = b + lane < nel ? __ldg(grow + b + lane) : PANN_PAD;
+                pend = __ballot_sync(FULL, v != PANN_PAD);
+                seen = false;
+                open = true;
+              }
+              if (pend) {
+                emu_batch_part(h, v, (pend >> lane) & 1u, lane, &seen, &g);
+                if (g >= 0) {
+                  pend &= ~((2u << g) - 1u);
+                  break;
+                }
+                pend = 0;
+              }
+              const bool isnew = v != PANN_PAD && !seen && v != self;
+              const unsigned mn = __ballot_sync(FULL, isnew);
+              if (isnew) {
+                const int at = nnew + __popc(mn & ((1u << lane) - 1));
+                nbuf[at] = v;
+                npos[at] = b + lane;
+              }
+              nnew += __popc(mn);
+              b += 32;
+              open = false;
+            }
+            const uint32_t gkey = __shfl_sync(FULL, v, g < 0 ? 0 : g);
+            if (lane == 0) {
+              ctrl[2] = (uint32_t)nnew;
+              ctrl[3] = full_tab;
+              ctrl[16] = g >= 0 && !full_tab ? gkey : PANN_PAD;
+              ctrl[18] = h.cur == tabB;
+              ctrl[19] = h.bits;
+              ctrl[28] = h.other_cap;
+            }
+          } else if (first_round) {
+            // every neighbour scored while warp 0 probes the table
+            for (uint32_t j = tid - 32; j < nel; j += nth - 32) {
+              const uint32_t u = __ldg(grow + j);
+              if (u != PANN_PAD)
+                dall[j] = row_dist_whole<DT, MT, CH>(a.points + (uint64_t)u * a.stride, qs, a.nchunks, qq);
+            }
           }
-          nnew += __popc(mn);
-        }
-        if (lane == 0) {
-          ctrl[2] = (uint32_t)nnew;
-          ctrl[3] = full_tab;
-        }
-      } else {
-        // every neighbour scored while warp 0 probes the table
-        for (uint32_t j = tid - 32; j < nel; j += nth - 32) {
-          const uint32_t v = __ldg(grow + j);
-          if (v != PANN_PAD) dall[j] = row_dist_whole<DT, MT, CH>(a.points + (uint64_t)v * a.stride, qs, a.nchunks, qq);
+          __syncthreads();
+          first_round = false;
+          const uint32_t gk = ctrl[16];
+          if (gk == PANN_PAD) break;
+          uint32_t* gcur = ctrl[18] ? tabB : tabA;
+          uint32_t* goth = ctrl[18] ? tabA : tabB;
+          uint32_t added = 0;
+          bool aseen = false;
+          const bool grew = emu_grow_block(gcur, goth, ctrl[19], ctrl[28], gk, tid, nth, ctrl + 20, &added, &aseen);
+          if (warp == 0) {
+            if (!grew) {
+              full_tab = true;
+            } else {
+              h.num_entries += added;
+              uint32_t* t = h.cur; h.cur = h.other; h.other = t;
+              const uint32_t c = h.cur_cap; h.cur_cap = h.other_cap; h.other_cap = c;
+              h.bits += 1;
+              if (!aseen) h.num_entries++;
+              if (lane == g) seen = aseen;
+            }
+          }
+          __syncthreads();
         }
       }
-      __syncthreads();
       const int nnew = (int)ctrl[2];
       if (ctrl[3]) {
         status |= QS_TABLE_FULL;
