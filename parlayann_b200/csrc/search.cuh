@@ -374,6 +374,38 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       // distances; keep those below the cutoff (:176-182)
       cmps += (uint32_t)nnew;
       if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
+#ifdef PANN_T0_ONE_ROW
+      // one row per lane per round, PANN_T0_ONE_ROW chunks of it in flight at once
+      if (PREC == PREC_F32 && DT == DT_F32) {
+        for (int b = 0; b < nnew; b += 32) {
+          const int i0 = b + lane;
+          float d0 = 0.0f;
+          uint32_t v0 = 0;
+          if (i0 < nnew) {
+            v0 = nbuf[i0];
+            const float4* row = reinterpret_cast<const float4*>(a.points + (uint64_t)v0 * a.stride);
+            const float4* q = reinterpret_cast<const float4*>(qs);
+            const int nv = (int)a.nchunks;
+            if (nv > PANN_T0_ONE_ROW) prefetch_row_l2(row, nv);
+            float r = 0.0f;
+            for (int c0 = 0; c0 < nv; c0 += PANN_T0_ONE_ROW) {
+              float4 buf[PANN_T0_ONE_ROW];
+#pragma unroll
+              for (int c = 0; c < PANN_T0_ONE_ROW; c++)
+                if (c0 + c < nv) buf[c] = __ldg(row + c0 + c);
+#pragma unroll
+              for (int c = 0; c < PANN_T0_ONE_ROW; c++)
+                if (c0 + c < nv) r = f32_chunk<MT>(r, buf[c], q[c0 + c]);
+            }
+            d0 = MT == MT_L2 ? r : -r;
+          }
+          const bool keep0 = i0 < nnew && !(d0 >= cutoff);
+          const unsigned m0 = __ballot_sync(FULL, keep0);
+          if (keep0) cand[cn + __popc(m0 & ((1u << lane) - 1))] = make_key(d0, v0);
+          cn += __popc(m0);
+        }
+      } else
+#endif
       // two rows per lane per round: rows b+lane and b+32+lane
       for (int b = 0; b < nnew; b += 64) {
         const int i0 = b + lane, i1 = b + 32 + lane;
