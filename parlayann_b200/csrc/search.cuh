@@ -199,6 +199,9 @@ __device__ __forceinline__ int table_insert(uint32_t* table, uint32_t mask, uint
   return 0;
 }
 
+// Chunks of a float32 row a tier-0 lane has in flight at once.
+constexpr int T0_ROW_CHUNKS = 12;
+
 // MINB: blocks of 128 threads the register budget is fitted to (3: 168
 // registers a thread; 4: 128).
 template <int DT, int MT, bool TABLE_GLOBAL, int PREC = PREC_F32, int MINB = 3>
@@ -374,8 +377,11 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
       // distances; keep those below the cutoff (:176-182)
       cmps += (uint32_t)nnew;
       if ((uint32_t)(cn + nnew) > a.Ccap) { status |= QS_INTERNAL; break; }
-#ifdef PANN_T0_ONE_ROW
-      // one row per lane per round, PANN_T0_ONE_ROW chunks of it in flight at once
+      // float32 rows: one row per lane per round, T0_ROW_CHUNKS chunks of it
+      // in flight at once (the rest of the row prefetched to L2 first). On the
+      // 1M x 96 workload this is 2.29 M QPS against 2.11 M for two rows per
+      // lane in batches of 8 chunks (PAIR_CHUNKS), 2.29 M with 16 chunks, and
+      // 1.89 M with all 24 chunks at once, which spills (A/B on one box).
       if (PREC == PREC_F32 && DT == DT_F32) {
         for (int b = 0; b < nnew; b += 32) {
           const int i0 = b + lane;
@@ -386,15 +392,15 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
             const float4* row = reinterpret_cast<const float4*>(a.points + (uint64_t)v0 * a.stride);
             const float4* q = reinterpret_cast<const float4*>(qs);
             const int nv = (int)a.nchunks;
-            if (nv > PANN_T0_ONE_ROW) prefetch_row_l2(row, nv);
+            if (nv > T0_ROW_CHUNKS) prefetch_row_l2(row, nv);
             float r = 0.0f;
-            for (int c0 = 0; c0 < nv; c0 += PANN_T0_ONE_ROW) {
-              float4 buf[PANN_T0_ONE_ROW];
+            for (int c0 = 0; c0 < nv; c0 += T0_ROW_CHUNKS) {
+              float4 buf[T0_ROW_CHUNKS];
 #pragma unroll
-              for (int c = 0; c < PANN_T0_ONE_ROW; c++)
+              for (int c = 0; c < T0_ROW_CHUNKS; c++)
                 if (c0 + c < nv) buf[c] = __ldg(row + c0 + c);
 #pragma unroll
-              for (int c = 0; c < PANN_T0_ONE_ROW; c++)
+              for (int c = 0; c < T0_ROW_CHUNKS; c++)
                 if (c0 + c < nv) r = f32_chunk<MT>(r, buf[c], q[c0 + c]);
             }
             d0 = MT == MT_L2 ? r : -r;
@@ -405,7 +411,6 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
           cn += __popc(m0);
         }
       } else
-#endif
       // two rows per lane per round: rows b+lane and b+32+lane
       for (int b = 0; b < nnew; b += 64) {
         const int i0 = b + lane, i1 = b + 32 + lane;
