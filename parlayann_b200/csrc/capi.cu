@@ -390,9 +390,17 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
 }
 
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a0, const TierSizes& z,
-                  const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank) {
+                  const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank, cudaStream_t side) {
   uint32_t* cnt = b.cnt;
   PANN_CUDA(cudaMemsetAsync(cnt, 0, 64, st));
+  // an emulation pass beside tier 0's tail: its blocks need most of an SM's
+  // shared memory, so they start only as tier 0's blocks leave the SMs
+  const bool early = side && idx->ev_fork && idx->ev_join && precision == PREC_F32 && z.emu_smem && !z.cta;
+  if (early) {
+    PANN_CUDA(cudaMemsetAsync(b.emu_rec, 0xFE, sizeof(uint32_t) * (size_t)std::max<uint32_t>(a0.nq, 1), st));
+    PANN_CUDA(cudaEventRecord(idx->ev_fork, st));
+    PANN_CUDA(cudaStreamWaitEvent(side, idx->ev_fork, 0));
+  }
   SearchArgs a = a0;
   a.emu_list = b.emu;
   a.emu_rec = b.emu_rec;
@@ -478,6 +486,30 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
     PANN_CUDA(launch_search(idx->dtype, idx->metric, false, t, z.blocks, 32 * z.wpb, (size_t)z.wb * z.wpb, st, precision,
                             z.minb));
   }
+  if (early) {
+    SearchArgs t = a;
+    t.redo_list = nullptr;
+    t.redo_count = nullptr;
+    t.emu_list = nullptr;
+    t.emu_count = nullptr;
+    t.job_list = b.emu;
+    t.njobs_dev = cnt + 6;
+    t.job_counter = cnt + 5;
+    EmuArgs e{};
+    e.bits0 = z.bits0;
+    e.vs_slots = z.vs;
+    e.base_bytes = z.base;
+    e.capA = (uint32_t)(4 * z.S0);
+    e.capB = (uint32_t)(2 * z.S0);
+    e.overflow_list = b.ovf;
+    e.overflow_rec = b.ovf_rec;
+    e.overflow_count = cnt + 8;
+    e.job_rec = b.emu_rec;
+    e.early = 1;
+    PANN_CUDA(launch_emulate_block(idx->dtype, idx->metric, t, e, (int)std::min<uint64_t>(idx->sm_count, a.nq),
+                                   z.emu_smem_need, side));
+    PANN_CUDA(cudaEventRecord(idx->ev_join, side));
+  }
   // ---- tier 2: queries whose tables still filled up, with one global-memory
   // seen table per warp sized above the reference's own capacity
   {
@@ -528,6 +560,8 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
       grec = b.ovf_rec;
       gcount = cnt + 8;
     }
+    // the pass beside tier 0 adds to the overflow list too
+    if (early) PANN_CUDA(cudaStreamWaitEvent(st, idx->ev_join, 0));
     e.gA = b.ge2;
     e.gB = e.gA + (size_t)z.e2_slots * z.capA;
     e.capA = (uint32_t)z.capA;
@@ -581,6 +615,37 @@ SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_
   return a;
 }
 
+// The index's side stream (lowest priority) and its fork / join events,
+// created on first use; nullptr if they cannot be created (the emulation
+// then runs only after the search tiers). PANN_EMU_OVERLAP=0 turns the
+// overlapped pass off.
+static cudaStream_t side_stream(pann_index* idx) {
+  static const bool off = [] {
+    const char* e = std::getenv("PANN_EMU_OVERLAP");
+    return e && e[0] == '0';
+  }();
+  if (off) return nullptr;
+  if (!idx->side) {
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) lo = 0;
+    cudaStream_t s = nullptr;
+    cudaEvent_t f = nullptr, j = nullptr;
+    if (cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      if (s) cudaStreamDestroy(s);
+      if (f) cudaEventDestroy(f);
+      if (j) cudaEventDestroy(j);
+      return nullptr;
+    }
+    idx->side = s;
+    idx->ev_fork = f;
+    idx->ev_join = j;
+  }
+  return idx->side;
+}
+
 int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries, const uint32_t* d_self_ids,
                uint32_t nq, const uint32_t* d_starts, uint32_t* d_ids, float* d_dists, uint32_t* d_vis,
                uint32_t* d_cmps, uint32_t* d_status, uint64_t* d_vis_keys, uint32_t vis_cap, cudaStream_t st,
@@ -603,7 +668,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   if (rc) return rc;
   SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
                            d_vis_keys, vis_cap);
-  return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank);
+  return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank, side_stream(idx));
 }
 
 int index_tier_buffers(pann_index* idx, const TierSizes& z, uint32_t nq, int precision, TierBufs* out) {
@@ -732,6 +797,7 @@ int pann_index_create(pann_index** out, int dtype, int metric, uint64_t n, uint3
 int pann_index_destroy(pann_index* idx) {
   if (!idx) return PANN_OK;
   if (idx->stream) cudaStreamSynchronize(idx->stream);
+  if (idx->side) cudaStreamSynchronize(idx->side);
   if (idx->quant) pann_index_destroy(idx->quant);
   if (idx->d_points) cudaFree(idx->d_points);
   if (idx->d_graph && !idx->graph_borrowed) cudaFree(idx->d_graph);
@@ -740,6 +806,10 @@ int pann_index_destroy(pann_index* idx) {
                     &idx->tmp, &idx->lp_rows, &idx->lp_scales, &idx->range_meta, &idx->range_tabs,
                     &idx->range_pool, &idx->range_out})
     b->release();
+  idx->lp_norms.release();
+  if (idx->ev_fork) cudaEventDestroy(idx->ev_fork);
+  if (idx->ev_join) cudaEventDestroy(idx->ev_join);
+  if (idx->side) cudaStreamDestroy(idx->side);
   if (idx->stream) cudaStreamDestroy(idx->stream);
   delete idx;
   return PANN_OK;

@@ -71,6 +71,10 @@ struct pann_index {
   uint32_t* d_graph = nullptr;
   bool points_set = false;
   cudaStream_t stream = nullptr;
+  // a low-priority stream and two events for the emulation pass that runs
+  // beside tier 0's tail (created on first use by a plain search)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // search scratch
   pann::DevBuf q, ids, dists, vis, cmps, status, redo, counters, gtables, gtables2, emu, handoff, starts, tmp;
   // range search: per-query metadata, expansion tables and queues, answer pool, CSR output

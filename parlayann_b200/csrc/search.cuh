@@ -484,11 +484,15 @@ __global__ void __launch_bounds__(128, MINB) search_kernel(SearchArgs a) {
           r = PANN_PAD;  // no room: the emulation re-runs the query from the start
         }
       }
+      // publish: the record and the list entry before the record index, which
+      // an emulation pass running beside this kernel reads as "ready"
+      __threadfence();
       __syncwarp();
       if (lane == 0) {
         uint32_t pos = atomicAdd(a.emu_count, 1u);
         a.emu_list[pos] = qi;
-        a.emu_rec[pos] = r;
+        __threadfence();
+        atomicExch(a.emu_rec + pos, r);
       }
       __syncwarp();
       continue;

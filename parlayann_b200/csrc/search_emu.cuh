@@ -38,7 +38,41 @@ struct EmuArgs {
   uint32_t* overflow_rec;
   uint32_t* overflow_count;
   const uint32_t* job_rec;  // per job: resume record (tier 0's saved state) or PAD
+  // 1: a pass that runs beside the search tiers still publishing hand-offs
+  // (see emu_claim); 0: every job is published
+  uint32_t early;
 };
+
+// job_rec value of a hand-off slot taken but not yet written
+constexpr uint32_t EMU_NOT_READY = 0xFEFEFEFEu;
+
+// The next job of an emulation pass, or PANN_PAD when there is none (one
+// thread). With early set the pass runs while tier 0 and tier 2 still hand
+// queries over: it takes the next job only if that slot is published (its
+// record index written after the record itself, behind a fence) and
+// otherwise ends; it never waits. A pass after the search tiers takes every
+// job left. Passes take jobs from one counter, so each job runs once.
+__device__ __forceinline__ uint32_t emu_claim(uint32_t* counter, const uint32_t* njobs_dev, uint32_t nq,
+                                              const uint32_t* job_rec, bool early) {
+  if (!early) {
+    const uint32_t njobs = njobs_dev ? *njobs_dev : nq;
+    const uint32_t j = atomicAdd(counter, 1u);
+    return j < njobs ? j : PANN_PAD;
+  }
+  uint32_t c = *reinterpret_cast<volatile uint32_t*>(counter);
+  for (uint32_t guard = 0; guard < (1u << 20); guard++) {
+    const uint32_t n = *reinterpret_cast<const volatile uint32_t*>(njobs_dev);
+    if (c >= n) break;
+    if (reinterpret_cast<const volatile uint32_t*>(job_rec)[c] == EMU_NOT_READY) break;
+    const uint32_t prev = atomicCAS(counter, c, c + 1);
+    if (prev == c) {
+      __threadfence();
+      return c;
+    }
+    c = prev;
+  }
+  return PANN_PAD;
+}
 
 // (k * 0xbf58476d1ce4e5b9) & mask for mask < 2^32: the product's low 32 bits
 // depend only on the multiplier's low 32 bits, so 32-bit arithmetic suffices.
@@ -1070,15 +1104,15 @@ __global__ void __launch_bounds__(NW * 32, 1) search_emulate_block_kernel(Search
   uint32_t* tabA = reinterpret_cast<uint32_t*>(smem + y.tabA);
   uint32_t* tabB = reinterpret_cast<uint32_t*>(smem + y.tabB);
   const uint32_t vmask = e.vs_slots - 1;
-  const uint32_t njobs = a.njobs_dev ? *a.njobs_dev : a.nq;
   const uint32_t nel = a.dl < a.R ? a.dl : a.R;
 
   for (;;) {
     __syncthreads();
-    if (tid == 0) ctrl[0] = atomicAdd(a.job_counter, 1u);
+    if (tid == 0) ctrl[0] = emu_claim(a.job_counter, a.njobs_dev, a.nq, e.job_rec, e.early != 0);
     __syncthreads();
     const uint32_t job = ctrl[0];
-    if (job >= njobs) break;
+    if (job == PANN_PAD) break;
+    if (e.early) __threadfence();  // the record was published behind a fence
     const uint32_t qi = a.job_list ? a.job_list[job] : job;
     const uint32_t rec_id = e.job_rec ? e.job_rec[job] : PANN_PAD;
     const uint32_t L = a.qL ? a.qL[qi] : a.L;

@@ -61,8 +61,11 @@ uint32_t tier0_slots(const SearchPlan& p, uint32_t R);
 // warps per block.
 int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int precision, uint32_t S_force,
                int wpb_force, TierSizes* z, int minb_force = 0);
+// side (optional): the index's side stream; the exact-emulation tier then
+// also runs a pass beside tier 0's tail on it (idx->ev_fork / ev_join order
+// it), taking hand-offs as they are published without waiting for any.
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a, const TierSizes& z,
-                  const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank);
+                  const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank, cudaStream_t side = nullptr);
 // The multi-parent tile search of the precision form (tile.cu).
 // tile_rows > 0 fixes the rows staged per round (CUDA-core scoring), else chosen for occupancy.
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
