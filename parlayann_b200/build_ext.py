@@ -7,7 +7,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-SOURCES = ["capi.cu", "build.cu", "bruteforce.cu", "batch.cu", "tile.cu", "range.cu", "noalloc.cu", "quant.cu", "score.cu", "synth.cpp", "serve.cpp"]
+SOURCES = ["capi.cu", "build.cu", "bruteforce.cu", "batch.cu", "tile.cu", "range.cu", "noalloc.cu", "quant.cu", "score.cu", "order.cu", "synth.cpp", "serve.cpp"]
 OUT = os.path.join(HERE, "libparlayann_b200.so")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

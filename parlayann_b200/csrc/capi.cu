@@ -668,6 +668,17 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   if (rc) return rc;
   SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
                            d_vis_keys, vis_cap);
+  // queries far from the start point first, where they queue for tier 0's warps
+  static const bool keep_order = [] {
+    const char* e = std::getenv("PANN_T0_ORDER");
+    return e && e[0] == '0';
+  }();
+  if (!keep_order && nq > z.slots) {
+    const uint32_t* order = nullptr;
+    rc = order_far_first(idx, d_queries, d_self_ids, d_starts, nq, st, &order);
+    if (rc) return rc;
+    b.job_list0 = order;
+  }
   return enqueue_tiers(idx, plan, a, z, b, st, precision, rerank, side_stream(idx));
 }
 
@@ -807,6 +818,7 @@ int pann_index_destroy(pann_index* idx) {
                     &idx->range_pool, &idx->range_out})
     b->release();
   idx->lp_norms.release();
+  idx->order.release();
   if (idx->ev_fork) cudaEventDestroy(idx->ev_fork);
   if (idx->ev_join) cudaEventDestroy(idx->ev_join);
   if (idx->side) cudaStreamDestroy(idx->side);

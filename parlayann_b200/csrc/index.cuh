@@ -82,6 +82,7 @@ struct pann_index {
   uint64_t range_held = 0;  // ids in range_out left for pann_range_fetch (0: none)
   // precision form: low-precision copy of float32 points (lowprec.cuh)
   pann::DevBuf lp_rows, lp_scales, lp_norms;
+  pann::DevBuf order;  // tier-0 job order of a plain search (order.cu)
   int lp_prec = 0;
   uint64_t lp_stride = 0;
   uint32_t lp_chunks = 0;

@@ -66,6 +66,10 @@ int size_tiers(const pann_index* idx, const SearchPlan& plan, uint64_t nq, int p
 // it), taking hand-offs as they are published without waiting for any.
 int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArgs& a, const TierSizes& z,
                   const TierBufs& b, cudaStream_t st, int precision, uint32_t rerank, cudaStream_t side = nullptr);
+// The tier-0 job order farthest-from-the-start-point first (order.cu):
+// *order points into idx->order, valid until the next call.
+int order_far_first(pann_index* idx, const uint8_t* d_queries, const uint32_t* d_self_ids, const uint32_t* d_starts,
+                    uint32_t nq, cudaStream_t st, const uint32_t** order);
 // The multi-parent tile search of the precision form (tile.cu).
 // tile_rows > 0 fixes the rows staged per round (CUDA-core scoring), else chosen for occupancy.
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
