@@ -35,7 +35,8 @@ struct pann_batch {
   pann::TierSizes z{};
   // device buffers, allocated at creation
   pann::DevBuf q, qk, qL, order, ids, dists, vis, cmps, status, counters, redo, spill, handoff, gt2, ge2, starts;
-  // pinned host staging for the per-query arrays (k, beam, order, nq)
+  pann::DevBuf oscratch;  // keys and sort scratch of the device-side job order
+  // pinned host staging for the per-query arrays (k, beam; nq in the last word)
   uint32_t* h_stage = nullptr;
   cudaEvent_t staged = nullptr;  // the last upload from h_stage has completed
   cudaStream_t cap = nullptr;    // capture stream
@@ -85,6 +86,11 @@ static int enqueue(pann_batch* b, const TierSizes& z, cudaStream_t st) {
   a.qk = b->qk.as<uint32_t>();
   a.qL = b->qL.as<uint32_t>();
   a.kstride = b->plan.k;
+  // job order: longest beam first, then the queries farthest from the start point
+  int orc = order_batch(idx, b->q.as<uint8_t>(), b->starts.as<uint32_t>(), b->qL.as<uint32_t>(),
+                        b->counters.as<uint32_t>() + 32, b->max_q, b->oscratch.p, b->oscratch.bytes,
+                        b->order.as<uint32_t>(), st);
+  if (orc) return orc;
   if (b->parents > 0 && b->prec != PREC_F32) {
     a.job_list = b->order.as<uint32_t>();
     a.njobs_dev = b->counters.as<uint32_t>() + 32;
@@ -351,6 +357,7 @@ int pann_batch_create(pann_batch** out, pann_index* idx, uint32_t max_queries, c
   need(b->qk, 4 * m);
   need(b->qL, 4 * m);
   need(b->order, 4 * m);
+  need(b->oscratch, batch_order_scratch_bytes((uint32_t)m));
   need(b->ids, 4 * m * plan.k);
   need(b->dists, 4 * m * plan.k);
   need(b->vis, 4 * m);
@@ -391,32 +398,19 @@ int pann_batch_run(pann_batch* b, const void* queries, uint32_t nq, const uint32
   }
   pann_index* idx = b->idx;
   cudaStream_t st = on_device ? static_cast<cudaStream_t>(stream) : idx->stream;
-  // stage k, beam, the longest-beam-first order and nq (counting sort on beam)
+  // stage k, beam and nq (the job order is made on the device by the launch sequence)
   PANN_CUDA(cudaEventSynchronize(b->staged));  // the previous run's upload is done with h_stage
   uint32_t* hk = b->h_stage;
   uint32_t* hL = hk + b->max_q;
-  uint32_t* ho = hL + b->max_q;
-  uint32_t* hn = ho + b->max_q;
+  uint32_t* hn = hL + 2 * b->max_q;
   std::memcpy(hk, k, 4ull * nq);
   std::memcpy(hL, beam, 4ull * nq);
-  {
-    std::vector<uint32_t> count(p.L + 2, 0);
-    for (uint32_t i = 0; i < nq; i++) count[p.L - beam[i]]++;
-    uint32_t acc = 0;
-    for (auto& c : count) {
-      uint32_t t = c;
-      c = acc;
-      acc += t;
-    }
-    for (uint32_t i = 0; i < nq; i++) ho[count[p.L - beam[i]]++] = i;
-  }
   *hn = nq;
   const size_t rb = (size_t)idx->d * idx->esize;
   PANN_CUDA(cudaMemcpy2DAsync(b->q.p, idx->stride, queries, rb, rb, nq,
                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(b->qk.p, hk, 4ull * nq, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(b->qL.p, hL, 4ull * nq, cudaMemcpyHostToDevice, st));
-  PANN_CUDA(cudaMemcpyAsync(b->order.p, ho, 4ull * nq, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(b->counters.as<uint32_t>() + 32, hn, 4, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaEventRecord(b->staged, st));
 
@@ -503,7 +497,7 @@ int pann_batch_destroy(pann_batch* b) {
   if (b->staged) cudaEventSynchronize(b->staged);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (DevBuf* d : {&b->q, &b->qk, &b->qL, &b->order, &b->ids, &b->dists, &b->vis, &b->cmps, &b->status, &b->counters,
+  for (DevBuf* d : {&b->q, &b->qk, &b->qL, &b->order, &b->oscratch, &b->ids, &b->dists, &b->vis, &b->cmps, &b->status, &b->counters,
                     &b->redo, &b->spill, &b->handoff, &b->gt2, &b->ge2, &b->starts})
     d->release();
   if (b->h_stage) cudaFreeHost(b->h_stage);

@@ -615,6 +615,15 @@ SearchArgs base_args(const pann_index* idx, const SearchPlan& plan, const uint8_
   return a;
 }
 
+// PANN_T0_ORDER=0: search jobs in the given query order.
+static bool t0_keep_order() {
+  static const bool keep = [] {
+    const char* e = std::getenv("PANN_T0_ORDER");
+    return e && e[0] == '0';
+  }();
+  return keep;
+}
+
 // The index's side stream (lowest priority) and its fork / join events,
 // created on first use; nullptr if they cannot be created (the emulation
 // then runs only after the search tiers). PANN_EMU_OVERLAP=0 turns the
@@ -657,6 +666,12 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
     PANN_CUDA(idx->counters.ensure(64));
     SearchArgs a = base_args(idx, plan, d_queries, nullptr, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
                              nullptr, 0);
+    if (!t0_keep_order() && nq > 4u * (uint32_t)idx->sm_count) {
+      const uint32_t* order = nullptr;
+      int orc = order_far_first(idx, d_queries, nullptr, d_starts, nq, st, &order);
+      if (orc) return orc;
+      a.job_list = order;  // one CTA per query: the far queries first as well
+    }
     int rc = enqueue_tile(idx, plan, a, parents, idx->counters.as<uint32_t>() + 10, precision, rerank, st, scorer);
     if (rc != PANN_EINVAL) return rc;  // EINVAL: does not fit; take the single-parent path
   }
@@ -669,11 +684,7 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
   SearchArgs a = base_args(idx, plan, d_queries, d_self_ids, nq, d_starts, d_ids, d_dists, d_vis, d_cmps, d_status,
                            d_vis_keys, vis_cap);
   // queries far from the start point first, where they queue for tier 0's warps
-  static const bool keep_order = [] {
-    const char* e = std::getenv("PANN_T0_ORDER");
-    return e && e[0] == '0';
-  }();
-  if (!keep_order && nq > z.slots) {
+  if (!t0_keep_order() && nq > z.slots) {
     const uint32_t* order = nullptr;
     rc = order_far_first(idx, d_queries, d_self_ids, d_starts, nq, st, &order);
     if (rc) return rc;

@@ -70,6 +70,12 @@ int enqueue_tiers(const pann_index* idx, const SearchPlan& plan, const SearchArg
 // *order points into idx->order, valid until the next call.
 int order_far_first(pann_index* idx, const uint8_t* d_queries, const uint32_t* d_self_ids, const uint32_t* d_starts,
                     uint32_t nq, cudaStream_t st, const uint32_t** order);
+// A batch's job order (order.cu): longest beam first, then farthest from the
+// first start point, for the nq queries in device memory (read at run time).
+size_t batch_order_scratch_bytes(uint32_t max_q);
+int order_batch(const pann_index* idx, const uint8_t* d_queries, const uint32_t* d_starts, const uint32_t* d_qL,
+                const uint32_t* d_nq, uint32_t max_q, void* scratch, size_t scratch_bytes, uint32_t* d_order,
+                cudaStream_t st);
 // The multi-parent tile search of the precision form (tile.cu).
 // tile_rows > 0 fixes the rows staged per round (CUDA-core scoring), else chosen for occupancy.
 int enqueue_tile(const pann_index* idx, const SearchPlan& plan, SearchArgs a, uint32_t parents, uint32_t* job_counter,
