@@ -127,6 +127,8 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
 // the inputs (pinned host arrays: nq query rows of d * element bytes, per-query
 // k and beam, the job order), enqueues the search on `st` and the copies of
 // its ids and distances (nq rows of bounds->k) to pinned host memory.
+// Takes range search's largest scratch up front (range.cu).
+int range_reserve(pann_index* idx);
 int batch_scratch_bytes(const pann_index* idx, const pann_query_params* bounds, uint32_t n_start, uint32_t nq,
                         int precision, uint32_t parents, size_t* bytes);
 int run_in_arena(pann_index* idx, uint8_t* arena, size_t arena_bytes, const pann_query_params* bounds,

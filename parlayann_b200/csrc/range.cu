@@ -406,6 +406,20 @@ static uint32_t ceil_log2(uint64_t x) {
 
 using namespace pann;
 
+namespace pann {
+// Range search's largest device scratch taken once: the expansion tables at
+// their design cap (4 GB across a tier's slots) and a pool of 4M answers.
+// A serving loop calls it at creation, so the range requests it groups never
+// reallocate (a free drains the whole device, stalling the k-NN batches
+// beside it).
+int range_reserve(pann_index* idx) {
+  PANN_CUDA(idx->range_tabs.ensure_grow(4ull << 30));
+  PANN_CUDA(idx->range_pool.ensure_grow(4ull << 22));
+  PANN_CUDA(idx->range_out.ensure_grow(4ull << 22));
+  return PANN_OK;
+}
+}  // namespace pann
+
 extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t nq, const pann_range_params* rp,
                                  uint32_t start_point, uint64_t* out_offsets, uint32_t* out_ids, uint64_t ids_cap,
                                  uint32_t* out_visited, uint32_t* out_cmps, uint32_t* out_flags) {
@@ -428,12 +442,12 @@ extern "C" int pann_range_search(pann_index* idx, const void* queries, uint32_t 
   if (rc) return rc;
   const uint32_t beam = rp->beam;
   const size_t rb = (size_t)idx->d * idx->esize;
-  PANN_CUDA(idx->q.ensure(idx->stride * (size_t)nq));
-  PANN_CUDA(idx->ids.ensure(4ull * beam * nq));
-  PANN_CUDA(idx->dists.ensure(4ull * beam * nq));
-  PANN_CUDA(idx->vis.ensure(4ull * nq));
-  PANN_CUDA(idx->cmps.ensure(4ull * nq));
-  PANN_CUDA(idx->status.ensure(4ull * nq));
+  PANN_CUDA(idx->q.ensure_grow(idx->stride * (size_t)nq));
+  PANN_CUDA(idx->ids.ensure_grow(4ull * beam * nq));
+  PANN_CUDA(idx->dists.ensure_grow(4ull * beam * nq));
+  PANN_CUDA(idx->vis.ensure_grow(4ull * nq));
+  PANN_CUDA(idx->cmps.ensure_grow(4ull * nq));
+  PANN_CUDA(idx->status.ensure_grow(4ull * nq));
   if (rb != idx->stride) PANN_CUDA(cudaMemsetAsync(idx->q.p, 0, idx->stride * (size_t)nq, st));
   PANN_CUDA(cudaMemcpy2DAsync(idx->q.p, idx->stride, queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
 

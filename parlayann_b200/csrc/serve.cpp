@@ -257,12 +257,16 @@ void ranger_main(pann_server* s) {
       s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
       continue;
     }
-    // every waiting range request with the same parameters, as one search
+    // the waiting range requests with the same parameters, up to 16 queries,
+    // as one search (the answers of a group stay within the reserved pool)
     std::vector<Request*> group;
+    uint32_t gq = 0;
     for (auto it = s->range_q.begin(); it != s->range_q.end();) {
       Request* r = *it;
       const Request* f = group.empty() ? r : group.front();
-      if (group.empty() || (r->start == f->start && std::memcmp(&r->rp, &f->rp, sizeof(pann_range_params)) == 0)) {
+      if (group.empty() || (gq + r->nq <= 16 && r->start == f->start &&
+                            std::memcmp(&r->rp, &f->rp, sizeof(pann_range_params)) == 0)) {
+        gq += r->nq;
         group.push_back(r);
         it = s->range_q.erase(it);
       } else {
@@ -390,6 +394,8 @@ int pann_server_create(pann_server** out, pann_index* idx, const pann_server_opt
     if (e == cudaSuccess) e = cudaMallocHost(&sl.h_d, 4 * m * opt->max_k);
     if (e != cudaSuccess) return bail(pann::cuda_fail(e, "server slot"));
   }
+  // range search's scratch taken now, not while k-NN batches run
+  if (pann::range_reserve(idx) != PANN_OK) cudaGetLastError();  // without it range search allocates as it goes
   s->stats_t0 = clk::now();
   s->dispatcher = std::thread(dispatcher_main, s);
   s->ranger = std::thread(ranger_main, s);
