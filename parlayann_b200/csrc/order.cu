@@ -18,9 +18,7 @@ namespace pann {
 template <int DT>
 __global__ void start_dist_kernel(const uint8_t* __restrict__ points, uint64_t stride, uint32_t d,
                                   const uint8_t* __restrict__ queries, const uint32_t* __restrict__ self_ids,
-                                  const uint32_t* __restrict__ starts, uint32_t nq, uint32_t* keys, uint32_t* vals,
-                                  uint64_t npoints) {
-  (void)npoints;
+                                  const uint32_t* __restrict__ starts, uint32_t nq, uint32_t* keys, uint32_t* vals) {
   const uint8_t* s = points + (uint64_t)starts[0] * stride;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
     const uint8_t* q = self_ids ? points + (uint64_t)self_ids[i] * stride : queries + (uint64_t)i * stride;
@@ -40,36 +38,7 @@ __global__ void start_dist_kernel(const uint8_t* __restrict__ points, uint64_t s
       const float df = x - y;
       acc = fmaf(df, df, acc);
     }
-#ifdef PANN_ORDER_PIVOTS
-    // variant: distance coarsened to 2^PANN_ORDER_BITS buckets an octave, then
-    // the nearest of PANN_ORDER_PIVOTS spread-out base points, so queries of
-    // one region follow each other within a bucket
-    uint32_t best = 0;
-    float bestd = 3.0e38f;
-    for (uint32_t pv = 0; pv < PANN_ORDER_PIVOTS; pv++) {
-      const uint8_t* r = points + (uint64_t)(npoints / PANN_ORDER_PIVOTS) * pv * stride;
-      float a2 = 0.0f;
-      for (uint32_t t = 0; t < d; t++) {
-        float x, y;
-        if (DT == DT_F32) {
-          x = reinterpret_cast<const float*>(q)[t];
-          y = reinterpret_cast<const float*>(r)[t];
-        } else if (DT == DT_U8) {
-          x = (float)q[t];
-          y = (float)r[t];
-        } else {
-          x = (float)(int8_t)q[t];
-          y = (float)(int8_t)r[t];
-        }
-        const float df = x - y;
-        a2 = fmaf(df, df, a2);
-      }
-      if (a2 < bestd) { bestd = a2; best = pv; }
-    }
-    keys[i] = ((__float_as_uint(acc) >> (23 - PANN_ORDER_BITS)) << 8) | (PANN_ORDER_PIVOTS - 1 - best);
-#else
     keys[i] = __float_as_uint(acc);  // non-negative: the bit pattern orders as the value
-#endif
     vals[i] = i;
   }
 }
@@ -90,13 +59,13 @@ int order_far_first(pann_index* idx, const uint8_t* d_queries, const uint32_t* d
   const int blocks = (int)std::min<uint64_t>((nq + 255) / 256, 4ull * idx->sm_count);
   if (idx->dtype == DT_F32)
     start_dist_kernel<DT_F32><<<blocks, 256, 0, st>>>(idx->d_points, idx->stride, idx->d, d_queries, d_self_ids,
-                                                      d_starts, nq, kin, vin, idx->n);
+                                                      d_starts, nq, kin, vin);
   else if (idx->dtype == DT_U8)
     start_dist_kernel<DT_U8><<<blocks, 256, 0, st>>>(idx->d_points, idx->stride, idx->d, d_queries, d_self_ids,
-                                                     d_starts, nq, kin, vin, idx->n);
+                                                     d_starts, nq, kin, vin);
   else
     start_dist_kernel<DT_I8><<<blocks, 256, 0, st>>>(idx->d_points, idx->stride, idx->d, d_queries, d_self_ids,
-                                                     d_starts, nq, kin, vin, idx->n);
+                                                     d_starts, nq, kin, vin);
   PANN_CUDA(cudaGetLastError());
   size_t tb = tmp;
   PANN_CUDA(cub::DeviceRadixSort::SortPairsDescending(ctmp, tb, kin, kout, vin, vout, (int)nq, 0, 32, st));
