@@ -289,3 +289,20 @@ def test_groundtruth_float_fast_path_with_duplicates(lib_built):
     np.testing.assert_array_equal(ids, oi)
     np.testing.assert_array_equal(dd, od)
     idx.close()
+
+
+def test_many_queries_far_first_order_and_overlapped_emulation(lib_built):
+    """More queries than tier 0 has warps, so the jobs are taken farthest from the start point first,
+    and enough hashset growth that the emulation pass beside tier 0 takes hand-offs while tier 0
+    still runs: every answer, counter and growth flag still equals the oracle's."""
+    base = random_points(np.uint8, 20000, 8, 11)
+    q = random_points(np.uint8, 3000, 8, 12)
+    g = O.random_graph(20000, 64, 13, min_deg=60)
+    idx = P.Index(base, 64)
+    idx.set_graph(g)
+    r = idx.search(q, 10, 40, batch_factor=1.0)
+    o = O.search("oracle", base, q, g, 10, 40, batch_factor=1.0)
+    assert (o["hash_grew"] > 0).sum() > 10
+    np.testing.assert_array_equal(r.flags == 1, o["hash_grew"] > 0)
+    check_same(r, o)
+    idx.close()
