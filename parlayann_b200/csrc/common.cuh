@@ -186,17 +186,21 @@ __device__ __forceinline__ uint64_t f32_chunk2(uint64_t r, float4 a, float4 b, f
 // query are zero-padded to whole 16-byte chunks; a padded term adds +0.0,
 // which leaves the running sum unchanged bit for bit (it starts at +0.0 and
 // can never be -0.0), so whole chunks are summed without per-element tests.
+#ifndef PANN_F32_ROW_CHUNKS
+#define PANN_F32_ROW_CHUNKS 8
+#endif
 template <int MT>
 __device__ __forceinline__ float dist_f32_row(const float4* __restrict__ row, const float4* q, int nvec) {
+  constexpr int CH = PANN_F32_ROW_CHUNKS;
   float r = 0.0f;
   prefetch_row_l2(row, nvec);
-  for (int c0 = 0; c0 < nvec; c0 += ROW_CHUNKS) {
-    float4 buf[ROW_CHUNKS];
+  for (int c0 = 0; c0 < nvec; c0 += CH) {
+    float4 buf[CH];
 #pragma unroll
-    for (int c = 0; c < ROW_CHUNKS; c++)
+    for (int c = 0; c < CH; c++)
       if (c0 + c < nvec) buf[c] = __ldg(row + c0 + c);
 #pragma unroll
-    for (int c = 0; c < ROW_CHUNKS; c++)
+    for (int c = 0; c < CH; c++)
       if (c0 + c < nvec) r = f32_chunk<MT>(r, buf[c], q[c0 + c]);
   }
   return MT == MT_L2 ? r : -r;
