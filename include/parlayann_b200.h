@@ -126,7 +126,13 @@ int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_qu
  * Does not synchronise. d_out_flags (may be NULL) receives per-query status
  * bits: 2 = the reference's hashset grows on this query (result reproduced
  * exactly), 1 or 16 = the query's state outgrew every buffer (result invalid),
- * 4 = fewer than k results. starts is a HOST array. */
+ * 4 = fewer than k results. starts is a HOST array. Part of the work (the
+ * exact emulation of the reference's hashset, beside the first search tier)
+ * may run on a stream the index owns; it is ordered after the work already
+ * on `stream` and before the rest of this call's work on `stream` by events,
+ * so to the caller the call behaves as work on `stream` alone. The queries
+ * are taken farthest from the first start point first (results do not
+ * depend on the order). */
 int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
                        uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
