@@ -223,7 +223,7 @@ def run_ours(args):
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=1800))
     dev = torch.device("cuda", local)
     lib = P.lib()
     base, q = make_data(P.synth_mixture)
