@@ -181,7 +181,8 @@ namespace {
 struct ArenaLayout {
   SearchPlan plan;
   TierSizes z;
-  size_t cnt, starts, q, qk, qL, order, ids, dists, vis, cmps, status, redo, spill, handoff, gt2, ge2, bytes;
+  size_t cnt, starts, q, qk, qL, order, okeys, okeys_bytes, ids, dists, vis, cmps, status, redo, spill, handoff, gt2,
+      ge2, bytes;
 };
 
 size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -211,6 +212,8 @@ int arena_layout(const pann_index* idx, const pann_query_params* bounds, uint32_
   y->qk = take(4ull * nq);
   y->qL = take(4ull * nq);
   y->order = take(4ull * nq);
+  y->okeys_bytes = batch_order_scratch_bytes(nq);
+  y->okeys = take(y->okeys_bytes);
   y->ids = take(4ull * nq * k);
   y->dists = take(4ull * nq * k);
   y->vis = take(4ull * nq);
@@ -258,8 +261,12 @@ int run_in_arena(pann_index* idx, uint8_t* arena, size_t arena_bytes, const pann
   PANN_CUDA(cudaMemcpy2DAsync(at(y.q), idx->stride, h_queries, rb, rb, nq, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(at(y.qk), h_k, 4ull * nq, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(at(y.qL), h_beam, 4ull * nq, cudaMemcpyHostToDevice, st));
-  PANN_CUDA(cudaMemcpyAsync(at(y.order), h_order, 4ull * nq, cudaMemcpyHostToDevice, st));
   PANN_CUDA(cudaMemcpyAsync(cnt + 32, h_order + nq, 4, cudaMemcpyHostToDevice, st));
+  // job order on the device: longest beam first, then farthest from the start point
+  rc = order_batch(idx, at(y.q), reinterpret_cast<const uint32_t*>(at(y.starts)),
+                   reinterpret_cast<const uint32_t*>(at(y.qL)), cnt + 32, nq, at(y.okeys), y.okeys_bytes,
+                   reinterpret_cast<uint32_t*>(at(y.order)), st);
+  if (rc) return rc;
   SearchArgs a = base_args(idx, y.plan, at(y.q), nullptr, nq, reinterpret_cast<const uint32_t*>(at(y.starts)),
                            reinterpret_cast<uint32_t*>(at(y.ids)), reinterpret_cast<float*>(at(y.dists)),
                            reinterpret_cast<uint32_t*>(at(y.vis)), reinterpret_cast<uint32_t*>(at(y.cmps)),

@@ -131,6 +131,8 @@ int run_search(pann_index* idx, const SearchPlan& plan, const uint8_t* d_queries
 int range_reserve(pann_index* idx);
 int batch_scratch_bytes(const pann_index* idx, const pann_query_params* bounds, uint32_t n_start, uint32_t nq,
                         int precision, uint32_t parents, size_t* bytes);
+// A batch laid out in a caller's arena (the serving loop's slots): h_order[nq]
+// holds nq in pinned memory; the job order itself is made on the device.
 int run_in_arena(pann_index* idx, uint8_t* arena, size_t arena_bytes, const pann_query_params* bounds,
                  const uint32_t* h_starts, uint32_t n_start, const uint8_t* h_queries, uint32_t nq, const uint32_t* h_k,
                  const uint32_t* h_beam, const uint32_t* h_order, int precision, uint32_t rerank, uint32_t parents,

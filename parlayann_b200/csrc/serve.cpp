@@ -65,7 +65,7 @@ struct Slot {
   uint8_t* h_q = nullptr;  // pinned: queries, per-query k / beam / job order, results
   uint32_t* h_k = nullptr;
   uint32_t* h_L = nullptr;
-  uint32_t* h_order = nullptr;  // nq job indices, then nq
+  uint32_t* h_order = nullptr;  // word nq: the job count (pinned, copied with the batch)
   uint32_t* h_ids = nullptr;
   float* h_d = nullptr;
   std::vector<Request*> reqs;
@@ -189,19 +189,8 @@ bool launch(pann_server* s, Slot& sl, std::unique_lock<std::mutex>& lk) {
     }
     at += r->nq;
   }
-  // longest beam first (counting sort), then the job count
-  {
-    std::vector<uint32_t> count(Lmax + 2, 0);
-    for (uint32_t i = 0; i < nq; i++) count[Lmax - sl.h_L[i]]++;
-    uint32_t acc = 0;
-    for (auto& c : count) {
-      const uint32_t t = c;
-      c = acc;
-      acc += t;
-    }
-    for (uint32_t i = 0; i < nq; i++) sl.h_order[count[Lmax - sl.h_L[i]]++] = i;
-    sl.h_order[nq] = nq;
-  }
+  // the job count (the job order, longest beam first, is made on the device)
+  sl.h_order[nq] = nq;
   pann_query_params bounds{kmax, Lmax, s->opt.limit, s->opt.degree_limit, s->opt.batch_factor};
   int rc = pann::run_in_arena(s->idx, sl.arena, s->scratch, &bounds, s->starts.data(), (uint32_t)s->starts.size(),
                               sl.h_q, nq, sl.h_k, sl.h_L, sl.h_order, s->opt.precision, 0, s->opt.parents,
