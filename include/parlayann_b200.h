@@ -132,7 +132,10 @@ int pann_search(pann_index* idx, const void* queries, uint32_t nq, const pann_qu
  * on `stream` and before the rest of this call's work on `stream` by events,
  * so to the caller the call behaves as work on `stream` alone. The queries
  * are taken farthest from the first start point first (results do not
- * depend on the order). */
+ * depend on the order). Searches on one index share its scratch buffers:
+ * device calls on the same index must be ordered on the GPU (one stream, or
+ * an event between them); concurrent work uses batch objects
+ * (pann_batch_create) or a server (pann_server_create), which own theirs. */
 int pann_search_device(pann_index* idx, const void* d_queries, uint32_t nq, const pann_query_params* qp,
                        const uint32_t* starts, uint32_t n_start, uint32_t* d_out_ids, float* d_out_dists,
                        uint32_t* d_out_visited, uint32_t* d_out_cmps, uint32_t* d_out_flags, void* stream);
