@@ -9,6 +9,12 @@
  * device pointers and a cudaStream_t (passed as void*) and return without
  * synchronising.
  *
+ * An index owns the scratch buffers of the searches and the build run on it:
+ * calls on one index are made from one host thread at a time. Batch objects
+ * (pann_batch_*) own their scratch, so different batches over one index may
+ * run from different threads and streams; a server (pann_server_*) takes
+ * requests from any thread.
+ *
  * Each declaration names the reference interface it replaces
  * (paths relative to the ParlayANN checkout).
  */
