@@ -1,6 +1,7 @@
 // Host-side pieces of the drop-in header, with no device call: PointRange
 // read from .bin files, Point::distance for both metrics and both element
-// types, the graph file read, edgeRange edits and the graph file write.
+// types, one-byte scalar quantization, the graph file read, edgeRange edits
+// and the graph file write.
 // Usage: host_check base_f32.bin base_u8.bin graph_in graph_out
 #include <cstdio>
 #include <vector>
@@ -20,6 +21,14 @@ int main(int argc, char** argv) {
     for (long j = 0; j < 6; j++)
       std::printf("d %ld %ld %a %a %a %a\n", i, j, F[i].distance(F[j]), FM[i].distance(FM[j]), U[i].distance(U[j]),
                   UM[i].distance(UM[j]));
+  // one-byte scalar quantization of the float range (point_range.h:55-71)
+  PointRange<Euclidian_Point<uint8_t>> Q(F);
+  std::printf("quant %a %d\n", Q.params.slope, Q.params.offset);
+  for (long i = 0; i < 3; i++) {
+    std::printf("qrow %ld", i);
+    for (long j = 0; j < Q.dimension(); j++) std::printf(" %d", (int)Q[i][j]);
+    std::printf("\n");
+  }
   Graph<uint32_t> G(argv[3]);
   std::printf("graph %zu %ld %zu\n", G.size(), G.max_degree(), G[4].size());
   G[0].clear_neighbors();

@@ -2,6 +2,7 @@
 that program builds, saves, reloads and searches an index on the GPU; its
 host-side pieces (point files, distances, graph files and edits) run on the
 CPU against restatements of the reference's formats and arithmetic."""
+import math
 import os
 import subprocess
 
@@ -112,6 +113,32 @@ def test_dropin_host_pieces_match_reference_formats(tmp_path, lib_built):
         assert float.fromhex(uip) == -float(np.float32((a * b).sum()))
         seen += 1
     assert seen == 36
+    # the same pairs through the oracle's distance (pinned to the reference)
+    from oracle import oracle as O
+    dist = O.olib().oracle_distance
+    for ln in lines:
+        if ln.startswith("d "):
+            _, i, j, fl2, fip, ul2, uip = ln.split()
+            i, j = int(i), int(j)
+            for dt, mt, base, got in ((2, 0, bf, fl2), (2, 1, bf, fip), (0, 0, bu, ul2), (0, 1, bu, uip)):
+                want = dist(dt, mt, base.shape[1], base[i].ctypes.data, base[j].ctypes.data)
+                assert float.fromhex(got) == want
+    # one-byte quantization: the oracle's parameters, translate_point restated
+    slope = np.zeros(1, np.float32)
+    offset = np.zeros(1, np.int32)
+    O.olib().oracle_quant_params(12, 24, bf.ctypes.data, slope.ctypes.data, offset.ctypes.data)
+    q = [ln for ln in lines if ln.startswith("quant ")][0].split()
+    assert np.float32(float.fromhex(q[1])) == slope[0] and int(q[2]) == int(offset[0])
+    for ln in lines:
+        if ln.startswith("qrow "):
+            parts = ln.split()
+            i = int(parts[1])
+            want = []
+            for x in bf[i]:
+                v = float(np.float32(x) * slope[0])
+                r = int(math.copysign(math.floor(abs(v) + 0.5), v)) - int(offset[0])  # roundf: half away from 0
+                want.append(min(255, max(0, r)))
+            assert [int(t) for t in parts[2:]] == want
     assert f"graph 12 8 {len(rows[4])}" in lines
     n, max_deg, out = _read_graph(paths[3])
     assert (n, max_deg) == (12, 8)
