@@ -91,6 +91,44 @@ def test_oracle_search_matches_reference(dtype, metric, lib_built):
 
 
 @needs_ref
+def test_oracle_search_matches_reference_random_sweep(lib_built):
+    """Seeded random QueryParams over every dtype and metric on small random
+    graphs (repeated neighbours included, as the reference's graph allows):
+    the restatement and the in-place reference agree on everything they
+    return."""
+    rng = np.random.default_rng(2024)
+    dts = [np.uint8, np.int8, np.float32]
+    for case in range(36):
+        dtype = dts[case % 3]
+        metric = (case // 3) % 2
+        n = int(rng.integers(200, 900))
+        d = int(rng.integers(3, 40))
+        R = int(rng.integers(4, 33))
+        base = random_points(dtype, n, d, 100 + case)
+        q = random_points(dtype, 8, d, 200 + case)
+        g = O.random_graph(n, R, 300 + case)
+        if case % 4 == 0:  # a repeated neighbour in some rows
+            for i in range(0, n, 7):
+                if g[i, 0] >= 2:
+                    g[i, 2] = g[i, 1]
+        L = int(rng.integers(1, 80))
+        k = int(rng.integers(1, L + 1))
+        lim = None if rng.random() < 0.6 else int(rng.integers(1, 3 * L + 2))
+        dl = None if rng.random() < 0.6 else int(rng.integers(1, R + 1))
+        # batch_factor <= 1: above it the reference's set_union can write past
+        # new_frontier (sized 2·max(L, starts) + max degree, beamSearch.h:95-96)
+        bf = float(rng.choice([0.0, 0.125, 0.5, 1.0]))
+        ns = int(rng.integers(1, min(L, 4) + 1))
+        st = tuple(int(x) for x in rng.choice(n, size=ns, replace=False))
+        args = dict(limit=lim, degree_limit=dl, batch_factor=bf, starts=st, metric=metric, full=True)
+        a = O.search("oracle", base, q, g, k, L, **args)
+        b = O.search("ref", base, q, g, k, L, **args)
+        for key in ["ids", "dists", "visited", "cmps", "frontier_n", "frontier_ids", "frontier_d", "visited_ids",
+                    "visited_d"]:
+            np.testing.assert_array_equal(a[key], b[key], err_msg=f"case {case} {key}")
+
+
+@needs_ref
 def test_oracle_hashset_growth_regime(lib_built):
     """A tiny beam with a dense graph pushes the reference's seen-set past its
     growth threshold; the restatement reproduces the reference's results there
