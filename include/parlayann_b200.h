@@ -55,7 +55,9 @@ typedef struct {
   uint32_t beam;          /* beamSize (L) */
   uint64_t limit;         /* maximum number of visited nodes */
   uint32_t degree_limit;  /* neighbours read per visited node */
-  double batch_factor;    /* deferral threshold, fraction of beam */
+  double batch_factor;    /* deferral threshold, fraction of beam; above 1 the reference's
+                             set_union can overrun its merge buffer (beamSearch.h:95-96,202-205),
+                             while here the buffers hold every deferred candidate */
 } pann_query_params;
 
 /* BuildParams fields used by the Vamana build (types.h:155-230). */
