@@ -218,6 +218,43 @@ def test_oracle_range_search_matches_reference(dtype, metric, lib_built):
     assert grew > 0   # the greedy expansion's seen-set grew somewhere
 
 
+@needs_ref
+def test_oracle_range_search_matches_reference_random_sweep(lib_built):
+    """Seeded random range searches (every dtype and metric, Greedy / Doubling
+    / Beam, beams 1-40, radii from the 0.2 % to the 20 % quantile, random
+    start points, early stopping on and off): the restatement and the
+    in-place reference return the same answers in the same order and the
+    same counters."""
+    rng = np.random.default_rng(77)
+    dts = [np.uint8, np.int8, np.float32]
+    answers = 0
+    for case in range(24):
+        dtype = dts[case % 3]
+        metric = (case // 3) % 2
+        n = int(rng.integers(300, 1500))
+        d = int(rng.integers(3, 24))
+        R = int(rng.integers(4, 25))
+        base = random_points(dtype, n, d, 500 + case)
+        q = random_points(dtype, 6, d, 600 + case)
+        g = O.random_graph(n, R, 700 + case)
+        quant = float(rng.choice([0.002, 0.01, 0.05, 0.2]))
+        beam = int(rng.integers(1, 41))
+        rtype = int(rng.choice([O.RANGE_GREEDY, O.RANGE_DOUBLING, O.RANGE_BEAM]))
+        start = int(rng.integers(0, n))
+        esc = 0 if rng.random() < 0.5 else int(rng.integers(1, 30))
+        esr_f = float(rng.choice([0.0, 1.0, 1.5, 3.0]))
+        radius = sample_radius(base, q, metric, quant)
+        kw = dict(start=start, esr=esr_f * radius, esc=esc, metric=metric)
+        a = O.range_search("oracle", base, q, g, beam, radius, rtype, **kw)
+        b = O.range_search("ref", base, q, g, beam, radius, rtype, **kw)
+        for x, y in zip(a["ids"], b["ids"]):
+            np.testing.assert_array_equal(x, y, err_msg=f"case {case}")
+        np.testing.assert_array_equal(a["visited"], b["visited"], err_msg=f"case {case}")
+        np.testing.assert_array_equal(a["cmps"], b["cmps"], err_msg=f"case {case}")
+        answers += sum(len(x) for x in a["ids"])
+    assert answers > 1000
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "rangegt_*.npz"))), ids=os.path.basename)
 def test_oracle_range_groundtruth_matches_golden(path, lib_built):
     """compute_range_groundtruth (data_tools/compute_range_groundtruth.cpp:14-30): every base id within the
