@@ -155,6 +155,32 @@ def test_oracle_build_matches_reference(dtype, metric, lib_built):
 
 
 @needs_ref
+def test_oracle_build_matches_reference_random_sweep(lib_built):
+    """Seeded random Vamana builds (every dtype and metric, R 3-24, L from R
+    to 80, alpha 1.0-1.5, one or two passes, search batch factors up to 1):
+    the restatement and the in-place reference give the same neighbour set
+    per vertex and the same distance-comparison total."""
+    rng = np.random.default_rng(91)
+    dts = [np.uint8, np.int8, np.float32]
+    for case in range(12):
+        dtype = dts[case % 3]
+        metric = (case // 3) % 2
+        n = int(rng.integers(200, 1500))
+        d = int(rng.integers(2, 24))
+        R = int(rng.integers(3, 25))
+        L = int(rng.integers(R, 81))
+        alpha = float(rng.choice([1.0, 1.1, 1.2, 1.5]))
+        passes = int(rng.integers(1, 3))
+        bf = float(rng.choice([0.125, 0.5, 1.0]))
+        base = random_points(dtype, n, d, 800 + case)
+        ga, ta = O.build_graph("oracle", base, R, L, alpha, passes, batch_factor=bf, metric=metric)
+        gb, tb = O.build_graph("ref", base, R, L, alpha, passes, batch_factor=bf, metric=metric)
+        assert ta == tb, case
+        for a, b in zip(_live_rows(ga), _live_rows(gb)):
+            assert sorted(a) == sorted(b), case
+
+
+@needs_ref
 def test_oracle_prune_matches_reference(lib_built):
     base = random_points(np.float32, 400, 12, 3)
     g = O.random_graph(400, 9, 4)
