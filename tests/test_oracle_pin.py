@@ -341,6 +341,42 @@ def test_oracle_mips_quantized_search_matches_reference(seed, n, d, R, L, k, rf,
 
 
 @needs_ref
+def test_oracle_quantized_search_matches_reference_random_sweep(lib_built):
+    """Seeded random beam_search_rerank cases over one-byte points (Euclidean
+    scalar quantization and the mips quantizer; value scales 0.01-37 so slope
+    and offset vary; k, beam, rerank factor, visit and degree limits, batch
+    factor and start point random): the restatement and the in-place
+    reference agree on parameters, ids, distance bits and counters."""
+    rng = np.random.default_rng(123)
+    for case in range(16):
+        metric = case % 2
+        n = int(rng.integers(300, 2500))
+        d = int(rng.integers(2, 40))
+        R = int(rng.integers(4, 25))
+        L = int(rng.integers(2, 70))
+        k = int(rng.integers(1, L + 1))
+        rf = float(rng.choice([1.0, 1.5, 2.0, 100.0]))
+        lim = None if rng.random() < 0.7 else int(rng.integers(k, 3 * L + 2))
+        dl = None if rng.random() < 0.7 else int(rng.integers(1, R + 1))
+        bf = float(rng.choice([0.0, 0.125, 0.5, 1.0]))
+        start = int(rng.integers(0, n))
+        scale = float(rng.choice([1.0, 0.01, 37.0]))
+        base = (rng.standard_normal((n, d)) * scale).astype(np.float32)
+        q = (rng.standard_normal((8, d)) * scale).astype(np.float32)
+        if metric == 1:
+            base /= np.linalg.norm(base, axis=1, keepdims=True).astype(np.float32)
+            q /= np.linalg.norm(q, axis=1, keepdims=True).astype(np.float32)
+        g = O.random_graph(n, R, 900 + case)
+        kw = dict(rerank_factor=rf, limit=lim, degree_limit=dl, batch_factor=bf, start=start, metric=metric)
+        a = O.search_quantized("oracle", base, q, g, k, L, **kw)
+        b = O.search_quantized("ref", base, q, g, k, L, **kw)
+        assert a["slope"] == b["slope"] and (metric == 1 or a["offset"] == b["offset"]), case
+        for key in ("ids", "visited", "cmps"):
+            np.testing.assert_array_equal(a[key], b[key], err_msg=f"case {case} {key}")
+        np.testing.assert_array_equal(a["dists"].view(np.uint32), b["dists"].view(np.uint32), err_msg=f"case {case}")
+
+
+@needs_ref
 def test_oracle_quantized_search_matches_reference(lib_built):
     for seed, (n, d, R, L, k, rf) in enumerate([(3000, 16, 20, 40, 10, 100.0), (3000, 24, 24, 30, 5, 2.0)]):
         base = random_points(np.float32, n, d, 140 + seed)
