@@ -198,6 +198,38 @@ def test_oracle_prune_matches_reference(lib_built):
                 assert a[1] == b[1]
 
 
+@needs_ref
+def test_oracle_prune_matches_reference_random_sweep(lib_built):
+    """Seeded random robustPrune calls (every dtype and metric, R 2-32, up to
+    120 candidates with repeated ids and the point itself among them in a
+    third of the cases, alpha 1.0-2.0, with and without the point's current
+    neighbours): same neighbours in the same order, same comparison count."""
+    rng = np.random.default_rng(31)
+    dts = [np.uint8, np.int8, np.float32]
+    for case in range(60):
+        dtype = dts[case % 3]
+        metric = (case // 3) % 2
+        n = int(rng.integers(50, 600))
+        d = int(rng.integers(2, 30))
+        R = int(rng.integers(2, 33))
+        base = random_points(dtype, n, d, 1000 + case)
+        g = O.random_graph(n, R, 1100 + case)
+        p = int(rng.integers(0, n))
+        m = int(rng.integers(1, min(n, 120)))
+        cand = rng.choice(n, size=m, replace=False).astype(np.uint32)
+        if case % 3 == 0:
+            cand = np.concatenate([cand, cand[: m // 3], [p]]).astype(np.uint32)
+        dt = O._DT[base.dtype]
+        cd = np.array([O.olib().oracle_distance(dt, metric, d, base[c].ctypes.data, base[p].ctypes.data)
+                       for c in cand], np.float32)
+        alpha = float(rng.choice([1.0, 1.1, 1.2, 1.5, 2.0]))
+        add = bool(rng.random() < 0.5)
+        a = O.robust_prune("oracle", base, g, p, cand, cd, alpha, add, metric=metric)
+        b = O.robust_prune("ref", base, g, p, cand, cd, alpha, add, metric=metric)
+        np.testing.assert_array_equal(a[0], b[0], err_msg=f"case {case}")
+        assert a[1] == b[1], case
+
+
 def sample_radius(base, q, metric, quant):
     d = q.shape[1]
     dt = O._DT[base.dtype]
@@ -303,6 +335,27 @@ def test_oracle_range_groundtruth_matches_reference(dtype, metric, lib_built):
         b = O.range_groundtruth("ref", base, q, radius, metric=metric)
         np.testing.assert_array_equal(a[0], b[0])
         np.testing.assert_array_equal(a[1], b[1])
+
+
+@needs_ref
+def test_oracle_range_groundtruth_matches_reference_random_sweep(lib_built):
+    """Seeded random range groundtruth runs (every dtype and metric, radii
+    from the 0.1 % to the 30 % quantile): every base id within the radius in
+    id order, as compute_range_groundtruth.cpp gives it."""
+    rng = np.random.default_rng(57)
+    dts = [np.uint8, np.int8, np.float32]
+    for case in range(12):
+        dtype = dts[case % 3]
+        metric = (case // 3) % 2
+        n = int(rng.integers(200, 3000))
+        d = int(rng.integers(2, 40))
+        base = random_points(dtype, n, d, 1200 + case)
+        q = random_points(dtype, 8, d, 1300 + case)
+        radius = sample_radius(base, q, metric, float(rng.choice([0.001, 0.01, 0.1, 0.3])))
+        a = O.range_groundtruth("oracle", base, q, radius, metric=metric)
+        b = O.range_groundtruth("ref", base, q, radius, metric=metric)
+        np.testing.assert_array_equal(a[0], b[0], err_msg=f"case {case}")
+        np.testing.assert_array_equal(a[1], b[1], err_msg=f"case {case}")
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLD, "quant_*.npz"))), ids=os.path.basename)
