@@ -101,3 +101,30 @@ def test_range_random_sweep_matches_oracle(lib_built):
         np.testing.assert_array_equal(r["visited"], o["visited"], err_msg=msg)
         np.testing.assert_array_equal(r["cmps"], o["cmps"], err_msg=msg)
         idx.close()
+
+
+def test_build_random_sweep_matches_oracle(lib_built):
+    """Seeded random Vamana builds (every dtype and metric, R 3-24, L from R to
+    80, alpha 1.0-1.5, one or two passes, search batch factors up to 1): the
+    GPU graph equals the oracle's (the oracle is pinned to the reference's
+    build by the same sweep in tests/test_oracle_pin.py)."""
+    rng = np.random.default_rng(91)
+    dts = [np.uint8, np.int8, np.float32]
+    for case in range(12):
+        dtype = dts[case % 3]
+        metric = [P.L2, P.MIPS][(case // 3) % 2]
+        n = int(rng.integers(200, 1500))
+        d = int(rng.integers(2, 24))
+        R = int(rng.integers(3, 25))
+        L = int(rng.integers(R, 81))
+        alpha = float(rng.choice([1.0, 1.1, 1.2, 1.5]))
+        passes = int(rng.integers(1, 3))
+        bf = float(rng.choice([0.125, 0.5, 1.0]))
+        base = random_points(dtype, n, d, 800 + case)
+        idx = P.Index(base, R, metric)
+        st = idx.build(L, alpha, num_passes=passes, batch_factor=bf)
+        o, tot = O.build_graph("oracle", base, R, L, alpha, passes, batch_factor=bf, metric=metric)
+        g = idx.get_graph()
+        assert [tuple(r[1:1 + r[0]].tolist()) for r in g] == [tuple(r[1:1 + r[0]].tolist()) for r in o], case
+        assert st.dist_cmps == tot, case
+        idx.close()
